@@ -1,0 +1,384 @@
+#!/usr/bin/env python3
+"""Benchmark: batched multi-GNSS acquisition cells/s on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload acq_multi_24mhz|acq_l1ca_12mhz]
+
+A step is one full search of the workload: every PRN of every signal group x
+every Doppler bin x every code offset, accumulated over all non-coherent sums,
+plus the per-PRN peak / C/N0 / fine-Doppler reduction. A cell is one
+(PRN, Doppler bin, code offset) of the final grid.
+
+Default workload acq_multi_24mhz: 24 MHz complex IQ, 3-bit, GPS L1 C/A (32
+PRNs, 21 bins, 20 x 1 ms), Galileo E1-B (36 PRNs, 81 bins, 5 x 4 ms, BOC(1,1)),
+BeiDou B1I (63 PRNs, 21 bins, 20 x 1 ms), GPS L5-I (32 PRNs, 21 bins, 20 x 1 ms),
+FFT length 2N - 343.9 M cells per step. Seeded synthetic IF (see
+pocketsdr_b200/synth.py); each rank searches its own IF block (weak scaling,
+no collective on the data path).
+
+Timing: W warm-up steps; then K steps, each bracketed by CUDA events on the
+launch stream, with an L2 flush (a 512 MB write) between steps outside the
+events; barrier + synchronize around the timed region; the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "acq cells/s (PRN x Doppler x code-offset) on 1 B200, batched vs plain, same peaks"
+UNIT = "cells/s"
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12   # 148 SM x 128 FP32 lanes x FMA at 1965 MHz
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--workload", default="acq_multi_24mhz")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+def dist_info():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.thr = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+
+        def rd():
+            for line in self.proc.stdout:
+                self.rows.append([x.strip() for x in line.split(",")])
+        self.thr = threading.Thread(target=rd, daemon=True)
+        self.thr.start()
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thr:
+            self.thr.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[0]))
+                mx = float(r[1])
+                for nm, v in zip(names, r[4:8]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def make_workload(name: str, seed: int):
+    from pocketsdr_b200 import synth
+    if name == "acq_multi_24mhz":
+        return synth.acq_multi_24mhz(seed=seed)
+    if name == "acq_l1ca_12mhz":
+        return synth.acq_l1ca_12mhz(seed=seed)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def cons_flops(groups) -> float:
+    """Algorithmic FLOPs of the consumer kernels of one step: per (PRN, bin,
+    sum) an L-point inverse FFT (5 L log2 L), the code product with scaling
+    (8 L) and the power accumulation (3 Nmax)."""
+    f = 0.0
+    for g in groups:
+        per = 5 * g.L * math.log2(g.L) + 8 * g.L + 3 * g.Nmax
+        f += len(g.prns) * len(g.fds) * g.n_sum * per
+    return f
+
+
+def cons_hbm_bytes(groups) -> float:
+    """Unique HBM bytes of the consumer kernels of one step: forward spectra
+    (8 L per bin and sum), code DFTs (8 L per PRN), grid written once
+    (4 Nmax per PRN and bin)."""
+    b = 0.0
+    for g in groups:
+        b += 8 * g.L * len(g.fds) * g.n_sum + 8 * g.L * len(g.prns) + 4 * g.Nmax * len(g.prns) * len(g.fds)
+    return b
+
+
+def load_traffic() -> dict:
+    """ncu dram bytes per consumer launch, from profiles/cons_kernel_traffic.txt
+    (`<workload> <bytes_per_launch>` lines), if recorded."""
+    path = os.path.join(ROOT, "profiles", "cons_kernel_traffic.txt")
+    out = {}
+    if os.path.exists(path):
+        for line in open(path):
+            p = line.split()
+            if len(p) == 2 and not line.startswith("#"):
+                try:
+                    out[p[0]] = float(p[1])
+                except ValueError:
+                    pass
+    return out
+
+
+# ---------------------------------------------------------------------------
+def cpu_reference_rate(wl, max_threads: int | None = None, budget_prn: int | None = None):
+    """Reference CPU throughput (cells/s) of the whole workload on this host,
+    estimated from a bounded sample: for each group, up to `threads` PRN
+    searches (every bin, every sum, the reference's own sdr_search_code built
+    from source, or the oracle restatement when that build is absent) run in
+    parallel threads; core-seconds per PRN scale to the full PRN set, spread
+    over all cores."""
+    import concurrent.futures as cf
+    from oracle import oracle
+    from pocketsdr_b200 import synth
+    R = oracle.best()
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    threads = min(cores, max_threads or cores)
+    total_core_s, total_cells, sample_desc = 0.0, 0, []
+    for g in wl.groups:
+        n = min(len(g.prns), threads, budget_prn or threads)
+        cfs = [synth.tiled_code_fft(g.sig, p, g.fs, g.tile, g.N, g.L - g.N) for p in g.prns[:n]]
+        buf = wl.bufs[g.buf]
+
+        def one(c):
+            P = np.zeros((len(g.fds), g.L), np.float32)
+            t0 = time.perf_counter()
+            for s in range(g.n_sum):
+                R.search_code(c, buf, (s * g.N) % len(buf), g.L, g.fs, g.fi, g.fds, P, g.T)
+            R.corr_max(P, g.L, g.Nmax, len(g.fds), g.T)
+            return time.perf_counter() - t0
+        t0 = time.perf_counter()
+        with cf.ThreadPoolExecutor(max_workers=n) as ex:
+            per = list(ex.map(one, cfs))
+        wall = time.perf_counter() - t0
+        core_s_per_prn = sum(per) / n
+        total_core_s += core_s_per_prn * len(g.prns)
+        total_cells += len(g.prns) * len(g.fds) * g.Nmax
+        sample_desc.append(f"{g.sig}:{n}/{len(g.prns)} PRN ({wall:.1f}s)")
+    rate = total_cells / (total_core_s / threads)
+    return rate, threads, R.kind, "; ".join(sample_desc) + \
+        f"; full PRN sets extrapolated from core-seconds per PRN over {threads} threads"
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args):
+    rank, world, _ = dist_info()
+    if rank != 0:
+        return 0
+    wl = make_workload(args.workload, 2)
+    vals = []
+    desc = ""
+    for k in range(args.warmup + args.steps):
+        rate, cores, kind, desc = cpu_reference_rate(wl, budget_prn=4)
+        if k >= args.warmup:
+            vals.append(rate)
+    v = statistics.median(vals)
+    ms = wl.cells / v * 1e3
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "cells_per_step": wl.cells},
+            "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": desc},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    rank, world, local = dist_info()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    from pocketsdr_b200 import acquire, synth
+    from pocketsdr_b200._lib import lib
+
+    wl = make_workload(args.workload, 2 + rank)
+    cfs = [synth.group_code_ffts(g) for g in wl.groups]
+    plan = acquire.AcqPlan(wl.groups, cfs)
+    cells = plan.cells
+    st = torch.cuda.current_stream()
+    bufs_d = [torch.from_numpy(b).cuda() for b in wl.bufs]
+    lens = [len(b) for b in wl.bufs]
+    res_d = torch.empty(plan.n_res * acquire.RESULT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+
+    def step():
+        plan.run_device([b.data_ptr() for b in bufs_d], lens, wl.ix, res_d.data_ptr(), st.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    plan.profile(True)
+    plan.profile_get()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    clk = ClockSampler(local)
+    clk.start()
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        flush.fill_(k & 0xFF)
+        ev[k][0].record(st)
+        step()
+        ev[k][1].record(st)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    if dist:
+        dist.barrier()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    prof = plan.profile_get()
+    plan.profile(False)
+    total_ms = sum(step_ms)
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = cells * args.steps * world / (total_ms / 1e3)
+
+    # ---- end to end through the public API: host IF -> device -> results -> host
+    bufs_h = [torch.from_numpy(b).pin_memory() for b in wl.bufs]
+    res_h = torch.empty(res_d.numel(), dtype=torch.uint8).pin_memory()
+    h2d = sum(b.numel() for b in bufs_h)
+    d2h = res_h.numel()
+
+    def e2e_step():
+        for bh, bd in zip(bufs_h, bufs_d):
+            bd.copy_(bh, non_blocking=True)
+        step()
+        res_h.copy_(res_d, non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.fill_((k + 1) & 0xFF)
+        e2e_ev[k][0].record(st)
+        e2e_step()
+        e2e_ev[k][1].record(st)
+    torch.cuda.synchronize()
+    e2e_ms = sum(a.elapsed_time(b) for a, b in e2e_ev)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = cells * args.steps * world / (e2e_ms / 1e3)
+    res = np.frombuffer(res_h.numpy().tobytes(), dtype=acquire.RESULT_DTYPE)
+
+    # ---- roofline of the dominant kernel (consumer: code product + inverse FFT + power)
+    cons_ms, cons_n = prof["cons"]
+    flops_step = cons_flops(wl.groups)
+    achieved = flops_step * args.steps / (cons_ms / 1e3) / 1e12 if cons_ms > 0 else None
+    hbm_b = cons_hbm_bytes(wl.groups)
+    traffic = load_traffic().get(args.workload)
+    n_groups = len(wl.groups)
+    roofline = {
+        "kernel": "cons_kernel (code product + inverse FFT + |y|^2 accumulate)",
+        "bound": "fp32", "achieved": achieved, "peak": FP32_NOMINAL_TFLOPS, "unit": "TFLOP/s",
+        "frac": achieved / FP32_NOMINAL_TFLOPS if achieved else None,
+        "peak_source": "nominal FP32 FMA rate at max clock (148 SM x 128 lanes x 2 x 1965 MHz); "
+                       "MEASURED_PEAKS.json has no FP32 CUDA-core figure",
+        "flops_per_step": flops_step,
+        "traffic": traffic,
+        "avg_launch_ms": cons_ms / cons_n if cons_n else None,
+        "launches": cons_n,
+        "share_of_step": cons_ms / sum(step_ms) if sum(step_ms) else None,
+        "hbm": {"algorithmic_bytes_per_step": hbm_b,
+                "achieved_gbs": hbm_b * args.steps / (cons_ms / 1e3) / 1e9 if cons_ms else None,
+                "peak_gbs": _measured_hbm(), "frac": None},
+    }
+    if roofline["hbm"]["achieved_gbs"] and roofline["hbm"]["peak_gbs"]:
+        roofline["hbm"]["frac"] = roofline["hbm"]["achieved_gbs"] / roofline["hbm"]["peak_gbs"]
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "cells_per_step": cells,
+                       "groups": [f"{g.sig}:{len(g.prns)}prn x {len(g.fds)}bin x {g.Nmax}off x "
+                                  f"{g.n_sum}sum L={g.L}" for g in wl.groups],
+                       "l2": "flushed between timed steps (512 MB write outside the events)",
+                       "parallelism": f"replica x{world} (one IF block per rank)"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": sum(n for _, n in prof.values()),
+            "kernel_ms": {k: v[0] / max(v[1], 1) for k, v in prof.items()},
+            "roofline": roofline, "clocks": clocks,
+            "detected": int(sum(1 for r in res if r["cn0"] >= 38.0))}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, cores, kind, desc = cpu_reference_rate(wl)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
+                                "sample": desc}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def _measured_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        return 6650.0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

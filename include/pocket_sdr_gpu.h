@@ -1,0 +1,214 @@
+/*
+ * pocket_sdr_gpu.h - B200 (sm_100a) implementation of Pocket SDR's
+ * signal-search and correlation hot path behind a C ABI.
+ *
+ * Part 1 ("drop-in") declares the reference's own entry points with the same
+ * names, argument types and meaning (Pocket SDR src/pocket_sdr.h), so a C
+ * program or the python/sdr_func.py ctypes layer can bind this library in
+ * place of the reference's src/sdr_func.c for these functions. All buffers are
+ * caller-owned HOST memory, exactly as in the reference; each call copies its
+ * window to the GPU, runs the kernels and copies the result back.
+ *
+ * Part 2 ("batched", prefix sdrg_) is additive: device-resident IF buffers,
+ * many signals x PRNs x Doppler bins x non-coherent sums in one launch
+ * sequence, device pointers, an explicit stream, and an int status.
+ *
+ * Errors: the reference functions return void and exit(-1) on allocation
+ * failure (src/sdr_func.c:150-153). Here nothing exits: a failing call leaves
+ * its outputs zero-filled (P is left unchanged), prints one line to stderr
+ * and records a message readable with sdr_gpu_last_error() on the calling
+ * thread.
+ *
+ * Threading: every entry point may be called concurrently from several host
+ * threads (the reference calls them from one thread per receiver channel,
+ * src/sdr_rcv.c:495-520); each host thread gets its own CUDA stream and
+ * staging buffers.
+ */
+#ifndef POCKET_SDR_GPU_H
+#define POCKET_SDR_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- types: same layout as src/pocket_sdr.h:105-113 and :242-245 -------- */
+#ifndef POCKET_SDR_H
+typedef uint8_t sdr_cpx8_t;                 /* 4+4-bit I/Q, I in low nibble */
+typedef struct { int8_t I, Q; } sdr_cpx16_t; /* mixed sample */
+typedef float sdr_cpx_t[2];                  /* single precision complex */
+typedef struct {                             /* IF data buffer */
+    sdr_cpx8_t *data;
+    int IQ, N;
+} sdr_buff_t;
+#define SDR_N_CODES  10                      /* src/pocket_sdr.h:60 */
+#define SDR_MAX_CORR 107                     /* src/pocket_sdr.h:58 */
+#endif
+
+/* =========================================================================
+ * Part 1: drop-in entry points (same signatures as the reference)
+ * ========================================================================= */
+
+/* Replaces src/sdr_func.c:113-134 (sdr_func_init, src/pocket_sdr.h:392).
+ * Initialises the GPU context and the quantised carrier table. `file` (an FFT
+ * wisdom path in the reference) is accepted and ignored. May be called more
+ * than once. */
+void sdr_func_init(const char *file);
+
+/* Replaces src/sdr_func.c:824-836 (sdr_mix_carr, src/pocket_sdr.h:429).
+ * Bit-exact carrier wipe-off, including the circular-buffer wrap. */
+void sdr_mix_carr(const sdr_buff_t *buff, int ix, int N, double fs, double fc,
+    double phi, sdr_cpx16_t *IQ);
+
+/* Replaces src/sdr_func.c:981-1008 (sdr_corr_std, src/pocket_sdr.h:415).
+ * Bit-exact integer correlation and FP32 scaling. `code` is the
+ * SDR_N_CODES x N bank. */
+void sdr_corr_std(const sdr_cpx16_t *IQ, const sdr_cpx16_t *code, int N,
+    double coff, const double *pos, int n, sdr_cpx_t *corr, sdr_cpx_t *C);
+
+/* Replaces src/sdr_func.c:1029-1057 (sdr_corr_std_cpx_code,
+ * src/pocket_sdr.h:417). Complex-code (E5 AltBOC) correlator. */
+void sdr_corr_std_cpx_code(const sdr_cpx16_t *IQ, const sdr_cpx16_t *code,
+    int N, double coff, const double *pos, int n, sdr_cpx_t *corr,
+    sdr_cpx_t *C);
+
+/* Replaces src/sdr_func.c:1060-1072 (sdr_corr_std_cpx, src/pocket_sdr.h:420),
+ * the python/sdr_func.py corr_std() binding (python/sdr_func.py:156-171). */
+void sdr_corr_std_cpx(const sdr_cpx_t *buff, int len_buff, int ix, int N,
+    double fs, double fc, double phi, const float *code, const double *pos,
+    int n, sdr_cpx_t *corr);
+
+/* Replaces src/sdr_func.c:1088-1102 (sdr_corr_fft, src/pocket_sdr.h:423).
+ * corr = IFFT(FFT(IQ * CSCALE) * code_fft / N^2), FP32, any N whose FFT plan
+ * is supported (see sdrg_fft_supported). */
+void sdr_corr_fft(const sdr_cpx16_t *IQ, const sdr_cpx_t *code_fft, int N,
+    sdr_cpx_t *corr);
+
+/* Replaces src/sdr_func.c:1105-1113 (sdr_corr_fft_cpx, src/pocket_sdr.h:425),
+ * the python/sdr_func.py corr_fft() binding (python/sdr_func.py:174-183). */
+void sdr_corr_fft_cpx(const sdr_cpx_t *buff, int len_buff, int ix, int N,
+    double fs, double fc, double phi, const sdr_cpx_t *code_fft,
+    sdr_cpx_t *corr);
+
+/* Replaces src/sdr_func.c:664-687 (sdr_search_code, src/pocket_sdr.h:404).
+ * P[i*N+j] += |corr_i[j]|^2 for every Doppler bin i (P is read, accumulated
+ * and written back). T is unused, as in the reference. The reference's 1 ms
+ * CPU-release sleep every 22 bins is not reproduced. */
+void sdr_search_code(const sdr_cpx_t *code_fft, double T,
+    const sdr_buff_t *buff, int ix, int N, double fs, double fi,
+    const float *fds, int len_fds, float *P);
+
+/* Replaces src/sdr_func.c:690-706 (sdr_corr_max, src/pocket_sdr.h:407).
+ * First strict maximum in row-major order and C/N0 from the grid mean. */
+float sdr_corr_max(const float *P, int N, int Nmax, int M, double T, int *ix);
+
+/* Replaces src/sdr_func.c:709-744 (sdr_fine_dop, src/pocket_sdr.h:408).
+ * Vertex of the parabola through the peak bin and its two neighbours. */
+double sdr_fine_dop(const float *P, int N, const float *fds, int len_fds,
+    const int *ix);
+
+/* Replaces src/sdr_func.c:757-769 (sdr_dop_bins, src/pocket_sdr.h:411).
+ * Returns a malloc'ed array; release it with free() (the reference's
+ * sdr_free is free()). */
+float *sdr_dop_bins(double T, float dop, float max_dop, int *len_fds);
+
+/* =========================================================================
+ * Part 2: additive entry points (no reference counterpart)
+ * ========================================================================= */
+
+#define SDRG_OK          0
+#define SDRG_ERR_ARG    -1   /* invalid argument / unsupported size */
+#define SDRG_ERR_CUDA   -2   /* CUDA runtime or launch error */
+#define SDRG_ERR_NOMEM  -3   /* device or pinned allocation failed */
+#define SDRG_ERR_NODEV  -4   /* no usable CUDA device */
+
+/* Message of the last failed call on this host thread ("" if none); copies
+ * at most size-1 bytes into buff and returns the last status code. */
+int sdr_gpu_last_error(char *buff, int size);
+
+/* Clears the calling thread's error state. */
+void sdr_gpu_clear_error(void);
+
+/* Selects and initialises a device (default: device 0, or $SDRG_DEVICE).
+ * Optional; every entry point initialises lazily. */
+int sdrg_init(int device);
+
+/* 1 when an FFT of length N has a GPU plan (N = R*M with R in
+ * {1,2,3,4,5,6,8}, M 2-3-5-smooth and small enough for one CTA), else 0. */
+int sdrg_fft_supported(int N);
+
+/* Library version string. */
+const char *sdrg_version(void);
+
+/* ---- batched parallel-code-phase acquisition ----------------------------
+ * One signal group = one code family at one sampling setup: all its PRNs
+ * share L, fs, fi, Doppler bins and sums, so the forward FFT of every
+ * (Doppler bin, sum) is computed once and reused by every PRN. */
+typedef struct {
+    int L;                 /* FFT length (samples mixed per coherent block) */
+    int N;                 /* sample advance between non-coherent sums */
+    int Nmax;              /* code offsets kept per Doppler bin (grid cols) */
+    int n_sum;             /* non-coherent sums */
+    int n_prn;             /* PRNs (code FFTs) in this group */
+    int len_fds;           /* Doppler bins */
+    double fs, fi, T;      /* sampling rate, IF (Hz), coherent time (s) */
+    const float *fds;      /* [len_fds] Doppler bins (Hz), HOST */
+    const sdr_cpx_t *code_fft; /* [n_prn][L] conjugated code DFTs, HOST */
+    int buf;               /* index of the IF buffer this group reads */
+} sdrg_acq_sig_t;
+
+/* Per (group, PRN) result of one sdrg_acq_run. */
+typedef struct {
+    int bin, offset;       /* peak Doppler bin and code offset (samples) */
+    float cn0;             /* C/N0 (dB-Hz), as sdr_corr_max */
+    float pmax;            /* peak power */
+    double pave;           /* grid mean power */
+    double fd;             /* fine Doppler (Hz), as sdr_fine_dop */
+} sdrg_acq_result_t;
+
+typedef struct sdrg_acq_plan sdrg_acq_plan_t;
+
+/* Builds a plan: uploads the code FFTs (permuted for the kernels), FFT
+ * tables, Doppler phase steps and allocates the grid and work buffers.
+ * Returns NULL on error (see sdr_gpu_last_error). */
+sdrg_acq_plan_t *sdrg_acq_plan_new(const sdrg_acq_sig_t *sigs, int n_sig);
+void sdrg_acq_plan_free(sdrg_acq_plan_t *plan);
+
+/* Total grid cells (sum over groups of n_prn * len_fds * Nmax). */
+int64_t sdrg_acq_plan_cells(const sdrg_acq_plan_t *plan);
+
+/* Runs the whole search on `stream` (a cudaStream_t, NULL = the calling
+ * thread's stream). if_dev[b] is a DEVICE pointer to packed IF buffer b of
+ * len_if[b] samples (circular); ix[b] is the first sample of sum 0. Results
+ * for group g, PRN p are written to res_dev[offset_g + p] (DEVICE pointer;
+ * offset_g = sum of n_prn of the groups before g). Asynchronous. */
+int sdrg_acq_run(sdrg_acq_plan_t *plan, const uint8_t *const *if_dev,
+    const int *len_if, const int *ix, sdrg_acq_result_t *res_dev,
+    void *stream);
+
+/* Device pointer to the accumulated grid of group g, laid out
+ * [n_prn][len_fds][Nmax] (float), valid after sdrg_acq_run completes. */
+const float *sdrg_acq_grid(const sdrg_acq_plan_t *plan, int g);
+
+/* Copies the grid of group g to HOST memory dst (n_prn*len_fds*Nmax floats),
+ * after the plan's last run on its stream has completed (synchronous). */
+int sdrg_acq_grid_host(const sdrg_acq_plan_t *plan, int g, float *dst);
+
+/* Kernel timing: when enabled, every sdrg_acq_run records CUDA events on its
+ * stream around each kernel launch. sdrg_acq_profile_get waits for them and
+ * returns, since the last get, the summed milliseconds and launch counts of
+ * the forward-FFT [0], consumer (code multiply + inverse FFT + power) [1] and
+ * peak-reduction [2] kernels, then resets. */
+int sdrg_acq_profile(sdrg_acq_plan_t *plan, int enable);
+int sdrg_acq_profile_get(sdrg_acq_plan_t *plan, double *ms, int64_t *launches);
+
+/* Host convenience: copies IF buffers to the device, runs, and copies the
+ * n_prn-total results back (synchronous). if_host[b] are HOST pointers. */
+int sdrg_acq_run_host(sdrg_acq_plan_t *plan, const uint8_t *const *if_host,
+    const int *len_if, const int *ix, sdrg_acq_result_t *res_host);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* POCKET_SDR_GPU_H */

@@ -1,0 +1,334 @@
+"""Test-only CPU oracle for Pocket SDR's search / correlation hot path.
+
+Two checkers live here, both test infrastructure (used by tests/, the smoke
+check and the CPU-baseline leg of bench.py; never by the product path):
+
+* ``Restatement`` - ctypes wrapper over ``_build/liboracle.so``, the plain C
+  restatement in ``sdr_oracle.c`` (each function cites the reference lines it
+  follows).
+* ``Reference`` - ctypes wrapper over ``_ref/libsdr_ref.so``, the reference's
+  own ``src/sdr_func.c`` + ``src/sdr_code.c`` compiled from source by
+  ``oracle/Makefile`` with the reference's flags. Present wherever ``make ref``
+  ran (the .so travels with the repository snapshot).
+
+Both expose the same numpy-level API:
+  mix_carr(buff_u8, ix, N, fs, fc, phi) -> int8[N, 2]
+  corr_std(IQ_i8[N,2], code_i8[10*N,2], coff, pos, cpx_code) -> (corr c64[n], C c64[2])
+  corr_fft(IQ_i8[N,2], code_fft_c64[N]) -> c64[N]
+  search_code(code_fft_c64[N], buff_u8, ix, N, fs, fi, fds, P_f32[len_fds,N]) (in/out)
+  corr_max(P, N, Nmax, M, T) -> (cn0, (bin, offset))
+  fine_dop(P, N, fds, ix) -> float
+  dop_bins(T, dop, max_dop) -> f32[]
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_SO = os.path.join(HERE, "_ref", "libsdr_ref.so")
+ORC_SO = os.path.join(HERE, "_build", "liboracle.so")
+
+_p = C.c_void_p
+_i = C.c_int
+_d = C.c_double
+_f = C.c_float
+
+
+def build(ref: bool = True) -> None:
+    """Compile the restatement, and the reference library when its sources
+    are present on this machine."""
+    targets = ["oracle"]
+    if ref and os.path.isdir(os.environ.get("POCKETSDR_REF", "/root/reference") + "/src"):
+        targets.append("ref")
+    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_p)
+
+
+class _SdrBuff(C.Structure):
+    # sdr_buff_t layout (src/pocket_sdr.h:242-245)
+    _fields_ = [("data", C.POINTER(C.c_uint8)), ("IQ", C.c_int), ("N", C.c_int)]
+
+
+class Restatement:
+    """The oracle's own C restatement (oracle/sdr_oracle.c)."""
+
+    kind = "port"
+
+    def __init__(self, path: str = ORC_SO):
+        if not os.path.exists(path):
+            build(ref=False)
+        L = self.lib = C.CDLL(path)
+        L.orc_init.argtypes = []
+        L.orc_mix_table.restype = C.POINTER(C.c_int8)
+        L.orc_mix_carr.argtypes = [_p, _i, _i, _i, _d, _d, _d, _p]
+        L.orc_mix_carr_cpx.argtypes = [_p, _i, _i, _i, _d, _d, _d, _p]
+        L.orc_corr_std.argtypes = [_p, _p, _i, _d, _p, _i, _i, _p, _p]
+        L.orc_corr_std_cpx.argtypes = [_p, _i, _i, _i, _d, _d, _d, _p, _p, _i, _p]
+        L.orc_fft.argtypes = [_p, _i, _i, _p]
+        L.orc_corr_fft.argtypes = [_p, _p, _i, _p]
+        L.orc_corr_fft_cpx.argtypes = [_p, _i, _i, _i, _d, _d, _d, _p, _p]
+        L.orc_search_code.argtypes = [_p, _p, _i, _i, _i, _d, _d, _p, _i, _p]
+        L.orc_corr_max.argtypes = [_p, _i, _i, _i, _d, _p]
+        L.orc_corr_max.restype = _f
+        L.orc_fine_dop.argtypes = [_p, _i, _p, _i, _p]
+        L.orc_fine_dop.restype = _d
+        L.orc_dop_bins.argtypes = [_d, _f, _f, _p]
+        L.orc_res_code.argtypes = [_p, _p, _i, _d, _d, _d, _i, _i, _p]
+        L.orc_gen_code_fft.argtypes = [_p, _p, _i, _d, _d, _d, _i, _i, _p]
+        L.orc_init()
+
+    def mix_table(self) -> np.ndarray:
+        t = self.lib.orc_mix_table()
+        return np.ctypeslib.as_array(t, shape=(65536, 2)).copy()
+
+    def mix_carr(self, buff, ix, N, fs, fc, phi):
+        buff = np.ascontiguousarray(buff, np.uint8)
+        out = np.zeros((N, 2), np.int8)
+        self.lib.orc_mix_carr(_ptr(buff), len(buff), ix, N, fs, fc, phi, _ptr(out))
+        return out
+
+    def mix_carr_cpx(self, buff, ix, N, fs, fc, phi):
+        buff = np.ascontiguousarray(buff, np.complex64)
+        out = np.zeros((N, 2), np.int8)
+        self.lib.orc_mix_carr_cpx(_ptr(buff), len(buff), ix, N, fs, fc, phi, _ptr(out))
+        return out
+
+    def corr_std(self, IQ, code, coff, pos, cpx_code=False):
+        IQ = np.ascontiguousarray(IQ, np.int8)
+        code = np.ascontiguousarray(code, np.int8)
+        pos = np.ascontiguousarray(pos, np.float64)
+        N = IQ.shape[0]
+        corr = np.zeros(len(pos), np.complex64)
+        Cb = np.zeros(2, np.complex64)
+        self.lib.orc_corr_std(_ptr(IQ), _ptr(code), N, coff, _ptr(pos), len(pos),
+                              int(cpx_code), _ptr(corr), _ptr(Cb))
+        return corr, Cb
+
+    def corr_std_cpx(self, buff, ix, N, fs, fc, phi, code, pos):
+        buff = np.ascontiguousarray(buff, np.complex64)
+        code = np.ascontiguousarray(code, np.float32)
+        pos = np.ascontiguousarray(pos, np.float64)
+        corr = np.zeros(len(pos), np.complex64)
+        self.lib.orc_corr_std_cpx(_ptr(buff), len(buff), ix, N, fs, fc, phi,
+                                  _ptr(code), _ptr(pos), len(pos), _ptr(corr))
+        return corr
+
+    def fft(self, x, inverse=False):
+        x = np.ascontiguousarray(x, np.complex128)
+        out = np.zeros_like(x)
+        self.lib.orc_fft(_ptr(x), len(x), int(inverse), _ptr(out))
+        return out
+
+    def corr_fft(self, IQ, code_fft):
+        IQ = np.ascontiguousarray(IQ, np.int8)
+        code_fft = np.ascontiguousarray(code_fft, np.complex64)
+        out = np.zeros(IQ.shape[0], np.complex64)
+        self.lib.orc_corr_fft(_ptr(IQ), _ptr(code_fft), IQ.shape[0], _ptr(out))
+        return out
+
+    def corr_fft_cpx(self, buff, ix, N, fs, fc, phi, code_fft):
+        buff = np.ascontiguousarray(buff, np.complex64)
+        code_fft = np.ascontiguousarray(code_fft, np.complex64)
+        out = np.zeros(N, np.complex64)
+        self.lib.orc_corr_fft_cpx(_ptr(buff), len(buff), ix, N, fs, fc, phi,
+                                  _ptr(code_fft), _ptr(out))
+        return out
+
+    def search_code(self, code_fft, buff, ix, N, fs, fi, fds, P):
+        code_fft = np.ascontiguousarray(code_fft, np.complex64)
+        buff = np.ascontiguousarray(buff, np.uint8)
+        fds = np.ascontiguousarray(fds, np.float32)
+        assert P.dtype == np.float32 and P.flags.c_contiguous
+        self.lib.orc_search_code(_ptr(code_fft), _ptr(buff), len(buff), ix, N, fs, fi,
+                                 _ptr(fds), len(fds), _ptr(P))
+        return P
+
+    def corr_max(self, P, N, Nmax, M, T):
+        P = np.ascontiguousarray(P, np.float32)
+        ix = np.zeros(2, np.int32)
+        cn0 = self.lib.orc_corr_max(_ptr(P), N, Nmax, M, T, _ptr(ix))
+        return float(cn0), (int(ix[0]), int(ix[1]))
+
+    def fine_dop(self, P, N, fds, ix):
+        P = np.ascontiguousarray(P, np.float32)
+        fds = np.ascontiguousarray(fds, np.float32)
+        ixa = np.asarray(ix, np.int32)
+        return float(self.lib.orc_fine_dop(_ptr(P), N, _ptr(fds), len(fds), _ptr(ixa)))
+
+    def dop_bins(self, T, dop, max_dop):
+        n = self.lib.orc_dop_bins(T, dop, max_dop, None)
+        out = np.zeros(n, np.float32)
+        self.lib.orc_dop_bins(T, dop, max_dop, _ptr(out))
+        return out
+
+    def res_code(self, code_I, code_Q, T, coff, fs, N, Nz):
+        code_I = np.ascontiguousarray(code_I, np.int8)
+        cq = None if code_Q is None else np.ascontiguousarray(code_Q, np.int8)
+        out = np.zeros((N + Nz, 2), np.int8)
+        self.lib.orc_res_code(_ptr(code_I), None if cq is None else _ptr(cq), len(code_I),
+                              T, coff, fs, N, Nz, _ptr(out))
+        return out
+
+    def gen_code_fft(self, code_I, code_Q, T, coff, fs, N, Nz):
+        code_I = np.ascontiguousarray(code_I, np.int8)
+        cq = None if code_Q is None else np.ascontiguousarray(code_Q, np.int8)
+        out = np.zeros(N + Nz, np.complex64)
+        self.lib.orc_gen_code_fft(_ptr(code_I), None if cq is None else _ptr(cq),
+                                  len(code_I), T, coff, fs, N, Nz, _ptr(out))
+        return out
+
+
+class Reference:
+    """The reference's own C functions, compiled from its sources."""
+
+    kind = "reference"
+
+    def __init__(self, path: str = REF_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        L = self.lib = C.CDLL(path)
+        L.sdr_func_init.argtypes = [C.c_char_p]
+        L.sdr_mix_carr.argtypes = [C.POINTER(_SdrBuff), _i, _i, _d, _d, _d, _p]
+        L.sdr_corr_std.argtypes = [_p, _p, _i, _d, _p, _i, _p, _p]
+        L.sdr_corr_std_cpx_code.argtypes = [_p, _p, _i, _d, _p, _i, _p, _p]
+        L.sdr_corr_std_cpx.argtypes = [_p, _i, _i, _i, _d, _d, _d, _p, _p, _i, _p]
+        L.sdr_corr_fft.argtypes = [_p, _p, _i, _p]
+        L.sdr_corr_fft_cpx.argtypes = [_p, _i, _i, _i, _d, _d, _d, _p, _p]
+        L.sdr_search_code.argtypes = [_p, _d, C.POINTER(_SdrBuff), _i, _i, _d, _d, _p, _i, _p]
+        L.sdr_corr_max.argtypes = [_p, _i, _i, _i, _d, _p]
+        L.sdr_corr_max.restype = _f
+        L.sdr_fine_dop.argtypes = [_p, _i, _p, _i, _p]
+        L.sdr_fine_dop.restype = _d
+        L.sdr_dop_bins.argtypes = [_d, _f, _f, C.POINTER(_i)]
+        L.sdr_dop_bins.restype = C.POINTER(_f)
+        L.sdr_gen_code.argtypes = [C.c_char_p, _i, C.POINTER(_i)]
+        L.sdr_gen_code.restype = C.POINTER(C.c_int8)
+        L.sdr_code_cyc.argtypes = [C.c_char_p]
+        L.sdr_code_cyc.restype = _d
+        L.sdr_res_code.argtypes = [_p, _p, _i, _d, _d, _d, _i, _i, _p]
+        L.sdr_gen_code_fft.argtypes = [_p, _p, _i, _d, _d, _d, _i, _i, _p]
+        L.sdr_cpx_fft.argtypes = [_p, _i, _i, _p]
+        L.sdr_cpx_fft.restype = _i
+        L.sdr_free.argtypes = [_p]
+        L.sdr_func_init(b"")
+
+    def _buff(self, buff):
+        b = np.ascontiguousarray(buff, np.uint8)
+        sb = _SdrBuff(b.ctypes.data_as(C.POINTER(C.c_uint8)), 2, len(b))
+        return b, sb
+
+    def mix_carr(self, buff, ix, N, fs, fc, phi):
+        b, sb = self._buff(buff)
+        out = np.zeros((N, 2), np.int8)
+        self.lib.sdr_mix_carr(C.byref(sb), ix, N, fs, fc, phi, _ptr(out))
+        return out
+
+    def corr_std(self, IQ, code, coff, pos, cpx_code=False):
+        IQ = np.ascontiguousarray(IQ, np.int8)
+        code = np.ascontiguousarray(code, np.int8)
+        pos = np.ascontiguousarray(pos, np.float64)
+        corr = np.zeros(len(pos), np.complex64)
+        Cb = np.zeros(2, np.complex64)
+        fn = self.lib.sdr_corr_std_cpx_code if cpx_code else self.lib.sdr_corr_std
+        fn(_ptr(IQ), _ptr(code), IQ.shape[0], coff, _ptr(pos), len(pos), _ptr(corr), _ptr(Cb))
+        return corr, Cb
+
+    def corr_std_cpx(self, buff, ix, N, fs, fc, phi, code, pos):
+        buff = np.ascontiguousarray(buff, np.complex64)
+        code = np.ascontiguousarray(code, np.float32)
+        pos = np.ascontiguousarray(pos, np.float64)
+        corr = np.zeros(len(pos), np.complex64)
+        self.lib.sdr_corr_std_cpx(_ptr(buff), len(buff), ix, N, fs, fc, phi,
+                                  _ptr(code), _ptr(pos), len(pos), _ptr(corr))
+        return corr
+
+    def fft(self, x, inverse=False):
+        x = np.ascontiguousarray(x, np.complex64)
+        out = np.zeros_like(x)
+        self.lib.sdr_cpx_fft(_ptr(x), len(x), int(inverse), _ptr(out))
+        return out
+
+    def corr_fft(self, IQ, code_fft):
+        IQ = np.ascontiguousarray(IQ, np.int8)
+        code_fft = np.ascontiguousarray(code_fft, np.complex64)
+        out = np.zeros(IQ.shape[0], np.complex64)
+        self.lib.sdr_corr_fft(_ptr(IQ), _ptr(code_fft), IQ.shape[0], _ptr(out))
+        return out
+
+    def corr_fft_cpx(self, buff, ix, N, fs, fc, phi, code_fft):
+        buff = np.ascontiguousarray(buff, np.complex64)
+        code_fft = np.ascontiguousarray(code_fft, np.complex64)
+        out = np.zeros(N, np.complex64)
+        self.lib.sdr_corr_fft_cpx(_ptr(buff), len(buff), ix, N, fs, fc, phi,
+                                  _ptr(code_fft), _ptr(out))
+        return out
+
+    def search_code(self, code_fft, buff, ix, N, fs, fi, fds, P, T=1e-3):
+        code_fft = np.ascontiguousarray(code_fft, np.complex64)
+        b, sb = self._buff(buff)
+        fds = np.ascontiguousarray(fds, np.float32)
+        assert P.dtype == np.float32 and P.flags.c_contiguous
+        self.lib.sdr_search_code(_ptr(code_fft), T, C.byref(sb), ix, N, fs, fi,
+                                 _ptr(fds), len(fds), _ptr(P))
+        return P
+
+    def corr_max(self, P, N, Nmax, M, T):
+        P = np.ascontiguousarray(P, np.float32)
+        ix = np.zeros(2, np.int32)
+        cn0 = self.lib.sdr_corr_max(_ptr(P), N, Nmax, M, T, _ptr(ix))
+        return float(cn0), (int(ix[0]), int(ix[1]))
+
+    def fine_dop(self, P, N, fds, ix):
+        P = np.ascontiguousarray(P, np.float32)
+        fds = np.ascontiguousarray(fds, np.float32)
+        ixa = np.asarray(ix, np.int32)
+        return float(self.lib.sdr_fine_dop(_ptr(P), N, _ptr(fds), len(fds), _ptr(ixa)))
+
+    def dop_bins(self, T, dop, max_dop):
+        n = _i(0)
+        p = self.lib.sdr_dop_bins(T, dop, max_dop, C.byref(n))
+        out = np.ctypeslib.as_array(p, shape=(n.value,)).copy()
+        self.lib.sdr_free(C.cast(p, _p))
+        return out
+
+    def gen_code(self, sig: str, prn: int) -> np.ndarray:
+        n = _i(0)
+        p = self.lib.sdr_gen_code(sig.encode(), prn, C.byref(n))
+        if not p:
+            raise ValueError(f"no code for {sig} {prn}")
+        return np.ctypeslib.as_array(p, shape=(n.value,)).copy()
+
+    def code_cyc(self, sig: str) -> float:
+        return float(self.lib.sdr_code_cyc(sig.encode()))
+
+    def res_code(self, code_I, code_Q, T, coff, fs, N, Nz):
+        code_I = np.ascontiguousarray(code_I, np.int8)
+        cq = None if code_Q is None else np.ascontiguousarray(code_Q, np.int8)
+        out = np.zeros((N + Nz, 2), np.int8)
+        self.lib.sdr_res_code(_ptr(code_I), None if cq is None else _ptr(cq), len(code_I),
+                              T, coff, fs, N, Nz, _ptr(out))
+        return out
+
+    def gen_code_fft(self, code_I, code_Q, T, coff, fs, N, Nz):
+        code_I = np.ascontiguousarray(code_I, np.int8)
+        cq = None if code_Q is None else np.ascontiguousarray(code_Q, np.int8)
+        out = np.zeros(N + Nz, np.complex64)
+        self.lib.sdr_gen_code_fft(_ptr(code_I), None if cq is None else _ptr(cq),
+                                  len(code_I), T, coff, fs, N, Nz, _ptr(out))
+        return out
+
+
+def reference_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def best():
+    """The reference build when present, else the restatement."""
+    return Reference() if reference_available() else Restatement()

@@ -1,0 +1,95 @@
+/*
+ * sdr_oracle.h - CPU restatement of Pocket SDR's signal-search / correlation
+ * hot path, used ONLY as a test checker (tests/, __graft_entry__.smoke() and
+ * bench.py's CPU-baseline leg). The product library never links this code.
+ *
+ * Every function states the reference lines it restates
+ * (paths relative to the Pocket SDR source tree).
+ *
+ * Types are plain C arrays so the file builds without the reference headers:
+ *   packed IF sample  : uint8_t, I in low nibble, Q in high nibble
+ *   mixed sample      : int8_t[2] (I, Q)
+ *   complex float     : float[2]
+ */
+#ifndef SDR_ORACLE_H
+#define SDR_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ORC_N_CODES 10     /* code banks per code (src/pocket_sdr.h:60) */
+#define ORC_MAX_CORR 107   /* max correlators (src/pocket_sdr.h:58) */
+
+/* Build the 256-entry carrier table and the 64K mixed-sample table
+ * (src/sdr_func.c:113-134). Idempotent. */
+void orc_init(void);
+
+/* Raw access to the 64K x (I,Q) table, for table-equivalence tests. */
+const int8_t *orc_mix_table(void);
+
+/* Carrier wipe-off over a circular buffer (src/sdr_func.c:772-836). */
+void orc_mix_carr(const uint8_t *buff, int len_buff, int ix, int N, double fs,
+                  double fc, double phi, int8_t *IQ);
+
+/* Float buffer -> packed 4+4 -> mix (src/sdr_func.c:839-848). */
+void orc_mix_carr_cpx(const float *buff, int len_buff, int ix, int N,
+                      double fs, double fc, double phi, int8_t *IQ);
+
+/* Standard correlator (src/sdr_func.c:981-1008) and its complex-code form
+ * (src/sdr_func.c:1029-1057). cpx_code selects the latter. */
+void orc_corr_std(const int8_t *IQ, const int8_t *code, int N, double coff,
+                  const double *pos, int n, int cpx_code, float *corr,
+                  float *C);
+
+/* Python-facing mix + correlate (src/sdr_func.c:1060-1072). */
+void orc_corr_std_cpx(const float *buff, int len_buff, int ix, int N,
+                      double fs, double fc, double phi, const float *code,
+                      const double *pos, int n, float *corr);
+
+/* In-place-free complex FFT in double precision, any length (mixed radix with
+ * a direct DFT for prime factors). dir = 0 forward (exp(-i)), 1 backward
+ * (exp(+i)), unnormalised, as the reference's FFT shim
+ * (lib/pocketfft/pocketfft_wrap.cpp, src/sdr_func.c:236-264). */
+void orc_fft(const double *in, int N, int dir, double *out);
+
+/* FFT correlator (src/sdr_func.c:1088-1102), FFT in double. */
+void orc_corr_fft(const int8_t *IQ, const float *code_fft, int N, float *corr);
+
+/* Python-facing mix + FFT correlate (src/sdr_func.c:1105-1113). */
+void orc_corr_fft_cpx(const float *buff, int len_buff, int ix, int N,
+                      double fs, double fc, double phi, const float *code_fft,
+                      float *corr);
+
+/* Parallel code phase search, accumulating into P (src/sdr_func.c:664-687),
+ * without the reference's 1 ms CPU-release sleep. */
+void orc_search_code(const float *code_fft, const uint8_t *buff, int len_buff,
+                     int ix, int N, double fs, double fi, const float *fds,
+                     int len_fds, float *P);
+
+/* Peak and C/N0 (src/sdr_func.c:690-706). */
+float orc_corr_max(const float *P, int N, int Nmax, int M, double T, int *ix);
+
+/* Fine Doppler by a 3-point quadratic (src/sdr_func.c:709-744). */
+double orc_fine_dop(const float *P, int N, const float *fds, int len_fds,
+                    const int *ix);
+
+/* Doppler bins (src/sdr_func.c:757-769); returns the count, fills fds when
+ * non-NULL. */
+int orc_dop_bins(double T, float dop, float max_dop, float *fds);
+
+/* Nearest-chip resampling (src/sdr_code.c:2556-2568); code_Q may be NULL. */
+void orc_res_code(const int8_t *code_I, const int8_t *code_Q, int len_code,
+                  double T, double coff, double fs, int N, int Nz,
+                  int8_t *code_res);
+
+/* Conjugated code DFT (src/sdr_code.c:2589-2608), FFT in double. */
+void orc_gen_code_fft(const int8_t *code_I, const int8_t *code_Q,
+                      int len_code, double T, double coff, double fs, int N,
+                      int Nz, float *code_fft);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,105 @@
+"""ctypes binding of libsdr_gpu.so (the C ABI declared in include/pocket_sdr_gpu.h).
+
+The library is required: importing this module without the built .so raises
+ImportError (build it with ``python -m pocketsdr_b200.build``). There is no
+CPU fallback anywhere in the package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libsdr_gpu.so")
+
+_p = C.c_void_p
+_i = C.c_int
+_d = C.c_double
+_f = C.c_float
+
+
+class SdrBuff(C.Structure):
+    """sdr_buff_t (src/pocket_sdr.h:242-245)."""
+    _fields_ = [("data", C.POINTER(C.c_uint8)), ("IQ", C.c_int), ("N", C.c_int)]
+
+
+class AcqSig(C.Structure):
+    """sdrg_acq_sig_t."""
+    _fields_ = [("L", _i), ("N", _i), ("Nmax", _i), ("n_sum", _i), ("n_prn", _i),
+                ("len_fds", _i), ("fs", _d), ("fi", _d), ("T", _d),
+                ("fds", C.POINTER(_f)), ("code_fft", _p), ("buf", _i)]
+
+
+class AcqResult(C.Structure):
+    """sdrg_acq_result_t."""
+    _fields_ = [("bin", _i), ("offset", _i), ("cn0", _f), ("pmax", _f),
+                ("pave", _d), ("fd", _d)]
+
+
+# every exported entry point and its signature; tests check the library
+# exports exactly these names
+SIGNATURES = {
+    "sdr_func_init": ([C.c_char_p], None),
+    "sdr_mix_carr": ([C.POINTER(SdrBuff), _i, _i, _d, _d, _d, _p], None),
+    "sdr_corr_std": ([_p, _p, _i, _d, _p, _i, _p, _p], None),
+    "sdr_corr_std_cpx_code": ([_p, _p, _i, _d, _p, _i, _p, _p], None),
+    "sdr_corr_std_cpx": ([_p, _i, _i, _i, _d, _d, _d, _p, _p, _i, _p], None),
+    "sdr_corr_fft": ([_p, _p, _i, _p], None),
+    "sdr_corr_fft_cpx": ([_p, _i, _i, _i, _d, _d, _d, _p, _p], None),
+    "sdr_search_code": ([_p, _d, C.POINTER(SdrBuff), _i, _i, _d, _d, _p, _i, _p], None),
+    "sdr_corr_max": ([_p, _i, _i, _i, _d, _p], _f),
+    "sdr_fine_dop": ([_p, _i, _p, _i, _p], _d),
+    "sdr_dop_bins": ([_d, _f, _f, C.POINTER(_i)], C.POINTER(_f)),
+    "sdr_gpu_last_error": ([C.c_char_p, _i], _i),
+    "sdr_gpu_clear_error": ([], None),
+    "sdrg_init": ([_i], _i),
+    "sdrg_fft_supported": ([_i], _i),
+    "sdrg_version": ([], C.c_char_p),
+    "sdrg_acq_plan_new": ([C.POINTER(AcqSig), _i], _p),
+    "sdrg_acq_plan_free": ([_p], None),
+    "sdrg_acq_plan_cells": ([_p], C.c_int64),
+    "sdrg_acq_run": ([_p, _p, _p, _p, _p, _p], _i),
+    "sdrg_acq_grid": ([_p, _i], _p),
+    "sdrg_acq_grid_host": ([_p, _i, _p], _i),
+    "sdrg_acq_profile": ([_p, _i], _i),
+    "sdrg_acq_profile_get": ([_p, _p, _p], _i),
+    "sdrg_acq_run_host": ([_p, _p, _p, _p, _p], _i),
+}
+
+
+def _load() -> C.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"pocketsdr_b200: {LIB_PATH} is missing; build it with "
+            "`python -m pocketsdr_b200.build` (nvcc, sm_100a)")
+    lib = C.CDLL(LIB_PATH)
+    for name, (args, res) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    return lib
+
+
+lib = _load()
+
+
+class GpuError(RuntimeError):
+    pass
+
+
+def last_error() -> tuple[int, str]:
+    buf = C.create_string_buffer(512)
+    code = lib.sdr_gpu_last_error(buf, 512)
+    return code, buf.value.decode(errors="replace")
+
+
+def check(what: str = "") -> None:
+    """Raises GpuError when the last call on this thread failed (and clears it)."""
+    code, msg = last_error()
+    if code:
+        lib.sdr_gpu_clear_error()
+        raise GpuError(f"{what}: {msg} (status {code})" if what else f"{msg} (status {code})")
+
+
+def ptr(a) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)

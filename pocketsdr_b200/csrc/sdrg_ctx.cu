@@ -1,0 +1,332 @@
+// sdrg_ctx.cu - device context, per-thread streams and scratch, error state,
+// FFT plan construction and the library's version/init entry points.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+
+#include "sdrg_internal.h"
+
+namespace sdrg {
+
+const float kCScale = 1 / 11.2f;
+
+// ---- errors --------------------------------------------------------------------
+ThreadCtx &tctx()
+{
+    static thread_local ThreadCtx ctx;
+    return ctx;
+}
+
+int set_error(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    ThreadCtx &c = tctx();
+    c.error = code;
+    c.msg = buf;
+    fprintf(stderr, "pocketsdr_b200: %s\n", buf);
+    return code;
+}
+
+int cuda_error(cudaError_t e, const char *what)
+{
+    return set_error(e == cudaErrorMemoryAllocation ? SDRG_ERR_NOMEM : SDRG_ERR_CUDA,
+                     "%s: %s", what, cudaGetErrorString(e));
+}
+
+// ---- device ------------------------------------------------------------------
+static std::mutex g_dev_mtx;
+static Device g_dev;
+static int g_dev_wanted = -1;
+
+static void build_ctab(int8_t *ctab)
+{
+    // src/sdr_func.c:115-118: ROUND(cos|sin(-2 pi i / 256) / SDR_CSCALE),
+    // ROUND(x) = floor(x + 0.5), PI = 3.1415926535897932, in double.
+    const double pi = 3.1415926535897932;
+    for (int i = 0; i < 256; ++i) {
+        ctab[2 * i] = (int8_t)floor(cos(-2.0 * pi * i / 256) / (double)kCScale + 0.5);
+        ctab[2 * i + 1] = (int8_t)floor(sin(-2.0 * pi * i / 256) / (double)kCScale + 0.5);
+    }
+}
+
+int ensure_device(Device **out)
+{
+    std::lock_guard<std::mutex> lk(g_dev_mtx);
+    if (g_dev.id < 0) {
+        int id = g_dev_wanted;
+        if (id < 0) {
+            const char *env = getenv("SDRG_DEVICE");
+            id = env ? atoi(env) : 0;
+        }
+        int n = 0;
+        cudaError_t e = cudaGetDeviceCount(&n);
+        if (e != cudaSuccess || n <= id) {
+            return set_error(SDRG_ERR_NODEV, "no CUDA device %d available (%s)", id,
+                             e != cudaSuccess ? cudaGetErrorString(e) : "count too small");
+        }
+        SDRG_CUDA(cudaSetDevice(id));
+        cudaDeviceProp prop;
+        SDRG_CUDA(cudaGetDeviceProperties(&prop, id));
+        if (prop.major < 10) {
+            return set_error(SDRG_ERR_NODEV, "device %d (%s, sm_%d%d) is not sm_100", id,
+                             prop.name, prop.major, prop.minor);
+        }
+        g_dev.sm_count = prop.multiProcessorCount;
+        g_dev.smem_optin = prop.sharedMemPerBlockOptin;
+        build_ctab(g_dev.ctab);
+        SDRG_CUDA(cudaMalloc(&g_dev.ctab_dev, 512));
+        SDRG_CUDA(cudaMemcpy(g_dev.ctab_dev, g_dev.ctab, 512, cudaMemcpyHostToDevice));
+        g_dev.id = id;
+    }
+    SDRG_CUDA(cudaSetDevice(g_dev.id));
+    if (out) *out = &g_dev;
+    return SDRG_OK;
+}
+
+size_t g_smem_limit() { return g_dev.id >= 0 ? g_dev.smem_optin : 232448; }
+
+int thread_stream(cudaStream_t *s)
+{
+    ThreadCtx &c = tctx();
+    if (!c.stream) {
+        SDRG_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    }
+    *s = c.stream;
+    return SDRG_OK;
+}
+
+Scratch::~Scratch()
+{
+    // Released at thread exit; errors are ignored (the context may be gone).
+    if (ptr) {
+        if (pinned) cudaFreeHost(ptr); else cudaFree(ptr);
+    }
+}
+
+int Scratch::reserve(size_t bytes)
+{
+    if (bytes <= size) return SDRG_OK;
+    size_t want = bytes + bytes / 4 + 256;
+    if (ptr) {
+        if (pinned) cudaFreeHost(ptr); else cudaFree(ptr);
+        ptr = nullptr;
+        size = 0;
+    }
+    cudaError_t e = pinned ? cudaMallocHost(&ptr, want) : cudaMalloc(&ptr, want);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        return cuda_error(e, pinned ? "cudaMallocHost" : "cudaMalloc");
+    }
+    size = want;
+    return SDRG_OK;
+}
+
+// ---- FFT plans -----------------------------------------------------------------
+static const int kRadices[] = {16, 15, 12, 10, 8, 6, 5, 4, 3, 2};
+
+struct Fact { int a, b, c; };  // 2^a 3^b 5^c
+
+static bool factor235(int n, Fact *f)
+{
+    f->a = f->b = f->c = 0;
+    if (n <= 0) return false;
+    while (n % 2 == 0) { n /= 2; f->a++; }
+    while (n % 3 == 0) { n /= 3; f->b++; }
+    while (n % 5 == 0) { n /= 5; f->c++; }
+    return n == 1;
+}
+
+// Best radix sequence for 2^a 3^b 5^c: fewest passes, then the largest
+// smallest radix (balanced passes). Exhaustive over the small exponent space.
+static void best_radices(int n, std::vector<int> &cur, std::vector<int> &best)
+{
+    if (n == 1) {
+        if (best.empty() || cur.size() < best.size()) { best = cur; return; }
+        if (cur.size() == best.size()) {
+            int mc = 1 << 30, mb = 1 << 30;
+            for (int r : cur) mc = r < mc ? r : mc;
+            for (int r : best) mb = r < mb ? r : mb;
+            if (mc > mb) best = cur;
+        }
+        return;
+    }
+    if (!best.empty() && cur.size() + 1 > best.size()) return;
+    int last = cur.empty() ? 1 << 30 : cur.back();
+    for (int r : kRadices) {
+        if (r > last || n % r) continue;  // non-increasing order avoids repeats
+        cur.push_back(r);
+        best_radices(n / r, cur, best);
+        cur.pop_back();
+    }
+}
+
+static size_t plan_smem(int M, const FftPlanK &k)
+{
+    return (size_t)M * sizeof(float2) + (size_t)k.twtot * sizeof(float2) + 512;
+}
+
+// Max dynamic shared memory per CTA assumed when no device is present.
+static const size_t kSmemDefault = 232448;
+
+bool plan_shape(int L, int *Rout, int *Mout, FftPlanK *kout)
+{
+    static const int Rs[] = {1, 2, 3, 4, 5, 6, 8};
+    size_t smax = g_dev.id >= 0 ? g_dev.smem_optin : kSmemDefault;
+    for (int R : Rs) {
+        if (L % R) continue;
+        int M = L / R;
+        Fact f;
+        if (!factor235(M, &f)) continue;
+        std::vector<int> cur, best;
+        if (M == 1) best.push_back(1);
+        else best_radices(M, cur, best);
+        if (best.empty() || (int)best.size() > kMaxPass) continue;
+        FftPlanK k{};
+        k.M = M;
+        k.npass = (int)best.size();
+        int Ls = M, off = 0;
+        for (int p = 0; p < k.npass; ++p) {
+            k.radix[p] = best[p];
+            k.Ls[p] = Ls;
+            k.twoff[p] = off;
+            off += Ls / best[p];
+            Ls /= best[p];
+        }
+        k.twtot = off;
+        if (M == 1) { k.npass = 0; k.twtot = 0; }
+        if (plan_smem(M, k) > smax) continue;
+        *Rout = R;
+        *Mout = M;
+        *kout = k;
+        return true;
+    }
+    return false;
+}
+
+static std::mutex g_plan_mtx;
+static std::map<int, FftPlan *> g_plans;
+
+static int build_plan(int L, FftPlan *pl)
+{
+    int R, M;
+    FftPlanK k;
+    if (!plan_shape(L, &R, &M, &k)) {
+        return set_error(SDRG_ERR_ARG,
+                         "FFT length %d unsupported (needs L = R*M, R in {1..6,8}, "
+                         "M 2-3-5-smooth and fitting one CTA)", L);
+    }
+    pl->L = L; pl->R = R; pl->M = M; pl->k = k;
+    int t = 32;
+    while (t < 512 && t * 8 < M) t *= 2;
+    pl->threads = t;
+    pl->smem = plan_smem(M, k);
+    // per-pass twiddles exp(-2 pi i * i / Ls_p), i < S_p
+    std::vector<float2> tw(k.twtot > 0 ? k.twtot : 1);
+    for (int p = 0; p < k.npass; ++p) {
+        int Ls = k.Ls[p], S = Ls / k.radix[p];
+        for (int i = 0; i < S; ++i) {
+            double a = -2.0 * M_PI * i / Ls;
+            tw[k.twoff[p] + i] = make_float2((float)cos(a), (float)sin(a));
+        }
+    }
+    // digit-reversed frequency index of each DIF output position
+    pl->kperm.resize(M);
+    for (int q = 0; q < M; ++q) {
+        int rem = q, blk = M, kk = 0, mul = 1;
+        for (int p = 0; p < k.npass; ++p) {
+            blk /= k.radix[p];
+            int j = rem / blk;
+            rem %= blk;
+            kk += j * mul;
+            mul *= k.radix[p];
+        }
+        pl->kperm[q] = kk;
+    }
+    std::vector<float2> split(M);
+    for (int q = 0; q < M; ++q) {
+        double a = 2.0 * M_PI * (double)pl->kperm[q] / L;
+        split[q] = make_float2((float)cos(a), (float)sin(a));
+    }
+    SDRG_CUDA(cudaMalloc(&pl->tw_dev, tw.size() * sizeof(float2)));
+    SDRG_CUDA(cudaMemcpy(pl->tw_dev, tw.data(), tw.size() * sizeof(float2),
+                         cudaMemcpyHostToDevice));
+    SDRG_CUDA(cudaMalloc(&pl->kperm_dev, M * sizeof(int)));
+    SDRG_CUDA(cudaMemcpy(pl->kperm_dev, pl->kperm.data(), M * sizeof(int),
+                         cudaMemcpyHostToDevice));
+    SDRG_CUDA(cudaMalloc(&pl->split_dev, M * sizeof(float2)));
+    SDRG_CUDA(cudaMemcpy(pl->split_dev, split.data(), M * sizeof(float2),
+                         cudaMemcpyHostToDevice));
+    return SDRG_OK;
+}
+
+const FftPlan *get_plan(int L)
+{
+    std::lock_guard<std::mutex> lk(g_plan_mtx);
+    auto it = g_plans.find(L);
+    if (it != g_plans.end()) return it->second;
+    FftPlan *pl = new FftPlan();
+    if (build_plan(L, pl) != SDRG_OK) {
+        delete pl;
+        return nullptr;
+    }
+    g_plans[L] = pl;
+    return pl;
+}
+
+} // namespace sdrg
+
+using namespace sdrg;
+
+extern "C" {
+
+int sdr_gpu_last_error(char *buff, int size)
+{
+    ThreadCtx &c = tctx();
+    if (buff && size > 0) {
+        snprintf(buff, (size_t)size, "%s", c.msg.c_str());
+    }
+    return c.error;
+}
+
+void sdr_gpu_clear_error(void)
+{
+    ThreadCtx &c = tctx();
+    c.error = 0;
+    c.msg.clear();
+}
+
+int sdrg_init(int device)
+{
+    {
+        std::lock_guard<std::mutex> lk(g_dev_mtx);
+        if (g_dev.id >= 0 && device >= 0 && device != g_dev.id) {
+            return set_error(SDRG_ERR_ARG, "already initialised on device %d", g_dev.id);
+        }
+        g_dev_wanted = device;
+    }
+    return ensure_device(nullptr);
+}
+
+int sdrg_fft_supported(int N)
+{
+    int R, M;
+    FftPlanK k;
+    return N > 0 && plan_shape(N, &R, &M, &k) ? 1 : 0;
+}
+
+const char *sdrg_version(void) { return "pocketsdr_b200 0.1 (sm_100a)"; }
+
+void sdr_func_init(const char *file)
+{
+    (void)file;
+    ensure_device(nullptr);
+}
+
+} // extern "C"

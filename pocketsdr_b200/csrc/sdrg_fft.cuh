@@ -1,0 +1,350 @@
+// sdrg_fft.cuh - shared-memory mixed-radix FFT for one CTA (sm_100a).
+//
+// One CTA transforms M <= ~27K complex floats held in shared memory.
+//   forward : decimation in frequency (DIF), natural-order input, output in
+//             mixed-radix digit-reversed positions;
+//   inverse : decimation in time (DIT), input in those digit-reversed
+//             positions, natural-order output, unnormalised (exp(+i)).
+// A forward DIF followed by the inverse DIT therefore needs no reordering:
+// the frequency-domain product is formed directly in the permuted order,
+// with the code DFT stored permuted once at plan time.
+//
+// Pass p works on sub-sequences of length Ls_p = M / (r_0 ... r_{p-1}); a
+// butterfly reads r_p elements at stride S_p = Ls_p / r_p, so butterflies
+// never overlap and each pass runs in place with one barrier after it.
+// Twiddles: pass p uses w = exp(-2 pi i * i / Ls_p) from a per-pass table of
+// S_p entries in shared memory; w^j for j >= 2 by repeated products.
+// Butterfly kernels are compile-time DFTs of size 2,3,4,5 and Cooley-Tukey
+// composites of them (6,8,10,12,15,16) with constant twiddles.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sdrg {
+
+constexpr int kMaxPass = 8;
+
+// ---- compile-time trigonometry (Taylor series, double) --------------------
+__host__ __device__ constexpr double cx_pi() { return 3.14159265358979323846; }
+
+__host__ __device__ constexpr double cx_sin(double x)
+{
+    double term = x, sum = x;
+    for (int n = 1; n < 24; ++n) {
+        term *= -x * x / ((2.0 * n) * (2.0 * n + 1.0));
+        sum += term;
+    }
+    return sum;
+}
+
+__host__ __device__ constexpr double cx_cos(double x)
+{
+    double term = 1.0, sum = 1.0;
+    for (int n = 1; n < 24; ++n) {
+        term *= -x * x / ((2.0 * n - 1.0) * (2.0 * n));
+        sum += term;
+    }
+    return sum;
+}
+
+// exp(dir * 2 pi i * e / n) with the angle folded into [-pi, pi]
+template <int N, int DIR>
+struct TwConst {
+    float c[N], s[N];
+    __host__ __device__ constexpr TwConst() : c(), s()
+    {
+        for (int e = 0; e < N; ++e) {
+            int ee = (e <= N / 2) ? e : e - N;
+            double a = DIR * 2.0 * cx_pi() * ee / N;
+            c[e] = (float)cx_cos(a);
+            s[e] = (float)cx_sin(a);
+        }
+    }
+};
+
+// ---- complex helpers --------------------------------------------------------
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b)
+{
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+// multiply by dir*i (dir=+1: i, dir=-1: -i)
+template <int DIR>
+__device__ __forceinline__ float2 cmul_i(float2 a)
+{
+    return DIR > 0 ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+// ---- in-register DFTs, natural order in and out ---------------------------
+// DIR = -1: forward (exp(-i)), DIR = +1: backward (exp(+i)).
+template <int N, int DIR> struct Dft;
+
+template <int DIR> struct Dft<1, DIR> {
+    __device__ __forceinline__ static void run(float2 *) {}
+};
+
+template <int DIR> struct Dft<2, DIR> {
+    __device__ __forceinline__ static void run(float2 *v)
+    {
+        float2 a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    }
+};
+
+template <int DIR> struct Dft<3, DIR> {
+    __device__ __forceinline__ static void run(float2 *v)
+    {
+        const float c = 0.86602540378443864676f; // sqrt(3)/2
+        float2 s = cadd(v[1], v[2]), d = csub(v[1], v[2]);
+        float2 a = make_float2(v[0].x - 0.5f * s.x, v[0].y - 0.5f * s.y);
+        float2 t = cmul_i<DIR>(make_float2(c * d.x, c * d.y));
+        v[0] = cadd(v[0], s);
+        v[1] = cadd(a, t);
+        v[2] = csub(a, t);
+    }
+};
+
+template <int DIR> struct Dft<4, DIR> {
+    __device__ __forceinline__ static void run(float2 *v)
+    {
+        float2 a = cadd(v[0], v[2]), b = csub(v[0], v[2]);
+        float2 c = cadd(v[1], v[3]), d = cmul_i<DIR>(csub(v[1], v[3]));
+        v[0] = cadd(a, c);
+        v[2] = csub(a, c);
+        v[1] = cadd(b, d);
+        v[3] = csub(b, d);
+    }
+};
+
+template <int DIR> struct Dft<5, DIR> {
+    __device__ __forceinline__ static void run(float2 *v)
+    {
+        const float c1 = 0.30901699437494742410f;  // cos(2pi/5)
+        const float c2 = -0.80901699437494742410f; // cos(4pi/5)
+        const float s1 = 0.95105651629515357212f;  // sin(2pi/5)
+        const float s2 = 0.58778525229247312917f;  // sin(4pi/5)
+        float2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+        float2 t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+        float2 x0 = v[0];
+        float2 a1 = make_float2(x0.x + c1 * t1.x + c2 * t2.x, x0.y + c1 * t1.y + c2 * t2.y);
+        float2 a2 = make_float2(x0.x + c2 * t1.x + c1 * t2.x, x0.y + c2 * t1.y + c1 * t2.y);
+        float2 b1 = make_float2(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y);
+        float2 b2 = make_float2(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y);
+        b1 = cmul_i<DIR>(b1);
+        b2 = cmul_i<DIR>(b2);
+        v[0] = cadd(x0, cadd(t1, t2));
+        v[1] = cadd(a1, b1);
+        v[4] = csub(a1, b1);
+        v[2] = cadd(a2, b2);
+        v[3] = csub(a2, b2);
+    }
+};
+
+// Cooley-Tukey composite N = A*B: n = B*n1 + n2, k = k1 + A*k2.
+template <int A, int B, int DIR>
+struct DftCT {
+    static constexpr int N = A * B;
+    __device__ __forceinline__ static void run(float2 *v)
+    {
+        constexpr TwConst<N, DIR> tw{};
+        float2 y[N];
+#pragma unroll
+        for (int n2 = 0; n2 < B; ++n2) {
+            float2 t[A];
+#pragma unroll
+            for (int n1 = 0; n1 < A; ++n1) t[n1] = v[B * n1 + n2];
+            Dft<A, DIR>::run(t);
+#pragma unroll
+            for (int k1 = 0; k1 < A; ++k1) {
+                const int e = (n2 * k1) % N;
+                if (e == 0) {
+                    y[n2 * A + k1] = t[k1];
+                } else {
+                    y[n2 * A + k1] = cmul(t[k1], make_float2(tw.c[e], tw.s[e]));
+                }
+            }
+        }
+#pragma unroll
+        for (int k1 = 0; k1 < A; ++k1) {
+            float2 t[B];
+#pragma unroll
+            for (int n2 = 0; n2 < B; ++n2) t[n2] = y[n2 * A + k1];
+            Dft<B, DIR>::run(t);
+#pragma unroll
+            for (int k2 = 0; k2 < B; ++k2) v[k1 + A * k2] = t[k2];
+        }
+    }
+};
+
+template <int DIR> struct Dft<6, DIR>  : DftCT<2, 3, DIR> {};
+template <int DIR> struct Dft<8, DIR>  : DftCT<2, 4, DIR> {};
+template <int DIR> struct Dft<10, DIR> : DftCT<2, 5, DIR> {};
+template <int DIR> struct Dft<12, DIR> : DftCT<4, 3, DIR> {};
+template <int DIR> struct Dft<15, DIR> : DftCT<3, 5, DIR> {};
+template <int DIR> struct Dft<16, DIR> : DftCT<4, 4, DIR> {};
+
+// ---- kernel-side plan --------------------------------------------------------
+struct FftPlanK {
+    int M;                  // transform length held by one CTA
+    int npass;
+    int radix[kMaxPass];    // DIF order
+    int Ls[kMaxPass];       // sub-sequence length at pass p
+    int twoff[kMaxPass];    // offset of pass p's table in the twiddle array
+    int twtot;              // total twiddle entries (sum of S_p)
+};
+
+// Runs fn<R>() for the runtime radix r (instantiates every supported radix).
+#define SDRG_RADIX_DISPATCH(r, CALL)            \
+    switch (r) {                                \
+    case 2:  { constexpr int R_ = 2;  CALL; } break;  \
+    case 3:  { constexpr int R_ = 3;  CALL; } break;  \
+    case 4:  { constexpr int R_ = 4;  CALL; } break;  \
+    case 5:  { constexpr int R_ = 5;  CALL; } break;  \
+    case 6:  { constexpr int R_ = 6;  CALL; } break;  \
+    case 8:  { constexpr int R_ = 8;  CALL; } break;  \
+    case 10: { constexpr int R_ = 10; CALL; } break;  \
+    case 12: { constexpr int R_ = 12; CALL; } break;  \
+    case 15: { constexpr int R_ = 15; CALL; } break;  \
+    case 16: { constexpr int R_ = 16; CALL; } break;  \
+    default: break;                             \
+    }
+
+// Twiddle powers w^1..w^(R-1) applied to v[1..R-1]
+template <int R>
+__device__ __forceinline__ void apply_tw(float2 *v, float2 w1)
+{
+    float2 w = w1;
+#pragma unroll
+    for (int j = 1; j < R; ++j) {
+        v[j] = cmul(v[j], w);
+        if (j + 1 < R) w = cmul(w, w1);
+    }
+}
+
+// One in-place DIF (forward) pass.
+template <int R>
+__device__ __forceinline__ void dif_pass(float2 *sm, int M, int Ls,
+                                         const float2 *twp, int tid, int nthr)
+{
+    const int S = Ls / R, nb = M / R;
+    for (int b = tid; b < nb; b += nthr) {
+        const int blk = b / S, i = b - blk * S;
+        float2 *p = sm + blk * Ls + i;
+        float2 v[R];
+#pragma unroll
+        for (int j = 0; j < R; ++j) v[j] = p[j * S];
+        Dft<R, -1>::run(v);
+        if (i) apply_tw<R>(v, twp[i]);
+#pragma unroll
+        for (int j = 0; j < R; ++j) p[j * S] = v[j];
+    }
+}
+
+// One in-place DIT (inverse) pass: conjugate twiddles, then backward DFT.
+template <int R>
+__device__ __forceinline__ void dit_pass(float2 *sm, int M, int Ls,
+                                         const float2 *twp, int tid, int nthr)
+{
+    const int S = Ls / R, nb = M / R;
+    for (int b = tid; b < nb; b += nthr) {
+        const int blk = b / S, i = b - blk * S;
+        float2 *p = sm + blk * Ls + i;
+        float2 v[R];
+#pragma unroll
+        for (int j = 0; j < R; ++j) v[j] = p[j * S];
+        if (i) apply_tw<R>(v, cconj(twp[i]));
+        Dft<R, 1>::run(v);
+#pragma unroll
+        for (int j = 0; j < R; ++j) p[j * S] = v[j];
+    }
+}
+
+// First DIF pass fused with the input: element m comes from load(m).
+template <int R, class Load>
+__device__ __forceinline__ void dif_pass0_load(float2 *sm, int M,
+                                               const float2 *twp, Load &load,
+                                               int tid, int nthr)
+{
+    const int S = M / R;
+    for (int i = tid; i < S; i += nthr) {
+        float2 v[R];
+#pragma unroll
+        for (int j = 0; j < R; ++j) v[j] = load(i + j * S);
+        Dft<R, -1>::run(v);
+        if (i) apply_tw<R>(v, twp[i]);
+#pragma unroll
+        for (int j = 0; j < R; ++j) sm[i + j * S] = v[j];
+    }
+}
+
+// Last DIT pass fused with the output: store(m, y_m) for natural index m.
+template <int R, class Store>
+__device__ __forceinline__ void dit_pass0_store(const float2 *sm, int M,
+                                                const float2 *twp, Store &store,
+                                                int tid, int nthr)
+{
+    const int S = M / R;
+    for (int i = tid; i < S; i += nthr) {
+        float2 v[R];
+#pragma unroll
+        for (int j = 0; j < R; ++j) v[j] = sm[i + j * S];
+        if (i) apply_tw<R>(v, cconj(twp[i]));
+        Dft<R, 1>::run(v);
+#pragma unroll
+        for (int j = 0; j < R; ++j) store(i + j * S, v[j]);
+    }
+}
+
+// Full forward transform: pass 0 fused with load(), result left in sm
+// (digit-reversed order). Ends with a barrier.
+template <class Load>
+__device__ void fft_forward(float2 *sm, const float2 *tw, const FftPlanK &pl,
+                            Load &load)
+{
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    {
+        const int r = pl.radix[0];
+        const float2 *twp = tw + pl.twoff[0];
+        SDRG_RADIX_DISPATCH(r, (dif_pass0_load<R_>(sm, pl.M, twp, load, tid, nthr)));
+    }
+    __syncthreads();
+    for (int p = 1; p < pl.npass; ++p) {
+        const int r = pl.radix[p], Ls = pl.Ls[p];
+        const float2 *twp = tw + pl.twoff[p];
+        SDRG_RADIX_DISPATCH(r, (dif_pass<R_>(sm, pl.M, Ls, twp, tid, nthr)));
+        __syncthreads();
+    }
+}
+
+// Full inverse transform of sm (digit-reversed input); the last pass hands
+// every natural-order output to store(). Starts after the caller's barrier;
+// no barrier at the end.
+template <class Store>
+__device__ void fft_inverse(float2 *sm, const float2 *tw, const FftPlanK &pl,
+                            Store &store)
+{
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    for (int p = pl.npass - 1; p >= 1; --p) {
+        const int r = pl.radix[p], Ls = pl.Ls[p];
+        const float2 *twp = tw + pl.twoff[p];
+        SDRG_RADIX_DISPATCH(r, (dit_pass<R_>(sm, pl.M, Ls, twp, tid, nthr)));
+        __syncthreads();
+    }
+    {
+        const int r = pl.radix[0];
+        const float2 *twp = tw + pl.twoff[0];
+        SDRG_RADIX_DISPATCH(r, (dit_pass0_store<R_>(sm, pl.M, twp, store, tid, nthr)));
+    }
+}
+
+// Copies the per-pass twiddle tables from global to shared memory.
+__device__ __forceinline__ void load_twiddles(float2 *tw_sm, const float2 *tw_g,
+                                              int n)
+{
+    for (int i = threadIdx.x; i < n; i += blockDim.x) tw_sm[i] = tw_g[i];
+}
+
+} // namespace sdrg

@@ -1,0 +1,89 @@
+// sdrg_internal.h - host-side internals shared by the library's .cu files.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "pocket_sdr_gpu.h"
+#include "sdrg_fft.cuh"
+
+namespace sdrg {
+
+// SDR_CSCALE of src/pocket_sdr.h:61, evaluated in float on the host
+// (1 / 11.2f) and handed to kernels as an argument.
+extern const float kCScale;
+
+// ---- error state (per host thread) ----------------------------------------
+int set_error(int code, const char *fmt, ...);
+int cuda_error(cudaError_t e, const char *what);
+#define SDRG_CUDA(call)                                            \
+    do {                                                           \
+        cudaError_t e__ = (call);                                  \
+        if (e__ != cudaSuccess) return ::sdrg::cuda_error(e__, #call); \
+    } while (0)
+
+// ---- device context ----------------------------------------------------------
+struct Device {
+    int id = -1;
+    int sm_count = 0;
+    size_t smem_optin = 0;      // max dynamic shared memory per block
+    int8_t ctab[512];           // quantised carrier (I,Q) for 256 phases
+    char2 *ctab_dev = nullptr;  // same table on the device
+};
+int ensure_device(Device **out);   // lazy init of the selected device
+size_t g_smem_limit();             // max dynamic shared memory per CTA
+
+// Grow-only device / pinned buffers owned by one host thread.
+struct Scratch {
+    void *ptr = nullptr;
+    size_t size = 0;
+    bool pinned = false;
+    ~Scratch();
+    int reserve(size_t bytes);
+};
+
+struct ThreadCtx {
+    cudaStream_t stream = nullptr;
+    Scratch dev[6];      // device scratch slots
+    Scratch host[3];     // pinned host staging slots
+    int error = 0;
+    std::string msg;
+};
+ThreadCtx &tctx();
+int thread_stream(cudaStream_t *s);  // creates the thread's stream lazily
+
+// ---- FFT plans -------------------------------------------------------------
+// A length-L transform is split as L = R * M: R CTAs (a thread-block cluster
+// when R > 1) each hold one length-M sub-transform in shared memory.
+struct FftPlan {
+    int L = 0, R = 0, M = 0;
+    FftPlanK k{};              // pass structure for the length-M transform
+    int threads = 0;           // CTA size
+    size_t smem = 0;           // dynamic shared memory bytes per CTA
+    float2 *tw_dev = nullptr;  // per-pass twiddles (k.twtot entries)
+    int *kperm_dev = nullptr;  // k(q): natural frequency index at position q
+    float2 *split_dev = nullptr; // exp(+2 pi i k(q) / L) at position q (R > 1)
+    std::vector<int> kperm;    // host copy of k(q)
+};
+// Returns a cached plan for length L (thread-safe), or nullptr with the
+// error set when L has no supported decomposition.
+const FftPlan *get_plan(int L);
+bool plan_shape(int L, int *R, int *M, FftPlanK *k);
+
+// ---- kernel launch helpers (defined in the .cu files) -----------------------
+// Packed IF source of one coherent block for the forward transform.
+struct IfWindow {
+    const uint8_t *buf;   // device circular buffer
+    int len;              // buffer length (samples)
+    int ix;               // first sample
+};
+
+// Packs a float I/Q window as the reference's python-facing calls do
+// (src/sdr_func.c:839-848) and mixes it into iq_dev (device, N samples).
+int mix_cpx_device(const sdr_cpx_t *buff, int len_buff, int ix, int N, double fs,
+                   double fc, double phi, char2 *iq_dev, cudaStream_t st);
+
+} // namespace sdrg

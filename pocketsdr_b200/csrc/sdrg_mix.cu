@@ -1,0 +1,180 @@
+// sdrg_mix.cu - carrier wipe-off (reference: src/sdr_func.c:772-848).
+//
+// A packed sample (I in the low nibble, Q in the high nibble, each sign-
+// extended) is rotated by the quantised carrier of its 8-bit phase:
+//   I' = (int8)(I*cI - Q*cQ),  Q' = (int8)(I*cQ + Q*cI)
+// which is exactly the reference's 64K-entry table entry (src/sdr_func.c:
+// 113-134); the phase of sample n is p0 + n*step (uint32, wrapping), and a
+// window that crosses the end of the circular buffer restarts the phase at
+// the wrap from phi + step*n (src/sdr_func.c:829-835).
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "sdrg_internal.h"
+
+namespace sdrg {
+
+__device__ __forceinline__ char2 mix_byte(uint8_t byte, uint32_t phase, const char2 *ctab)
+{
+    const int I = (int)(int8_t)(uint8_t)(byte << 4) >> 4;
+    const int Q = (int)(int8_t)byte >> 4;
+    const char2 c = ctab[phase >> 24];
+    char2 o;
+    o.x = (signed char)(I * c.x - Q * c.y);
+    o.y = (signed char)(I * c.y + Q * c.x);
+    return o;
+}
+
+// 4 samples per thread; win is a linear copy of the window (N samples).
+__global__ void mix_kernel(const uint8_t *__restrict__ win, int N, int nsplit,
+                           uint32_t p0a, uint32_t p0b, uint32_t step,
+                           const char2 *__restrict__ ctab_g, char2 *__restrict__ out)
+{
+    __shared__ char2 ctab[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) ctab[i] = ctab_g[i];
+    __syncthreads();
+    const int n0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (n0 >= N) return;
+    if (n0 + 4 <= N) {
+        const uchar4 b = *(const uchar4 *)(win + n0);
+        const uint8_t bb[4] = {b.x, b.y, b.z, b.w};
+        char2 o[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int n = n0 + j;
+            const uint32_t ph = n < nsplit ? p0a + step * (uint32_t)n
+                                           : p0b + step * (uint32_t)(n - nsplit);
+            o[j] = mix_byte(bb[j], ph, ctab);
+        }
+        *(int2 *)(out + n0) = make_int2(
+            (int)((uint32_t)(uint8_t)o[0].x | ((uint32_t)(uint8_t)o[0].y << 8) |
+                  ((uint32_t)(uint8_t)o[1].x << 16) | ((uint32_t)(uint8_t)o[1].y << 24)),
+            (int)((uint32_t)(uint8_t)o[2].x | ((uint32_t)(uint8_t)o[2].y << 8) |
+                  ((uint32_t)(uint8_t)o[3].x << 16) | ((uint32_t)(uint8_t)o[3].y << 24)));
+    } else {
+        for (int n = n0; n < N; ++n) {
+            const uint32_t ph = n < nsplit ? p0a + step * (uint32_t)n
+                                           : p0b + step * (uint32_t)(n - nsplit);
+            out[n] = mix_byte(win[n], ph, ctab);
+        }
+    }
+}
+
+// float I/Q -> (int8) -> 4+4-bit pack (src/sdr_func.c:842-844, SDR_CPX8 of
+// src/pocket_sdr.h:103): C's float->int8 conversion truncates toward zero.
+__global__ void pack_cpx_kernel(const float2 *__restrict__ in, int N, uint8_t *__restrict__ out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const float2 v = in[i];
+    const int8_t re = (int8_t)__float2int_rz(v.x);
+    const int8_t im = (int8_t)__float2int_rz(v.y);
+    out[i] = (uint8_t)(((uint8_t)im << 4) | ((uint8_t)re & 0x0F));
+}
+
+static inline uint32_t phase_of(double phi)
+{
+    return (uint32_t)((phi - floor(phi)) * 4294967296.0);
+}
+static inline uint32_t step_of(double step)
+{
+    return (uint32_t)(int)(step * 4294967296.0);
+}
+
+int launch_mix(const uint8_t *win_dev, int N, int nsplit, uint32_t p0a, uint32_t p0b,
+               uint32_t step, const char2 *ctab_dev, char2 *out_dev, cudaStream_t st)
+{
+    const int threads = 256;
+    const int blocks = (N / 4 + threads) / threads + 1;
+    mix_kernel<<<blocks, threads, 0, st>>>(win_dev, N, nsplit, p0a, p0b, step, ctab_dev, out_dev);
+    SDRG_CUDA(cudaGetLastError());
+    return SDRG_OK;
+}
+
+// Mixes the float buffer as sdr_corr_*_cpx do (src/sdr_func.c:839-848) into
+// iq_dev (device, N samples) on stream st. The phase runs continuously over
+// the N samples (the float buffer is repacked first, so no phase restart).
+int mix_cpx_device(const sdr_cpx_t *buff, int len_buff, int ix, int N, double fs,
+                        double fc, double phi, char2 *iq_dev, cudaStream_t st)
+{
+    if (!buff || len_buff <= 0 || N <= 0)
+        return set_error(SDRG_ERR_ARG, "mix_carr_cpx: bad buffer (len=%d N=%d)", len_buff, N);
+    Device *dev;
+    int e;
+    if ((e = ensure_device(&dev))) return e;
+    ThreadCtx &c = tctx();
+    c.host[1].pinned = true;
+    if ((e = c.host[1].reserve((size_t)N * 8)) || (e = c.dev[4].reserve((size_t)N * 9 + 64)))
+        return e;
+    // gather the window j = ix, ix+1, ... (mod len_buff)
+    float2 *h = (float2 *)c.host[1].ptr;
+    int j = ((ix % len_buff) + len_buff) % len_buff;
+    for (int i = 0; i < N;) {
+        int n = len_buff - j < N - i ? len_buff - j : N - i;
+        memcpy(h + i, buff + j, (size_t)n * 8);
+        i += n;
+        j = 0;
+    }
+    float2 *fin = (float2 *)c.dev[4].ptr;
+    uint8_t *packed = (uint8_t *)(fin + N);
+    SDRG_CUDA(cudaMemcpyAsync(fin, h, (size_t)N * 8, cudaMemcpyHostToDevice, st));
+    pack_cpx_kernel<<<(N + 255) / 256, 256, 0, st>>>(fin, N, packed);
+    SDRG_CUDA(cudaGetLastError());
+    if ((e = launch_mix(packed, N, N, phase_of(phi), 0, step_of(fc / fs), dev->ctab_dev,
+                        iq_dev, st)))
+        return e;
+    // the staging buffer is reused by the next call: finish the copy first
+    SDRG_CUDA(cudaStreamSynchronize(st));
+    return SDRG_OK;
+}
+
+} // namespace sdrg
+
+using namespace sdrg;
+
+extern "C" {
+
+void sdr_mix_carr(const sdr_buff_t *buff, int ix, int N, double fs, double fc, double phi,
+                  sdr_cpx16_t *IQ)
+{
+    if (N <= 0) return;
+    if (!buff || !buff->data || ix < 0 || ix >= buff->N || N > buff->N) {
+        set_error(SDRG_ERR_ARG, "sdr_mix_carr: bad window ix=%d N=%d len=%d", ix, N,
+                  buff ? buff->N : 0);
+        memset(IQ, 0, (size_t)N * 2);
+        return;
+    }
+    Device *dev;
+    cudaStream_t st;
+    int e;
+    ThreadCtx &c = tctx();
+    c.host[0].pinned = true;
+    if ((e = ensure_device(&dev)) || (e = thread_stream(&st)) ||
+        (e = c.host[0].reserve((size_t)N * 3 + 16)) || (e = c.dev[0].reserve((size_t)N * 3 + 64))) {
+        memset(IQ, 0, (size_t)N * 2);
+        return;
+    }
+    const double step = fc / fs;
+    const int n1 = (ix + N <= buff->N) ? N : buff->N - ix;
+    uint8_t *h = (uint8_t *)c.host[0].ptr;
+    memcpy(h, buff->data + ix, (size_t)n1);
+    if (n1 < N) memcpy(h + n1, buff->data, (size_t)(N - n1));
+    const uint32_t p0a = phase_of(phi);
+    const uint32_t p0b = n1 < N ? phase_of(phi + step * n1) : 0;
+    uint8_t *win_d = (uint8_t *)c.dev[0].ptr;
+    const size_t off = ((size_t)N + 15) / 16 * 16;
+    char2 *out_d = (char2 *)(win_d + off);
+    char2 *out_h = (char2 *)(h + off);
+    if (cudaMemcpyAsync(win_d, h, (size_t)N, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        launch_mix(win_d, N, n1, p0a, p0b, step_of(step), dev->ctab_dev, out_d, st) ||
+        cudaMemcpyAsync(out_h, out_d, (size_t)N * 2, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+        cuda_error(cudaGetLastError(), "sdr_mix_carr");
+        memset(IQ, 0, (size_t)N * 2);
+        return;
+    }
+    memcpy(IQ, out_h, (size_t)N * 2);
+}
+
+} // extern "C"

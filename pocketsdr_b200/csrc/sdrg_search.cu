@@ -1,0 +1,832 @@
+// sdrg_search.cu - FFT correlator and parallel-code-phase search on sm_100a.
+//
+// Reference path: src/sdr_func.c:664-687 (sdr_search_code), :1088-1113
+// (sdr_corr_fft, sdr_corr_fft_cpx). A length-L correlation is computed as
+//   X   = FFT_L(mix(IF) * CSCALE)                         (fwd_kernel)
+//   Z   = X * code_fft * (1/L^2)
+//   y   = IFFT_L(Z);  P += |y|^2   or  corr = y           (cons_kernel)
+// with L = R*M split over R CTAs:
+//   forward  (decimation in time):  F_r = FFT_M(x[R m + r]),  r < R, one
+//            independent CTA each;
+//   inverse  (decimation in frequency): CTA c of an R-CTA cluster produces
+//            y[R m + c] = IFFT_M(w_c)[m] with
+//            w_c[k] = e^{+2 pi i c k / L} sum_j Z[k + j M] e^{+2 pi i c j / R}
+//            and Z[k + j M] = code[k + j M] * sum_r e^{-2 pi i r (k + j M)/L} F_r[k].
+// Each cluster CTA forms w_0..w_{R-1} for 1/R of the k range and stores them
+// into the owners' shared memory (distributed shared memory), so X and the
+// code are read from L2/HBM exactly once per (PRN, bin, sum).
+// The forward transform of a (bin, sum) block does not depend on the PRN: it
+// is computed once per signal group and reused by every PRN's consumer task.
+#include <cooperative_groups.h>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "sdrg_internal.h"
+
+namespace cg = cooperative_groups;
+
+namespace sdrg {
+
+// ---------------------------------------------------------------------------
+// mixing of one packed sample (bit-exact with the reference's 64K table,
+// src/sdr_func.c:113-134 and :772-807)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ char2 mix_one(uint8_t byte, uint32_t phase,
+                                         const char2 *ctab)
+{
+    const int I = (int)(int8_t)(uint8_t)(byte << 4) >> 4;
+    const int Q = (int)(int8_t)byte >> 4;
+    const char2 c = ctab[phase >> 24];
+    char2 o;
+    o.x = (signed char)(I * c.x - Q * c.y);
+    o.y = (signed char)(I * c.y + Q * c.x);
+    return o;
+}
+
+// ---------------------------------------------------------------------------
+// forward kernel
+// ---------------------------------------------------------------------------
+struct FwdArgs {
+    FftPlanK pl;
+    const float2 *tw;      // per-pass twiddles (global)
+    const char2 *ctab;     // carrier table (global)
+    int R;                 // split factor
+    int n_bin, n_sum;
+    float cscale;
+    // mode 0: packed IF + mixing
+    const uint8_t *buf;    // circular IF buffer
+    int buf_len;
+    const int *ix;         // [n_sum] first sample of each sum
+    const uint32_t *phstep;   // [n_bin] phase step per sample
+    const uint32_t *ph0a;     // [n_bin] phase at sample 0
+    const uint32_t *ph0b;     // [n_bin * n_sum] phase restart after the wrap
+    const int *nsplit;        // [n_sum] samples before the buffer wrap
+    // mode 1: already mixed samples (sdr_cpx16_t), one block
+    const char2 *iq;
+    float2 *X;             // out: [n_bin][n_sum][R][M]
+};
+
+struct LoadIF {
+    const uint8_t *buf;
+    int len, ix0, nsplit, R, r;
+    uint32_t step, p0a, p0b;
+    const char2 *ctab;
+    float cs;
+    __device__ __forceinline__ float2 operator()(int m) const
+    {
+        const int n = R * m + r;
+        int pos = ix0 + n;
+        if (pos >= len) pos -= len;
+        const uint32_t ph = n < nsplit ? p0a + step * (uint32_t)n
+                                       : p0b + step * (uint32_t)(n - nsplit);
+        const char2 v = mix_one(__ldg(buf + pos), ph, ctab);
+        return make_float2(__fmul_rn((float)v.x, cs), __fmul_rn((float)v.y, cs));
+    }
+};
+
+struct LoadIQ {
+    const char2 *iq;
+    int R, r;
+    float cs;
+    __device__ __forceinline__ float2 operator()(int m) const
+    {
+        const char2 v = iq[R * m + r];
+        return make_float2(__fmul_rn((float)v.x, cs), __fmul_rn((float)v.y, cs));
+    }
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(512, 1) fwd_kernel(FwdArgs a)
+{
+    extern __shared__ float2 smem[];
+    float2 *sm = smem;
+    float2 *tw = smem + a.pl.M;
+    char2 *ctab = (char2 *)(tw + a.pl.twtot);
+
+    const int blk = blockIdx.x;
+    const int r = blk % a.R;
+    const int bs = blk / a.R;            // b * n_sum + s
+    const int s = bs % a.n_sum, b = bs / a.n_sum;
+
+    load_twiddles(tw, a.tw, a.pl.twtot);
+    if (MODE == 0) {
+        for (int i = threadIdx.x; i < 256; i += blockDim.x) ctab[i] = a.ctab[i];
+    }
+    __syncthreads();
+
+    if (MODE == 0) {
+        LoadIF ld{a.buf, a.buf_len, a.ix[s], a.nsplit[s], a.R, r, a.phstep[b],
+                  a.ph0a[b], a.ph0b[bs], ctab, a.cscale};
+        fft_forward(sm, tw, a.pl, ld);
+    } else {
+        LoadIQ ld{a.iq, a.R, r, a.cscale};
+        fft_forward(sm, tw, a.pl, ld);
+    }
+    // store F_r (digit-reversed order) contiguously
+    float2 *dst = a.X + ((size_t)bs * a.R + r) * a.pl.M;
+    const int M = a.pl.M;
+    if ((M & 1) == 0) {
+        float4 *d4 = (float4 *)dst;
+        const float4 *s4 = (const float4 *)sm;
+        for (int i = threadIdx.x; i < M / 2; i += blockDim.x) d4[i] = s4[i];
+    } else {
+        for (int i = threadIdx.x; i < M; i += blockDim.x) dst[i] = sm[i];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// consumer kernel
+// ---------------------------------------------------------------------------
+struct ConsArgs {
+    FftPlanK pl;
+    const float2 *tw;       // per-pass twiddles
+    const float2 *split;    // [M] exp(+2 pi i k(q) / L)
+    const float2 *X;        // [n_bin][n_sum][R][M]
+    const float2 *code;     // [n_prn][R][M] permuted conj code DFT
+    int n_prn, n_bin, n_sum;
+    int prn0;               // first PRN of this launch (task = prn-major)
+    float scale;            // 1/L^2 as the reference computes it in float
+    int Nmax;               // grid columns kept
+    size_t prn_stride;      // P stride between PRNs (elements)
+    size_t bin_stride;      // P stride between bins (elements)
+    int accumulate;         // 1: P += |y|^2 from the first sum on (IN/OUT P)
+    float *P;               // mode 0
+    float2 *Y;              // mode 1: [n_bin][L]
+};
+
+template <int R>
+struct StorePower {
+    float *row;       // P for this (prn, bin)
+    int c, Nmax;
+    bool add;
+    __device__ __forceinline__ void operator()(int m, float2 y) const
+    {
+        const int n = R * m + c;
+        if (n < Nmax) {
+            const float pw = y.x * y.x + y.y * y.y;
+            row[n] = add ? row[n] + pw : pw;
+        }
+    }
+};
+
+template <int R>
+struct StoreComplex {
+    float2 *row;
+    int c;
+    __device__ __forceinline__ void operator()(int m, float2 y) const { row[R * m + c] = y; }
+};
+
+template <int R, int MODE>
+__global__ void __launch_bounds__(512, 1) cons_kernel(ConsArgs a)
+{
+    extern __shared__ float2 smem[];
+    float2 *sm = smem;
+    float2 *tw = smem + a.pl.M;
+    const int M = a.pl.M;
+    const int c = (R > 1) ? (int)(blockIdx.x % R) : 0;
+    const int task = blockIdx.x / R;
+    const int prn = a.prn0 + task / a.n_bin;
+    const int b = task % a.n_bin;
+    if (prn >= a.n_prn) return;   // uniform across the cluster
+
+    load_twiddles(tw, a.tw, a.pl.twtot);
+
+    float2 *dst[R];
+    if constexpr (R > 1) {
+        cg::cluster_group cl = cg::this_cluster();
+#pragma unroll
+        for (int j = 0; j < R; ++j) dst[j] = cl.map_shared_rank(sm, j);
+    } else {
+        dst[0] = sm;
+    }
+    const int Mc = (M + R - 1) / R;
+    const int q0 = c * Mc, q1 = min(M, q0 + Mc);
+    const float2 *code = a.code + (size_t)prn * R * M;
+
+    for (int s = 0; s < a.n_sum; ++s) {
+        // all CTAs of the cluster are done with their shared memory
+        if constexpr (R > 1) cg::this_cluster().sync(); else __syncthreads();
+        const float2 *Xs = a.X + ((size_t)b * a.n_sum + s) * R * M;
+        for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
+            float2 g[R];
+            if constexpr (R == 1) {
+                const float2 z = cmul(Xs[q], code[q]);
+                dst[0][q] = make_float2(z.x * a.scale, z.y * a.scale);
+            } else {
+                const float2 t = a.split[q];
+                const float2 tc = cconj(t);
+                g[0] = Xs[q];
+                float2 w = tc;
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    g[r] = cmul(Xs[(size_t)r * M + q], w);
+                    if (r + 1 < R) w = cmul(w, tc);
+                }
+                Dft<R, -1>::run(g);                 // X[k + jM]
+#pragma unroll
+                for (int j = 0; j < R; ++j) {
+                    const float2 z = cmul(g[j], code[(size_t)j * M + q]);
+                    g[j] = make_float2(z.x * a.scale, z.y * a.scale);
+                }
+                Dft<R, 1>::run(g);                  // sum_j Z e^{+2 pi i c j/R}
+                w = t;
+#pragma unroll
+                for (int j = 1; j < R; ++j) {
+                    g[j] = cmul(g[j], w);
+                    if (j + 1 < R) w = cmul(w, t);
+                }
+#pragma unroll
+                for (int j = 0; j < R; ++j) dst[j][q] = g[j];
+            }
+        }
+        if constexpr (R > 1) cg::this_cluster().sync(); else __syncthreads();
+
+        if (MODE == 0) {
+            float *row = a.P + (size_t)(prn) * a.prn_stride + (size_t)b * a.bin_stride;
+            StorePower<R> st{row, c, a.Nmax, a.accumulate || s > 0};
+            fft_inverse(sm, tw, a.pl, st);
+        } else {
+            float2 *row = a.Y + (size_t)b * (size_t)R * M;
+            StoreComplex<R> st{row, c};
+            fft_inverse(sm, tw, a.pl, st);
+        }
+    }
+    // keep remote shared memory alive until every CTA has finished reading
+    if constexpr (R > 1) cg::this_cluster().sync();
+}
+
+// out[p][j][q] = code_nat[p][k(q) + j M] (permuted order of the DIF output)
+__global__ void perm_code_kernel(const float2 *code_nat, const int *kperm, int M,
+                                 int R, int n_prn, float2 *out)
+{
+    const size_t total = (size_t)n_prn * R * M;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const int q = (int)(i % M);
+        const size_t pj = i / M;           // p * R + j
+        const int j = (int)(pj % R);
+        const size_t p = pj / R;
+        out[i] = code_nat[p * (size_t)R * M + (size_t)j * M + kperm[q]];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launch helpers
+// ---------------------------------------------------------------------------
+template <int MODE>
+static int launch_fwd(const FftPlan *pl, const FwdArgs &a, int n_blocks, cudaStream_t st)
+{
+    static bool attr_set[2] = {false, false};
+    if (!attr_set[MODE]) {
+        SDRG_CUDA(cudaFuncSetAttribute(fwd_kernel<MODE>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(g_smem_limit())));
+        attr_set[MODE] = true;
+    }
+    fwd_kernel<MODE><<<n_blocks, pl->threads, pl->smem, st>>>(a);
+    SDRG_CUDA(cudaGetLastError());
+    return SDRG_OK;
+}
+
+template <int R, int MODE>
+static int launch_cons_R(const FftPlan *pl, const ConsArgs &a, int n_tasks, cudaStream_t st)
+{
+    static bool attr_set = false;
+    if (!attr_set) {
+        SDRG_CUDA(cudaFuncSetAttribute(cons_kernel<R, MODE>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(g_smem_limit())));
+        if (R > 1) {
+            SDRG_CUDA(cudaFuncSetAttribute(cons_kernel<R, MODE>,
+                                           cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        }
+        attr_set = true;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(n_tasks * R));
+    cfg.blockDim = dim3(pl->threads);
+    cfg.dynamicSmemBytes = pl->smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = R;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = R > 1 ? 1 : 0;
+    SDRG_CUDA(cudaLaunchKernelEx(&cfg, cons_kernel<R, MODE>, a));
+    return SDRG_OK;
+}
+
+template <int MODE>
+static int launch_cons(const FftPlan *pl, const ConsArgs &a, int n_tasks, cudaStream_t st)
+{
+    switch (pl->R) {
+    case 1: return launch_cons_R<1, MODE>(pl, a, n_tasks, st);
+    case 2: return launch_cons_R<2, MODE>(pl, a, n_tasks, st);
+    case 3: return launch_cons_R<3, MODE>(pl, a, n_tasks, st);
+    case 4: return launch_cons_R<4, MODE>(pl, a, n_tasks, st);
+    case 5: return launch_cons_R<5, MODE>(pl, a, n_tasks, st);
+    case 6: return launch_cons_R<6, MODE>(pl, a, n_tasks, st);
+    case 8: return launch_cons_R<8, MODE>(pl, a, n_tasks, st);
+    default: return set_error(SDRG_ERR_ARG, "unsupported split %d", pl->R);
+    }
+}
+
+static int perm_code(const FftPlan *pl, const float2 *nat, int n_prn, float2 *out,
+                     cudaStream_t st)
+{
+    size_t total = (size_t)n_prn * pl->L;
+    int blocks = (int)((total + 255) / 256);
+    if (blocks > 4096) blocks = 4096;
+    perm_code_kernel<<<blocks, 256, 0, st>>>(nat, pl->kperm_dev, pl->M, pl->R, n_prn, out);
+    SDRG_CUDA(cudaGetLastError());
+    return SDRG_OK;
+}
+
+// reference phase arithmetic (src/sdr_func.c:776-778)
+static inline uint32_t phase_of(double phi)
+{
+    return (uint32_t)((phi - floor(phi)) * 4294967296.0);
+}
+static inline uint32_t step_of(double step)
+{
+    return (uint32_t)(int)(step * 4294967296.0);
+}
+
+// Common body of the drop-in FFT correlator calls. iq_dev holds N mixed
+// samples on the device; code_host is the natural-order conjugated code DFT.
+static int corr_fft_device(const char2 *iq_dev, const sdr_cpx_t *code_host, int N,
+                           sdr_cpx_t *corr_host)
+{
+    const FftPlan *pl = get_plan(N);
+    if (!pl) return tctx().error;
+    Device *dev;
+    int e;
+    if ((e = ensure_device(&dev))) return e;
+    cudaStream_t st;
+    if ((e = thread_stream(&st))) return e;
+    ThreadCtx &c = tctx();
+    const size_t cb = (size_t)N * sizeof(float2);
+    if ((e = c.dev[1].reserve(2 * cb)) || (e = c.dev[2].reserve(cb)) ||
+        (e = c.dev[3].reserve(cb)))
+        return e;
+    c.host[0].pinned = true;
+    if ((e = c.host[0].reserve(cb))) return e;
+    float2 *code_nat = (float2 *)c.dev[1].ptr;
+    float2 *code_perm = code_nat + N;
+    float2 *X = (float2 *)c.dev[2].ptr;
+    float2 *Y = (float2 *)c.dev[3].ptr;
+    memcpy(c.host[0].ptr, code_host, cb);
+    SDRG_CUDA(cudaMemcpyAsync(code_nat, c.host[0].ptr, cb, cudaMemcpyHostToDevice, st));
+    if ((e = perm_code(pl, code_nat, 1, code_perm, st))) return e;
+
+    FwdArgs fa = {};
+    fa.pl = pl->k; fa.tw = pl->tw_dev; fa.ctab = dev->ctab_dev; fa.R = pl->R;
+    fa.n_bin = 1; fa.n_sum = 1; fa.cscale = kCScale; fa.iq = iq_dev; fa.X = X;
+    if ((e = launch_fwd<1>(pl, fa, pl->R, st))) return e;
+
+    ConsArgs ca = {};
+    ca.pl = pl->k; ca.tw = pl->tw_dev; ca.split = pl->split_dev; ca.X = X;
+    ca.code = code_perm; ca.n_prn = 1; ca.n_bin = 1; ca.n_sum = 1; ca.prn0 = 0;
+    ca.scale = 1.0f / N / N; ca.Nmax = N; ca.Y = Y;
+    if ((e = launch_cons<1>(pl, ca, 1, st))) return e;
+    SDRG_CUDA(cudaMemcpyAsync(c.host[0].ptr, Y, cb, cudaMemcpyDeviceToHost, st));
+    SDRG_CUDA(cudaStreamSynchronize(st));
+    memcpy(corr_host, c.host[0].ptr, cb);
+    return SDRG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// batched plan
+// ---------------------------------------------------------------------------
+struct GroupState {
+    sdrg_acq_sig_t sig;
+    const FftPlan *pl;
+    std::vector<float> fds;
+    std::vector<uint32_t> phstep;       // per bin
+    float2 *code = nullptr;             // [n_prn][R][M]
+    float2 *X = nullptr;                // [n_bin][n_sum][R][M]
+    float *P = nullptr;                 // [n_prn][n_bin][Nmax]
+    uint32_t *tab_dev = nullptr;        // phstep | ph0a | ph0b | (int) ix | nsplit
+    uint32_t *tab_host = nullptr;       // pinned mirror
+    size_t tab_words = 0;
+    cudaEvent_t tab_ev = nullptr;       // last upload of tab_host
+    int last_len = -1, last_ix = -1;
+    int res_off = 0;
+};
+
+} // namespace sdrg
+
+struct sdrg_acq_plan {
+    std::vector<sdrg::GroupState> g;
+    int n_res = 0;
+    int64_t cells = 0;
+    // kernel timing (sdrg_acq_profile): event pairs recorded around launches
+    bool prof = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_used;
+};
+
+namespace sdrg {
+
+// device reduction for (group, PRN) peaks, defined in sdrg_peak.cu
+int launch_peaks(const float *P, int n_prn, int M_rows, int Nmax, size_t row_stride,
+                 size_t prn_stride, double T, const float *fds_dev,
+                 sdrg_acq_result_t *res, cudaStream_t st);
+
+static int group_tables(GroupState &G, const int *len_if, const int *ix)
+{
+    const sdrg_acq_sig_t &s = G.sig;
+    const int nb = s.len_fds, ns = s.n_sum;
+    uint32_t *t = G.tab_host;
+    uint32_t *phstep = t, *ph0a = t + nb, *ph0b = t + 2 * nb;
+    int *ixs = (int *)(t + 2 * nb + (size_t)nb * ns);
+    int *nsplit = ixs + ns;
+    const int len = len_if[s.buf];
+    for (int b = 0; b < nb; ++b) {
+        phstep[b] = G.phstep[b];
+        ph0a[b] = 0;   // sdr_search_code mixes with phi = 0 (src/sdr_func.c:673)
+    }
+    for (int k = 0; k < ns; ++k) {
+        long long pos = ((long long)ix[s.buf] + (long long)k * s.N) % len;
+        if (pos < 0) pos += len;
+        ixs[k] = (int)pos;
+        nsplit[k] = (pos + s.L > len) ? (int)(len - pos) : s.L;
+        for (int b = 0; b < nb; ++b) {
+            const double step = (s.fi + (double)G.fds[b]) / s.fs;
+            ph0b[(size_t)b * ns + k] = nsplit[k] < s.L ? phase_of(0.0 + step * nsplit[k]) : 0;
+        }
+    }
+    return SDRG_OK;
+}
+
+static int prof_begin(sdrg_acq_plan *plan, cudaStream_t st, cudaEvent_t *ev)
+{
+    if (!plan->prof) return SDRG_OK;
+    for (int i = 0; i < 2; ++i) {
+        if (plan->ev_pool.empty()) {
+            cudaEvent_t e;
+            SDRG_CUDA(cudaEventCreate(&e));
+            plan->ev_pool.push_back(e);
+        }
+        ev[i] = plan->ev_pool.back();
+        plan->ev_pool.pop_back();
+    }
+    SDRG_CUDA(cudaEventRecord(ev[0], st));
+    return SDRG_OK;
+}
+
+static int prof_end(sdrg_acq_plan *plan, cudaStream_t st, cudaEvent_t *ev, int kind)
+{
+    if (!plan->prof) return SDRG_OK;
+    SDRG_CUDA(cudaEventRecord(ev[1], st));
+    plan->ev_used.push_back({kind, {ev[0], ev[1]}});
+    return SDRG_OK;
+}
+
+} // namespace sdrg
+
+using namespace sdrg;
+
+extern "C" {
+
+int sdrg_acq_profile(sdrg_acq_plan_t *plan, int enable)
+{
+    if (!plan) return set_error(SDRG_ERR_ARG, "sdrg_acq_profile: null plan");
+    plan->prof = enable != 0;
+    return SDRG_OK;
+}
+
+int sdrg_acq_profile_get(sdrg_acq_plan_t *plan, double *ms, int64_t *launches)
+{
+    if (!plan || !ms || !launches) return set_error(SDRG_ERR_ARG, "sdrg_acq_profile_get: null");
+    for (int k = 0; k < 3; ++k) { ms[k] = 0.0; launches[k] = 0; }
+    for (auto &u : plan->ev_used) {
+        SDRG_CUDA(cudaEventSynchronize(u.second.second));
+        float t = 0.0f;
+        SDRG_CUDA(cudaEventElapsedTime(&t, u.second.first, u.second.second));
+        ms[u.first] += t;
+        launches[u.first] += 1;
+        plan->ev_pool.push_back(u.second.first);
+        plan->ev_pool.push_back(u.second.second);
+    }
+    plan->ev_used.clear();
+    return SDRG_OK;
+}
+
+void sdr_corr_fft(const sdr_cpx16_t *IQ, const sdr_cpx_t *code_fft, int N,
+                  sdr_cpx_t *corr)
+{
+    if (N <= 0) return;
+    int e;
+    Device *dev;
+    if ((e = ensure_device(&dev))) { memset(corr, 0, sizeof(sdr_cpx_t) * N); return; }
+    cudaStream_t st;
+    ThreadCtx &c = tctx();
+    if ((e = thread_stream(&st)) || (e = c.dev[0].reserve((size_t)N * 2)) ||
+        ((c.host[1].pinned = true), (e = c.host[1].reserve((size_t)N * 2)))) {
+        memset(corr, 0, sizeof(sdr_cpx_t) * N);
+        return;
+    }
+    memcpy(c.host[1].ptr, IQ, (size_t)N * 2);
+    if (cudaMemcpyAsync(c.dev[0].ptr, c.host[1].ptr, (size_t)N * 2,
+                        cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        corr_fft_device((const char2 *)c.dev[0].ptr, code_fft, N, corr)) {
+        memset(corr, 0, sizeof(sdr_cpx_t) * N);
+    }
+}
+
+void sdr_corr_fft_cpx(const sdr_cpx_t *buff, int len_buff, int ix, int N, double fs,
+                      double fc, double phi, const sdr_cpx_t *code_fft, sdr_cpx_t *corr)
+{
+    if (N <= 0) return;
+    int e;
+    cudaStream_t st;
+    ThreadCtx &c = tctx();
+    if ((e = ensure_device(nullptr)) || (e = thread_stream(&st)) ||
+        (e = c.dev[0].reserve((size_t)N * 2)) ||
+        (e = mix_cpx_device(buff, len_buff, ix, N, fs, fc, phi,
+                                 (char2 *)c.dev[0].ptr, st)) ||
+        (e = corr_fft_device((const char2 *)c.dev[0].ptr, code_fft, N, corr))) {
+        memset(corr, 0, sizeof(sdr_cpx_t) * N);
+    }
+}
+
+void sdr_search_code(const sdr_cpx_t *code_fft, double T, const sdr_buff_t *buff,
+                     int ix, int N, double fs, double fi, const float *fds, int len_fds,
+                     float *P)
+{
+    (void)T;
+    if (N <= 0 || len_fds <= 0) return;
+    if (!buff || !buff->data || ix < 0 || ix >= buff->N || N > buff->N) {
+        set_error(SDRG_ERR_ARG, "sdr_search_code: bad buffer window ix=%d N=%d len=%d", ix, N,
+                  buff ? buff->N : 0);
+        return;
+    }
+    const FftPlan *pl = get_plan(N);
+    if (!pl) return;
+    int e;
+    Device *dev;
+    cudaStream_t st;
+    if ((e = ensure_device(&dev)) || (e = thread_stream(&st))) return;
+    ThreadCtx &c = tctx();
+    const size_t cb = (size_t)N * sizeof(float2);
+    const size_t pb = (size_t)len_fds * N * sizeof(float);
+    const size_t xb = (size_t)len_fds * cb;
+    const size_t tabw = 3 * (size_t)len_fds + 2;
+    for (int i = 0; i < 3; ++i) c.host[i].pinned = true;
+    if ((e = c.dev[0].reserve((size_t)N + 64)) || (e = c.dev[1].reserve(2 * cb)) ||
+        (e = c.dev[2].reserve(xb)) || (e = c.dev[3].reserve(pb)) ||
+        (e = c.dev[4].reserve(tabw * 4)) || (e = c.host[0].reserve(cb)) ||
+        (e = c.host[1].reserve((size_t)N + 16 + tabw * 4)) || (e = c.host[2].reserve(pb)))
+        return;
+    uint8_t *win_h = (uint8_t *)c.host[1].ptr;
+    uint32_t *tab_h = (uint32_t *)(win_h + ((N + 15) / 16) * 16);
+    // window copy with the circular wrap (src/sdr_func.c:829-835)
+    const int n1 = (ix + N <= buff->N) ? N : buff->N - ix;
+    memcpy(win_h, buff->data + ix, (size_t)n1);
+    if (n1 < N) memcpy(win_h + n1, buff->data, (size_t)(N - n1));
+    // tables: phstep[len_fds] | ph0a[len_fds] | ph0b[len_fds] | ix | nsplit
+    uint32_t *phstep = tab_h, *ph0a = tab_h + len_fds, *ph0b = tab_h + 2 * len_fds;
+    int *ixs = (int *)(tab_h + 3 * len_fds), *nsplit = ixs + 1;
+    for (int b = 0; b < len_fds; ++b) {
+        const double step = (fi + (double)fds[b]) / fs;
+        phstep[b] = step_of(step);
+        ph0a[b] = phase_of(0.0);
+        ph0b[b] = n1 < N ? phase_of(0.0 + step * n1) : 0;
+    }
+    ixs[0] = 0;
+    nsplit[0] = n1;
+    uint8_t *win_d = (uint8_t *)c.dev[0].ptr;
+    float2 *code_nat = (float2 *)c.dev[1].ptr, *code_perm = code_nat + N;
+    float2 *X = (float2 *)c.dev[2].ptr;
+    float *P_d = (float *)c.dev[3].ptr;
+    uint32_t *tab_d = (uint32_t *)c.dev[4].ptr;
+    memcpy(c.host[0].ptr, code_fft, cb);
+    memcpy(c.host[2].ptr, P, pb);
+    if (cudaMemcpyAsync(win_d, win_h, (size_t)N, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(tab_d, tab_h, tabw * 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(code_nat, c.host[0].ptr, cb, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(P_d, c.host[2].ptr, pb, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+        cuda_error(cudaGetLastError(), "sdr_search_code H2D");
+        return;
+    }
+    if ((e = perm_code(pl, code_nat, 1, code_perm, st))) return;
+    FwdArgs fa = {};
+    fa.pl = pl->k; fa.tw = pl->tw_dev; fa.ctab = dev->ctab_dev; fa.R = pl->R;
+    fa.n_bin = len_fds; fa.n_sum = 1; fa.cscale = kCScale;
+    fa.buf = win_d; fa.buf_len = N;
+    fa.phstep = tab_d; fa.ph0a = tab_d + len_fds; fa.ph0b = tab_d + 2 * len_fds;
+    fa.ix = (const int *)(tab_d + 3 * len_fds);
+    fa.nsplit = fa.ix + 1;
+    fa.X = X;
+    if ((e = launch_fwd<0>(pl, fa, len_fds * pl->R, st))) return;
+    ConsArgs ca = {};
+    ca.pl = pl->k; ca.tw = pl->tw_dev; ca.split = pl->split_dev; ca.X = X; ca.code = code_perm;
+    ca.n_prn = 1; ca.n_bin = len_fds; ca.n_sum = 1; ca.prn0 = 0;
+    ca.scale = 1.0f / N / N; ca.Nmax = N; ca.prn_stride = 0; ca.bin_stride = N;
+    ca.accumulate = 1; ca.P = P_d;
+    if ((e = launch_cons<0>(pl, ca, len_fds, st))) return;
+    if (cudaMemcpyAsync(c.host[2].ptr, P_d, pb, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+        cuda_error(cudaGetLastError(), "sdr_search_code D2H");
+        return;
+    }
+    memcpy(P, c.host[2].ptr, pb);
+}
+
+// ---- batched --------------------------------------------------------------
+sdrg_acq_plan_t *sdrg_acq_plan_new(const sdrg_acq_sig_t *sigs, int n_sig)
+{
+    if (!sigs || n_sig <= 0) {
+        set_error(SDRG_ERR_ARG, "sdrg_acq_plan_new: no signal groups");
+        return nullptr;
+    }
+    Device *dev;
+    cudaStream_t st;
+    if (ensure_device(&dev) || thread_stream(&st)) return nullptr;
+    sdrg_acq_plan_t *plan = new sdrg_acq_plan_t();
+    plan->g.resize(n_sig);
+    int res_off = 0;
+    for (int gi = 0; gi < n_sig; ++gi) {
+        GroupState &G = plan->g[gi];
+        G.sig = sigs[gi];
+        const sdrg_acq_sig_t &s = G.sig;
+        if (s.L <= 0 || s.N <= 0 || s.Nmax <= 0 || s.Nmax > s.L || s.n_sum <= 0 ||
+            s.n_prn <= 0 || s.len_fds <= 0 || !s.fds || !s.code_fft || s.fs <= 0) {
+            set_error(SDRG_ERR_ARG, "sdrg_acq_plan_new: bad parameters for group %d", gi);
+            sdrg_acq_plan_free(plan);
+            return nullptr;
+        }
+        G.pl = get_plan(s.L);
+        if (!G.pl) { sdrg_acq_plan_free(plan); return nullptr; }
+        G.fds.assign(s.fds, s.fds + s.len_fds);
+        G.sig.fds = nullptr;
+        G.sig.code_fft = nullptr;
+        G.phstep.resize(s.len_fds);
+        for (int b = 0; b < s.len_fds; ++b) G.phstep[b] = step_of((s.fi + (double)G.fds[b]) / s.fs);
+        const size_t L = (size_t)s.L;
+        float2 *nat = nullptr;
+        bool ok = cudaMalloc(&G.code, (size_t)s.n_prn * L * sizeof(float2)) == cudaSuccess &&
+                  cudaMalloc(&nat, (size_t)s.n_prn * L * sizeof(float2)) == cudaSuccess &&
+                  cudaMalloc(&G.X, (size_t)s.len_fds * s.n_sum * L * sizeof(float2)) == cudaSuccess &&
+                  cudaMalloc(&G.P, (size_t)s.n_prn * s.len_fds * s.Nmax * sizeof(float)) == cudaSuccess;
+        G.tab_words = 2 * (size_t)s.len_fds + (size_t)s.len_fds * s.n_sum + 2 * (size_t)s.n_sum + s.len_fds;
+        ok = ok && cudaMalloc(&G.tab_dev, G.tab_words * 4) == cudaSuccess &&
+             cudaMallocHost(&G.tab_host, G.tab_words * 4) == cudaSuccess &&
+             cudaEventCreateWithFlags(&G.tab_ev, cudaEventDisableTiming) == cudaSuccess;
+        ok = ok && cudaMemcpy(nat, sigs[gi].code_fft, (size_t)s.n_prn * L * sizeof(float2),
+                              cudaMemcpyHostToDevice) == cudaSuccess;
+        ok = ok && perm_code(G.pl, nat, s.n_prn, G.code, st) == SDRG_OK &&
+             cudaStreamSynchronize(st) == cudaSuccess;
+        // Doppler bins as float on the device for the fine-Doppler fit
+        if (ok) {
+            float *fd_dev = (float *)(G.tab_dev + G.tab_words - s.len_fds);
+            ok = cudaMemcpy(fd_dev, G.fds.data(), s.len_fds * sizeof(float),
+                            cudaMemcpyHostToDevice) == cudaSuccess;
+        }
+        if (nat) cudaFree(nat);
+        if (!ok) {
+            cuda_error(cudaGetLastError(), "sdrg_acq_plan_new allocation");
+            sdrg_acq_plan_free(plan);
+            return nullptr;
+        }
+        G.res_off = res_off;
+        res_off += s.n_prn;
+        plan->cells += (int64_t)s.n_prn * s.len_fds * s.Nmax;
+    }
+    plan->n_res = res_off;
+    return plan;
+}
+
+void sdrg_acq_plan_free(sdrg_acq_plan_t *plan)
+{
+    if (!plan) return;
+    for (auto ev : plan->ev_pool) cudaEventDestroy(ev);
+    for (auto &u : plan->ev_used) {
+        cudaEventDestroy(u.second.first);
+        cudaEventDestroy(u.second.second);
+    }
+    for (auto &G : plan->g) {
+        if (G.code) cudaFree(G.code);
+        if (G.X) cudaFree(G.X);
+        if (G.P) cudaFree(G.P);
+        if (G.tab_dev) cudaFree(G.tab_dev);
+        if (G.tab_host) cudaFreeHost(G.tab_host);
+        if (G.tab_ev) cudaEventDestroy(G.tab_ev);
+    }
+    delete plan;
+}
+
+int64_t sdrg_acq_plan_cells(const sdrg_acq_plan_t *plan) { return plan ? plan->cells : 0; }
+
+const float *sdrg_acq_grid(const sdrg_acq_plan_t *plan, int g)
+{
+    if (!plan || g < 0 || g >= (int)plan->g.size()) return nullptr;
+    return plan->g[g].P;
+}
+
+int sdrg_acq_grid_host(const sdrg_acq_plan_t *plan, int g, float *dst)
+{
+    if (!plan || g < 0 || g >= (int)plan->g.size() || !dst)
+        return set_error(SDRG_ERR_ARG, "sdrg_acq_grid_host: bad argument");
+    int e;
+    if ((e = ensure_device(nullptr))) return e;
+    const sdrg_acq_sig_t &s = plan->g[g].sig;
+    SDRG_CUDA(cudaDeviceSynchronize());
+    SDRG_CUDA(cudaMemcpy(dst, plan->g[g].P, (size_t)s.n_prn * s.len_fds * s.Nmax * sizeof(float),
+                         cudaMemcpyDeviceToHost));
+    return SDRG_OK;
+}
+
+int sdrg_acq_run(sdrg_acq_plan_t *plan, const uint8_t *const *if_dev, const int *len_if,
+                 const int *ix, sdrg_acq_result_t *res_dev, void *stream)
+{
+    if (!plan || !if_dev || !len_if || !ix || !res_dev)
+        return set_error(SDRG_ERR_ARG, "sdrg_acq_run: null argument");
+    Device *dev;
+    int e;
+    if ((e = ensure_device(&dev))) return e;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!st && (e = thread_stream(&st))) return e;
+    for (auto &G : plan->g) {
+        const sdrg_acq_sig_t &s = G.sig;
+        if (len_if[s.buf] < s.L)
+            return set_error(SDRG_ERR_ARG, "IF buffer %d shorter than L=%d", s.buf, s.L);
+        if (G.last_len != len_if[s.buf] || G.last_ix != ix[s.buf]) {
+            SDRG_CUDA(cudaEventSynchronize(G.tab_ev));   // previous upload done
+            group_tables(G, len_if, ix);
+            SDRG_CUDA(cudaMemcpyAsync(G.tab_dev, G.tab_host, (G.tab_words - s.len_fds) * 4,
+                                      cudaMemcpyHostToDevice, st));
+            SDRG_CUDA(cudaEventRecord(G.tab_ev, st));
+            G.last_len = len_if[s.buf];
+            G.last_ix = ix[s.buf];
+        }
+        const int nb = s.len_fds, ns = s.n_sum;
+        FwdArgs fa = {};
+        fa.pl = G.pl->k; fa.tw = G.pl->tw_dev; fa.ctab = dev->ctab_dev; fa.R = G.pl->R;
+        fa.n_bin = nb; fa.n_sum = ns; fa.cscale = kCScale;
+        fa.buf = if_dev[s.buf]; fa.buf_len = len_if[s.buf];
+        fa.phstep = G.tab_dev; fa.ph0a = G.tab_dev + nb; fa.ph0b = G.tab_dev + 2 * nb;
+        fa.ix = (const int *)(G.tab_dev + 2 * nb + (size_t)nb * ns);
+        fa.nsplit = fa.ix + ns;
+        fa.X = G.X;
+        cudaEvent_t ev[2];
+        if ((e = prof_begin(plan, st, ev))) return e;
+        if ((e = launch_fwd<0>(G.pl, fa, nb * ns * G.pl->R, st))) return e;
+        if ((e = prof_end(plan, st, ev, 0))) return e;
+        ConsArgs ca = {};
+        ca.pl = G.pl->k; ca.tw = G.pl->tw_dev; ca.split = G.pl->split_dev; ca.X = G.X;
+        ca.code = G.code; ca.n_prn = s.n_prn; ca.n_bin = nb; ca.n_sum = ns; ca.prn0 = 0;
+        ca.scale = 1.0f / s.L / s.L; ca.Nmax = s.Nmax;
+        ca.prn_stride = (size_t)nb * s.Nmax; ca.bin_stride = s.Nmax;
+        ca.accumulate = 0; ca.P = G.P;
+        if ((e = prof_begin(plan, st, ev))) return e;
+        if ((e = launch_cons<0>(G.pl, ca, s.n_prn * nb, st))) return e;
+        if ((e = prof_end(plan, st, ev, 1))) return e;
+        const float *fd_dev = (const float *)(G.tab_dev + G.tab_words - nb);
+        if ((e = prof_begin(plan, st, ev))) return e;
+        if ((e = launch_peaks(G.P, s.n_prn, nb, s.Nmax, s.Nmax, (size_t)nb * s.Nmax, s.T,
+                              fd_dev, res_dev + G.res_off, st)))
+            return e;
+        if ((e = prof_end(plan, st, ev, 2))) return e;
+    }
+    return SDRG_OK;
+}
+
+int sdrg_acq_run_host(sdrg_acq_plan_t *plan, const uint8_t *const *if_host, const int *len_if,
+                      const int *ix, sdrg_acq_result_t *res_host)
+{
+    if (!plan || !if_host || !len_if || !ix || !res_host)
+        return set_error(SDRG_ERR_ARG, "sdrg_acq_run_host: null argument");
+    int e;
+    if ((e = ensure_device(nullptr))) return e;
+    cudaStream_t st;
+    if ((e = thread_stream(&st))) return e;
+    int nbuf = 0;
+    for (auto &G : plan->g) nbuf = G.sig.buf + 1 > nbuf ? G.sig.buf + 1 : nbuf;
+    std::vector<uint8_t *> bufs(nbuf, nullptr);
+    sdrg_acq_result_t *res_dev = nullptr;
+    e = SDRG_OK;
+    for (int b = 0; b < nbuf && !e; ++b) {
+        if (cudaMalloc(&bufs[b], len_if[b]) != cudaSuccess ||
+            cudaMemcpyAsync(bufs[b], if_host[b], len_if[b], cudaMemcpyHostToDevice, st) != cudaSuccess)
+            e = cuda_error(cudaGetLastError(), "sdrg_acq_run_host IF upload");
+    }
+    if (!e && cudaMalloc(&res_dev, plan->n_res * sizeof(sdrg_acq_result_t)) != cudaSuccess)
+        e = cuda_error(cudaGetLastError(), "sdrg_acq_run_host result alloc");
+    if (!e) e = sdrg_acq_run(plan, (const uint8_t *const *)bufs.data(), len_if, ix, res_dev, st);
+    if (!e && (cudaMemcpyAsync(res_host, res_dev, plan->n_res * sizeof(sdrg_acq_result_t),
+                               cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess))
+        e = cuda_error(cudaGetLastError(), "sdrg_acq_run_host D2H");
+    cudaStreamSynchronize(st);
+    for (auto p : bufs) if (p) cudaFree(p);
+    if (res_dev) cudaFree(res_dev);
+    return e;
+}
+
+} // extern "C"

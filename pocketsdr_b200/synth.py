@@ -1,0 +1,185 @@
+"""Seeded synthetic IF data and search workloads.
+
+The reference measures on live or recorded front-end data; these generators
+stand in for it with the same sample formats: every sample is one packed
+4+4-bit byte (I low nibble, Q high nibble; Q = 0 for real sampling), values
+quantised to 2-bit {-3,-1,1,3} or 3-bit {-7,...,7} odd levels. Each
+satellite is code * carrier at its IF + Doppler with a carrier-aided code
+Doppler, scaled to its C/N0 against unit-variance Gaussian noise.
+
+Workloads:
+  acq_l1ca_12mhz  - 12 MHz real IF at 3 MHz, 2-bit, 8 visible GPS L1 C/A
+                    satellites; search 32 PRNs x 41 bins (+-5 kHz, 250 Hz) with
+                    4 ms coherent (48,000-sample FFT, replica tiled x4) x 5 sums.
+  acq_multi_24mhz - 24 MHz complex IQ, 3-bit, two RF buffers (L1/E1/B1 band
+                    and L5 band), 10 satellites per signal; search every PRN of
+                    L1CA (1 ms), E1-B (4 ms, BOC(1,1)), B1I (1 ms) and L5-I
+                    (1 ms), zero-padded FFTs of 2N, Doppler bins by
+                    sdr_dop_bins(T, 0, 5000), 20 ms of non-coherent sums.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import codes
+
+CARRIER = {"L1CA": 1575.42e6, "E1B": 1575.42e6, "B1I": 1561.098e6,
+           "L5I": 1176.45e6, "L5Q": 1176.45e6, "L6D": 1278.75e6}
+
+
+@dataclass
+class Sat:
+    sig: str
+    prn: int
+    code_phase: float     # chips at sample 0
+    doppler: float        # Hz
+    phase: float          # cycles at sample 0
+    cn0: float            # dB-Hz
+    buf: int = 0
+
+
+@dataclass
+class Group:
+    """One signal group of a search (one sdrg_acq_sig_t)."""
+    sig: str
+    prns: list
+    fs: float
+    fi: float
+    T: float              # code period = coherent time (s)
+    N: int                # samples per period / sum advance
+    L: int                # FFT length
+    Nmax: int             # code offsets kept
+    n_sum: int
+    fds: np.ndarray       # float32 Doppler bins
+    buf: int = 0
+    tile: int = 1         # replica periods per coherent block
+
+
+@dataclass
+class Workload:
+    name: str
+    fs: float
+    iq: bool
+    bufs: list            # packed uint8 IF buffers
+    groups: list
+    sats: list = field(default_factory=list)
+    ix: list = field(default_factory=list)
+
+    @property
+    def cells(self) -> int:
+        return sum(len(g.prns) * len(g.fds) * g.Nmax for g in self.groups)
+
+
+def dop_bins(T: float, dop: float, max_dop: float) -> np.ndarray:
+    """sdr_dop_bins (src/sdr_func.c:757-769), float32, with the fused
+    multiply-add the reference build uses."""
+    step = np.float32(0.5 / T)
+    n = int(2.0 * max_dop / step) + 1
+    i = np.arange(n, dtype=np.float64)
+    return (i * np.float64(step) + np.float64(np.float32(dop) - np.float32(max_dop))).astype(np.float32)
+
+
+def _quant(x: np.ndarray, bits: int) -> np.ndarray:
+    """Nearest odd level of a mid-rise quantiser: 2-bit step 1 sigma,
+    3-bit step 0.5 sigma, clipped."""
+    step = 1.0 if bits == 2 else 0.5
+    top = (1 << bits) - 1
+    q = 2 * np.floor(x / step) + 1
+    return np.clip(q, -top, top).astype(np.int8)
+
+
+def pack(I: np.ndarray, Q: np.ndarray | None) -> np.ndarray:
+    lo = I.astype(np.uint8) & 0x0F
+    hi = (Q.astype(np.uint8) & 0x0F) << 4 if Q is not None else np.zeros_like(lo)
+    return (hi | lo).astype(np.uint8)
+
+
+def gen_if(n: int, fs: float, fi_of: dict, sats: list, *, iq: bool, bits: int,
+           seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    t = np.arange(n, dtype=np.float64) / fs
+    if iq:
+        x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+        n0 = 2.0 / fs
+    else:
+        x = rng.standard_normal(n).astype(np.complex128)
+        n0 = 2.0 / fs
+    for s in sats:
+        chips = codes.gen_code(s.sig, s.prn).astype(np.float64)
+        L, T = codes.SIGNALS[s.sig]
+        rate = L / T * (1.0 + s.doppler / CARRIER[s.sig])
+        idx = np.floor(s.code_phase + rate * t).astype(np.int64) % L
+        ph = 2 * np.pi * ((fi_of[s.sig] + s.doppler) * t + s.phase)
+        if iq:
+            amp = np.sqrt(10 ** (s.cn0 / 10) * n0)
+            x += amp * chips[idx] * np.exp(1j * ph)
+        else:
+            amp = np.sqrt(2 * 10 ** (s.cn0 / 10) * n0)
+            x += amp * chips[idx] * np.cos(ph)
+    I = _quant(x.real, bits)
+    Q = _quant(x.imag, bits) if iq else None
+    return pack(I, Q)
+
+
+def tiled_code_fft(sig: str, prn: int, fs: float, tile: int, N: int, Nz: int) -> np.ndarray:
+    chips = np.tile(codes.gen_code(sig, prn), tile)
+    T = codes.code_cyc(sig) * tile
+    return codes.gen_code_fft(chips, T, 0.0, fs, N, Nz)
+
+
+def acq_l1ca_12mhz(seed: int = 1) -> Workload:
+    fs, fi, bits = 12e6, 3e6, 2
+    rng = np.random.default_rng(seed)
+    vis = sorted(rng.choice(np.arange(1, 33), 8, replace=False).tolist())
+    sats = [Sat("L1CA", int(p), float(rng.uniform(0, 1023)), float(rng.uniform(-4000, 4000)),
+                float(rng.uniform(0, 1)), float(rng.uniform(38, 48))) for p in vis]
+    N = int(fs * 4e-3)
+    n_sum = 5
+    buf = gen_if(N * n_sum, fs, {"L1CA": fi}, sats, iq=False, bits=bits, seed=seed + 100)
+    fds = np.arange(-5000, 5001, 250, dtype=np.float32)
+    g = Group("L1CA", list(range(1, 33)), fs, fi, 4e-3, N, N, N, n_sum, fds, 0, tile=4)
+    return Workload("acq_l1ca_12mhz", fs, False, [buf], [g], sats, [0])
+
+
+MULTI_SIGS = (("L1CA", 0), ("E1B", 0), ("B1I", 0), ("L5I", 1))
+
+
+def acq_multi_24mhz(seed: int = 2, prn_limit: int | None = None, t_sum: float = 20e-3,
+                    sigs=MULTI_SIGS) -> Workload:
+    """prn_limit / t_sum shrink the search for parity tests."""
+    fs, bits = 24e6, 3
+    fi_of = {"L1CA": 7.161e6, "E1B": 7.161e6, "B1I": -7.161e6, "L5I": 2.0e6}
+    rng = np.random.default_rng(seed)
+    sats, groups = [], []
+    n_buf = max(b for _, b in sigs) + 1
+    n_samp = 0
+    for sig, b in sigs:
+        T = codes.code_cyc(sig)
+        N = int(round(fs * T))
+        n_sum = max(1, int(round(t_sum / T)))
+        n_samp = max(n_samp, N * (n_sum + 1))
+        prns = list(codes.PRN_SETS[sig])
+        if prn_limit:
+            prns = prns[:prn_limit]
+        vis = sorted(rng.choice(prns, min(10, len(prns)), replace=False).tolist())
+        for p in vis:
+            L_code = codes.SIGNALS[sig][0]
+            sats.append(Sat(sig, int(p), float(rng.uniform(0, L_code)), float(rng.uniform(-5000, 5000)),
+                            float(rng.uniform(0, 1)), float(rng.uniform(35, 48)), b))
+        groups.append(Group(sig, prns, fs, fi_of[sig], T, N, 2 * N, N, n_sum,
+                            dop_bins(T, 0.0, 5000.0), b))
+    bufs = []
+    for b in range(n_buf):
+        bsats = [s for s in sats if s.buf == b]
+        bufs.append(gen_if(n_samp, fs, fi_of, bsats, iq=True, bits=bits, seed=seed * 10 + b))
+    return Workload("acq_multi_24mhz", fs, True, bufs, groups, sats, [0] * n_buf)
+
+
+def group_code_ffts(g: Group) -> np.ndarray:
+    """[n_prn, L] complex64 conjugated code DFTs of a group."""
+    out = np.empty((len(g.prns), g.L), np.complex64)
+    for i, p in enumerate(g.prns):
+        out[i] = tiled_code_fft(g.sig, p, g.fs, g.tile, g.N, g.L - g.N)
+    return out

@@ -1,0 +1,247 @@
+"""GPU parity through the C ABI against the oracle and the reference's golden
+vectors.
+
+Bars:
+* mixing and standard correlators: bit-exact (integer stages and the FP32
+  scaling, compared as raw float bits);
+* FFT correlator / search grids (FP32): per cell
+  |GPU - ref| <= 1e-4 * max(|ref|, mean(ref))   (POWER_RTOL below), and
+  for complex correlations |GPU - ref| <= 1e-4 * max(|ref|, rms(ref));
+* peaks (Doppler bin, code offset) identical; C/N0 within 0.1 dB.
+"""
+import numpy as np
+import pytest
+
+from pocketsdr_b200 import codes, synth
+
+pytestmark = pytest.mark.gpu
+
+POWER_RTOL = 1e-4
+CPLX_RTOL = 1e-4
+
+
+def assert_power_close(P, ref):
+    floor = max(float(np.mean(ref)), 0.0)
+    err = np.abs(P.astype(np.float64) - ref)
+    bound = POWER_RTOL * np.maximum(np.abs(ref), floor)
+    bad = err > bound
+    assert not bad.any(), f"{bad.sum()} cells off; worst ratio {np.max(err / np.maximum(bound, 1e-30)):.3g}"
+
+
+def assert_cplx_close(c, ref):
+    rms = float(np.sqrt(np.mean(np.abs(ref) ** 2)))
+    err = np.abs(c.astype(np.complex128) - ref)
+    bound = CPLX_RTOL * np.maximum(np.abs(ref), rms)
+    assert np.all(err <= bound), f"worst ratio {np.max(err / np.maximum(bound, 1e-30)):.3g}"
+
+
+def pack_cpx8(re, im):
+    return ((im & 0x0F) << 4) | (re & 0x0F)
+
+
+# ---- carrier wipe-off -----------------------------------------------------------
+def test_mix_known_answers(gpu):
+    buf = np.array([pack_cpx8(1, -2), pack_cpx8(2, 1), pack_cpx8(-1, 3), pack_cpx8(0, -1)],
+                   np.uint8)
+    assert gpu.sdr_mix_carr(buf, 0, 2, 4.0, 0.0, 0.0).tolist() == [[11, -22], [22, 11]]
+    assert gpu.sdr_mix_carr(buf, 3, 3, 4.0, 0.0, 0.0)[:2].tolist() == [[0, -11], [11, -22]]
+
+
+def test_mix_full_table(gpu, orc):
+    tb = np.repeat(np.arange(256, dtype=np.uint8), 256)
+    assert np.array_equal(gpu.sdr_mix_carr(tb, 0, 65536, 256.0, 1.0, 0.0), orc.mix_table())
+
+
+def test_mix_golden(gpu, golden):
+    g = golden("mix.npz")
+    off = 0
+    for (ix, N, fs, fc, phi), n in zip(g["cases"], g["lens"]):
+        o = gpu.sdr_mix_carr(g["buf"], int(ix), int(N), fs, fc, phi)
+        assert np.array_equal(o, g["out"][off:off + n])
+        off += n
+
+
+def test_mix_random_vs_oracle(gpu, orc):
+    rng = np.random.default_rng(11)
+    for _ in range(40):
+        L = int(rng.integers(100, 300000))
+        N = int(rng.integers(1, L + 1))
+        buf = rng.integers(0, 256, L, dtype=np.uint8)
+        ix = int(rng.integers(0, L))
+        fs = float(rng.uniform(1e6, 48e6))
+        fc = float(rng.uniform(-0.49 * fs, 0.49 * fs))
+        phi = float(rng.uniform(-5, 5))
+        assert np.array_equal(gpu.sdr_mix_carr(buf, ix, N, fs, fc, phi),
+                              orc.mix_carr(buf, ix, N, fs, fc, phi))
+
+
+# ---- standard correlators -------------------------------------------------------
+def test_corr_std_golden(gpu, golden):
+    g = golden("corr_std.npz")
+    for name, cpx in (("real", False), ("cpx", True)):
+        off = 0
+        for k, (coff, n) in enumerate(zip(g["coffs"], g["npos"])):
+            pos = g["pos"][off:off + n]
+            c, Cb = gpu.sdr_corr_std(g["IQ"], g[f"code_{name}"], float(coff), pos, cpx)
+            assert np.array_equal(c.view(np.uint32), g[f"corr_{name}"][off:off + n].view(np.uint32))
+            assert np.array_equal(Cb.view(np.uint32), g[f"C_{name}"][k].view(np.uint32))
+            off += n
+
+
+def test_corr_std_random_vs_oracle(gpu, orc):
+    rng = np.random.default_rng(5)
+    for t in range(40):
+        N = int(rng.integers(16, 30000))
+        IQ = rng.integers(-128, 128, (N, 2), dtype=np.int8)
+        cpx = bool(t % 2)
+        code = (rng.choice(np.array([-1, 0, 1], np.int8), (10 * N, 2)) if cpx else
+                np.repeat(rng.choice(np.array([-1, 1], np.int8), (10 * N, 1)), 2, 1))
+        n = int(rng.integers(3, 108))
+        pos = np.concatenate([[0.0, -3.3, 3.3], rng.uniform(-N, N, n - 3)])
+        coff = float(rng.uniform(0, N))
+        a, A = gpu.sdr_corr_std(IQ, code, coff, pos, cpx)
+        b, B = orc.corr_std(IQ, code, coff, pos, cpx)
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), t
+        assert np.array_equal(A.view(np.uint32), B.view(np.uint32)), t
+
+
+def test_cpx_buffer_golden(gpu, golden):
+    g = golden("cpx_buffer.npz")
+    c = gpu.corr_std(g["buff"], 1700, 2000, 4e6, 1.1e6, 0.25, g["code"], g["pos"])
+    assert np.array_equal(c.view(np.uint32), g["corr_std"].view(np.uint32))
+    f = gpu.corr_fft(g["buff"], 900, 2000, 4e6, -0.7e6, 0.6, g["code_fft"])
+    assert_cplx_close(f, g["corr_fft"])
+
+
+# ---- FFT correlator ----------------------------------------------------------------
+def test_corr_fft_zero_code(gpu):
+    IQ = np.array([[1, 0], [2, -1], [3, -2], [4, -3]], np.int8)
+    assert np.max(np.abs(gpu.sdr_corr_fft(IQ, np.zeros(4, np.complex64)))) <= 1e-6
+
+
+def test_corr_fft_golden(gpu, golden):
+    g = golden("search.npz")
+    assert_cplx_close(gpu.sdr_corr_fft(g["IQm"], g["code_fft"]), g["corr"])
+
+
+@pytest.mark.parametrize("N", [1, 2, 3, 4, 5, 8, 30, 100, 1023 * 0 + 1000, 2000, 4096, 12000,
+                               24000, 25000, 48000, 64000, 96000, 120000, 192000])
+def test_corr_fft_sizes_vs_oracle(gpu, orc, N):
+    rng = np.random.default_rng(N)
+    IQ = rng.integers(-100, 101, (N, 2), dtype=np.int8)
+    cf = (rng.standard_normal(N) + 1j * rng.standard_normal(N)).astype(np.complex64)
+    assert_cplx_close(gpu.sdr_corr_fft(IQ, cf), orc.corr_fft(IQ, cf))
+
+
+# ---- search ----------------------------------------------------------------------------
+def test_search_golden(gpu, golden):
+    g = golden("search.npz")
+    fs, fi, T = g["params"]
+    Ns = int(fs * T)
+    P = np.zeros_like(g["P"])
+    for ix in g["ix"]:
+        gpu.sdr_search_code(g["code_fft"], T, g["ifbuf"], int(ix), 2 * Ns, fs, fi, g["fds"], P)
+    assert_power_close(P, g["P"])
+    cn0, pk = gpu.sdr_corr_max(P, 2 * Ns, Ns, len(g["fds"]), T)
+    assert pk == tuple(g["peak"])
+    assert abs(cn0 - float(g["cn0"])) < 0.1
+    assert abs(gpu.sdr_fine_dop(P, 2 * Ns, g["fds"], pk) - float(g["fd"])) < 0.5
+
+
+def test_search_accumulates(gpu):
+    buf = np.array([pack_cpx8(i + 1, -i) for i in range(4)], np.uint8)
+    P = np.ones((1, 4), np.float32)
+    gpu.sdr_search_code(np.zeros(4, np.complex64), 1.0, buf, 0, 4, 4.0, 0.0,
+                        np.zeros(1, np.float32), P)
+    assert np.allclose(P, 1.0, atol=1e-6)
+
+
+def test_search_helpers_known_answers(gpu):
+    P = np.array([1, 1, 1, 1, 1, 1, 4, 1, 1, 1, 1, 1], np.float32)
+    cn0, ix = gpu.sdr_corr_max(P, 4, 4, 3, 0.001)
+    assert cn0 > 0 and ix == (1, 2)
+    fds = np.array([-500.0, 0.0, 500.0], np.float32)
+    assert abs(gpu.sdr_fine_dop(P, 4, fds, ix)) < 1e-6
+    assert abs(gpu.sdr_fine_dop(P, 4, fds, (0, 0)) + 500.0) < 1e-6
+    assert abs(gpu.sdr_corr_max(np.zeros(4, np.float32), 4, 4, 1, 0.001)[0]) < 1e-6
+    b = gpu.sdr_dop_bins(0.001, 0.0, 1000.0)
+    assert b.tolist() == [-1000.0, -500.0, 0.0, 500.0, 1000.0]
+
+
+def test_dop_bins_golden(gpu):
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "meta.json")) as f:
+        meta = json.load(f)
+    for key, vals in meta["dop_bins"].items():
+        T, d, m = (float(x) for x in key.split("_"))
+        assert gpu.sdr_dop_bins(T, d, m).tolist() == vals
+
+
+def _oracle_group_grid(ref, g, code_fft, buf, ix0):
+    """Reference grid of one PRN: sdr_search_code per sum (N = L), first Nmax
+    columns kept."""
+    P = np.zeros((len(g.fds), g.L), np.float32)
+    for s in range(g.n_sum):
+        ix = (ix0 + s * g.N) % len(buf)
+        ref.search_code(code_fft, buf, ix, g.L, g.fs, g.fi, g.fds, P)
+    return P[:, :g.Nmax]
+
+
+def test_batched_acquisition_vs_oracle(gpu, ref):
+    from pocketsdr_b200.acquire import AcqPlan
+    wl = synth.acq_multi_24mhz(seed=3, prn_limit=3, t_sum=3e-3)
+    cf = [synth.group_code_ffts(g) for g in wl.groups]
+    plan = AcqPlan(wl.groups, cf)
+    res = plan.run_host(wl.bufs, wl.ix)
+    k = 0
+    for g, c in zip(wl.groups, cf):
+        for p in range(len(g.prns)):
+            Pref = _oracle_group_grid(ref, g, c[p], wl.bufs[g.buf], wl.ix[g.buf])
+            cn0, pk = ref.corr_max(Pref, g.Nmax, g.Nmax, len(g.fds), g.T)
+            r = res[k]
+            assert (r["bin"], r["offset"]) == pk, (g.sig, g.prns[p])
+            assert abs(float(r["cn0"]) - cn0) < 0.1
+            k += 1
+
+
+def test_batched_grid_matches_search_code(gpu):
+    """The batched grid equals sdr_search_code accumulated over the sums."""
+    from pocketsdr_b200.acquire import AcqPlan
+    wl = synth.acq_multi_24mhz(seed=4, prn_limit=2, t_sum=2e-3, sigs=(("L1CA", 0),))
+    g = wl.groups[0]
+    cf = synth.group_code_ffts(g)
+    plan = AcqPlan([g], [cf])
+    plan.run_host(wl.bufs, wl.ix)
+    G = plan.grid(0)
+    assert G.shape == (len(g.prns), len(g.fds), g.Nmax)
+    for p in range(len(g.prns)):
+        P = np.zeros((len(g.fds), g.L), np.float32)
+        for s in range(g.n_sum):
+            gpu.sdr_search_code(cf[p], g.T, wl.bufs[0], s * g.N, g.L, g.fs, g.fi, g.fds, P)
+        assert_power_close(G[p], P[:, :g.Nmax])
+
+
+def test_acq_l1ca_12mhz_peaks(gpu, ref):
+    """The 12 MHz real-IF L1 C/A search (4 ms coherent x 5 sums) on the
+    visible PRNs and a few absent ones: identical peaks, C/N0 within 0.1 dB."""
+    from pocketsdr_b200.acquire import AcqPlan
+    wl = synth.acq_l1ca_12mhz(seed=1)
+    g = wl.groups[0]
+    vis = sorted({s.prn for s in wl.sats})
+    absent = [p for p in g.prns if p not in vis][:3]
+    g.prns = vis + absent
+    cf = synth.group_code_ffts(g)
+    plan = AcqPlan([g], [cf])
+    res = plan.run_host(wl.bufs, wl.ix)
+    truth = {s.prn: s for s in wl.sats}
+    for p, prn in enumerate(g.prns):
+        Pref = _oracle_group_grid(ref, g, cf[p], wl.bufs[0], 0)
+        cn0, pk = ref.corr_max(Pref, g.Nmax, g.Nmax, len(g.fds), g.T)
+        r = res[p]
+        assert (r["bin"], r["offset"]) == pk, prn
+        assert abs(float(r["cn0"]) - cn0) < 0.1, prn
+        if prn in truth:
+            s = truth[prn]
+            assert abs(float(g.fds[r["bin"]]) - s.doppler) <= 250.0
+            assert cn0 > 38.0
