@@ -45,11 +45,15 @@ FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12   # 148 SM x 128 FP32 lanes
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", default="acq_multi_24mhz")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--prn-limit", type=int, default=None,
+                    help="fewer PRNs per group (profiling runs)")
+    ap.add_argument("--t-sum", type=float, default=20e-3,
+                    help="non-coherent time per group (s)")
     return ap.parse_args()
 
 
@@ -114,10 +118,10 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-def make_workload(name: str, seed: int):
+def make_workload(name: str, seed: int, prn_limit=None, t_sum=20e-3):
     from pocketsdr_b200 import synth
     if name == "acq_multi_24mhz":
-        return synth.acq_multi_24mhz(seed=seed)
+        return synth.acq_multi_24mhz(seed=seed, prn_limit=prn_limit, t_sum=t_sum)
     if name == "acq_l1ca_12mhz":
         return synth.acq_l1ca_12mhz(seed=seed)
     raise SystemExit(f"unknown workload {name}")
@@ -238,11 +242,12 @@ def run_ours(args):
     from pocketsdr_b200 import acquire, synth
     from pocketsdr_b200._lib import lib
 
-    wl = make_workload(args.workload, 2 + rank)
+    wl = make_workload(args.workload, 2 + rank, args.prn_limit, args.t_sum)
     cfs = [synth.group_code_ffts(g) for g in wl.groups]
     plan = acquire.AcqPlan(wl.groups, cfs)
     cells = plan.cells
-    st = torch.cuda.current_stream()
+    st = torch.cuda.Stream()          # every launch of ours and every event on it
+    torch.cuda.set_stream(st)
     bufs_d = [torch.from_numpy(b).cuda() for b in wl.bufs]
     lens = [len(b) for b in wl.bufs]
     res_d = torch.empty(plan.n_res * acquire.RESULT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
@@ -273,7 +278,9 @@ def run_ours(args):
     if dist:
         dist.barrier()
     step_ms = [a.elapsed_time(b) for a, b in ev]
-    prof = plan.profile_get()
+    prof_g = plan.profile_get(per_group=True)
+    prof = {k: (sum(v[0] for (g, kk), v in prof_g.items() if kk == k),
+                sum(v[1] for (g, kk), v in prof_g.items() if kk == k)) for k in ("fwd", "cons", "peak")}
     plan.profile(False)
     total_ms = sum(step_ms)
     if dist:
@@ -349,7 +356,8 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": sum(n for _, n in prof.values()),
-            "kernel_ms": {k: v[0] / max(v[1], 1) for k, v in prof.items()},
+            "kernel_ms_per_step": {f"{wl.groups[g].sig}.{k}": v[0] / args.steps
+                                   for (g, k), v in prof_g.items()},
             "roofline": roofline, "clocks": clocks,
             "detected": int(sum(1 for r in res if r["cn0"] >= 38.0))}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

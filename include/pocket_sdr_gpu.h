@@ -197,9 +197,10 @@ int sdrg_acq_grid_host(const sdrg_acq_plan_t *plan, int g, float *dst);
 
 /* Kernel timing: when enabled, every sdrg_acq_run records CUDA events on its
  * stream around each kernel launch. sdrg_acq_profile_get waits for them and
- * returns, since the last get, the summed milliseconds and launch counts of
- * the forward-FFT [0], consumer (code multiply + inverse FFT + power) [1] and
- * peak-reduction [2] kernels, then resets. */
+ * returns, since the last get, the summed milliseconds and launch counts per
+ * group g and kernel: index 3*g + 0 forward FFT, 3*g + 1 consumer (code
+ * multiply + inverse FFT + power), 3*g + 2 peak reduction (arrays of
+ * 3 * n_sig entries), then resets. */
 int sdrg_acq_profile(sdrg_acq_plan_t *plan, int enable);
 int sdrg_acq_profile_get(sdrg_acq_plan_t *plan, double *ms, int64_t *launches);
 

@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <map>
 
 #include "sdrg_internal.h"
@@ -83,6 +84,9 @@ int ensure_device(Device **out)
         build_ctab(g_dev.ctab);
         SDRG_CUDA(cudaMalloc(&g_dev.ctab_dev, 512));
         SDRG_CUDA(cudaMemcpy(g_dev.ctab_dev, g_dev.ctab, 512, cudaMemcpyHostToDevice));
+        // a pageable cudaMemcpy may return before its DMA completes, and the
+        // library's kernels run on non-blocking streams: settle it here
+        SDRG_CUDA(cudaDeviceSynchronize());
         g_dev.id = id;
     }
     SDRG_CUDA(cudaSetDevice(g_dev.id));
@@ -188,6 +192,13 @@ bool plan_shape(int L, int *Rout, int *Mout, FftPlanK *kout)
         if (M == 1) best.push_back(1);
         else best_radices(M, cur, best);
         if (best.empty() || (int)best.size() > kMaxPass) continue;
+        // Even radices first (largest first), odd radices last: the last
+        // passes have the smallest strides, and an odd stride of 8-byte
+        // elements spreads a half-warp over all 16 bank pairs.
+        std::stable_sort(best.begin(), best.end(), [](int a, int b) {
+            if ((a & 1) != (b & 1)) return (a & 1) == 0;
+            return a > b;
+        });
         FftPlanK k{};
         k.M = M;
         k.npass = (int)best.size();
@@ -196,11 +207,12 @@ bool plan_shape(int L, int *Rout, int *Mout, FftPlanK *kout)
             k.radix[p] = best[p];
             k.Ls[p] = Ls;
             k.twoff[p] = off;
-            off += Ls / best[p];
+            // pass 0: S entries (powers formed in registers); later passes:
+            // S * (r - 1) entries, every twiddle of the pass
+            off += (p == 0) ? Ls / best[p] : (Ls / best[p]) * (best[p] - 1);
             Ls /= best[p];
         }
-        k.twtot = off;
-        if (M == 1) { k.npass = 0; k.twtot = 0; }
+        k.twtot = off;   // M == 1: one radix-1 pass, one unit twiddle
         if (plan_smem(M, k) > smax) continue;
         *Rout = R;
         *Mout = M;
@@ -227,13 +239,17 @@ static int build_plan(int L, FftPlan *pl)
     while (t < 512 && t * 8 < M) t *= 2;
     pl->threads = t;
     pl->smem = plan_smem(M, k);
-    // per-pass twiddles exp(-2 pi i * i / Ls_p), i < S_p
+    // per-pass twiddles: pass 0 exp(-2 pi i * i / Ls_0), i < S_0; pass p >= 1
+    // exp(-2 pi i * i*j / Ls_p) at (j-1)*S_p + i, j = 1..r_p-1 (double, rounded)
     std::vector<float2> tw(k.twtot > 0 ? k.twtot : 1);
     for (int p = 0; p < k.npass; ++p) {
-        int Ls = k.Ls[p], S = Ls / k.radix[p];
-        for (int i = 0; i < S; ++i) {
-            double a = -2.0 * M_PI * i / Ls;
-            tw[k.twoff[p] + i] = make_float2((float)cos(a), (float)sin(a));
+        int Ls = k.Ls[p], r = k.radix[p], S = Ls / r;
+        int jmax = (p == 0) ? 1 : r - 1;
+        for (int j = 1; j <= jmax; ++j) {
+            for (int i = 0; i < S; ++i) {
+                double a = -2.0 * M_PI * (double)((long)i * j % Ls) / Ls;
+                tw[k.twoff[p] + (j - 1) * S + i] = make_float2((float)cos(a), (float)sin(a));
+            }
         }
     }
     // digit-reversed frequency index of each DIF output position
@@ -263,6 +279,9 @@ static int build_plan(int L, FftPlan *pl)
     SDRG_CUDA(cudaMalloc(&pl->split_dev, M * sizeof(float2)));
     SDRG_CUDA(cudaMemcpy(pl->split_dev, split.data(), M * sizeof(float2),
                          cudaMemcpyHostToDevice));
+    // the plan is used at once by kernels on non-blocking streams, which do
+    // not order after these legacy-stream copies
+    SDRG_CUDA(cudaDeviceSynchronize());
     return SDRG_OK;
 }
 
@@ -323,9 +342,14 @@ int sdrg_fft_supported(int N)
 
 const char *sdrg_version(void) { return "pocketsdr_b200 0.1 (sm_100a)"; }
 
+// When the reference's sdr_func.o is linked with its hot symbols renamed to
+// *_cpu (the integration recipe), its initialiser still sets up the log
+// streams and CPU tables; call it if present.
+void sdr_func_init_cpu(const char *file) __attribute__((weak));
+
 void sdr_func_init(const char *file)
 {
-    (void)file;
+    if (sdr_func_init_cpu) sdr_func_init_cpu(file ? file : "");
     ensure_device(nullptr);
 }
 

@@ -12,8 +12,9 @@
 // Pass p works on sub-sequences of length Ls_p = M / (r_0 ... r_{p-1}); a
 // butterfly reads r_p elements at stride S_p = Ls_p / r_p, so butterflies
 // never overlap and each pass runs in place with one barrier after it.
-// Twiddles: pass p uses w = exp(-2 pi i * i / Ls_p) from a per-pass table of
-// S_p entries in shared memory; w^j for j >= 2 by repeated products.
+// Twiddles: pass 0 uses w = exp(-2 pi i * i / Ls_0) from a table of S_0
+// entries and forms w^j by repeated products; every later pass reads all of
+// its twiddles from a table of S_p * (r_p - 1) entries.
 // Butterfly kernels are compile-time DFTs of size 2,3,4,5 and Cooley-Tukey
 // composites of them (6,8,10,12,15,16) with constant twiddles.
 #pragma once
@@ -199,6 +200,7 @@ struct FftPlanK {
 // Runs fn<R>() for the runtime radix r (instantiates every supported radix).
 #define SDRG_RADIX_DISPATCH(r, CALL)            \
     switch (r) {                                \
+    case 1:  { constexpr int R_ = 1;  CALL; } break;  \
     case 2:  { constexpr int R_ = 2;  CALL; } break;  \
     case 3:  { constexpr int R_ = 3;  CALL; } break;  \
     case 4:  { constexpr int R_ = 4;  CALL; } break;  \
@@ -224,38 +226,69 @@ __device__ __forceinline__ void apply_tw(float2 *v, float2 w1)
     }
 }
 
-// One in-place DIF (forward) pass.
+// Per-thread walk over the butterflies of a pass without a division per
+// butterfly: butterfly b = blk*S + i; the thread starts at b = tid and
+// advances by nthr = dblk*S + di.
+struct BflyWalk {
+    int blk, i, dblk, di, S;
+    __device__ __forceinline__ BflyWalk(int tid, int nthr, int S_) : S(S_)
+    {
+        blk = tid / S; i = tid - blk * S;
+        dblk = nthr / S; di = nthr - dblk * S;
+    }
+    __device__ __forceinline__ void next()
+    {
+        blk += dblk; i += di;
+        if (i >= S) { i -= S; ++blk; }
+    }
+};
+
+// Pass tables for p >= 1 hold every twiddle: twp[(j-1)*S + i] =
+// exp(-2 pi i * i*j / Ls), j = 1..R-1, so consecutive threads read
+// consecutive entries.
+template <int R, bool CONJ>
+__device__ __forceinline__ void apply_tw_table(float2 *v, const float2 *twp, int S, int i)
+{
+#pragma unroll
+    for (int j = 1; j < R; ++j) {
+        const float2 w = twp[(j - 1) * S + i];
+        v[j] = cmul(v[j], CONJ ? cconj(w) : w);
+    }
+}
+
+// One in-place DIF (forward) pass, p >= 1.
 template <int R>
 __device__ __forceinline__ void dif_pass(float2 *sm, int M, int Ls,
                                          const float2 *twp, int tid, int nthr)
 {
     const int S = Ls / R, nb = M / R;
-    for (int b = tid; b < nb; b += nthr) {
-        const int blk = b / S, i = b - blk * S;
-        float2 *p = sm + blk * Ls + i;
+    BflyWalk w(tid, nthr, S);
+    for (int b = tid; b < nb; b += nthr, w.next()) {
+        float2 *p = sm + w.blk * Ls + w.i;
         float2 v[R];
 #pragma unroll
         for (int j = 0; j < R; ++j) v[j] = p[j * S];
         Dft<R, -1>::run(v);
-        if (i) apply_tw<R>(v, twp[i]);
+        apply_tw_table<R, false>(v, twp, S, w.i);
 #pragma unroll
         for (int j = 0; j < R; ++j) p[j * S] = v[j];
     }
 }
 
-// One in-place DIT (inverse) pass: conjugate twiddles, then backward DFT.
+// One in-place DIT (inverse) pass, p >= 1: conjugate twiddles, then the
+// backward DFT.
 template <int R>
 __device__ __forceinline__ void dit_pass(float2 *sm, int M, int Ls,
                                          const float2 *twp, int tid, int nthr)
 {
     const int S = Ls / R, nb = M / R;
-    for (int b = tid; b < nb; b += nthr) {
-        const int blk = b / S, i = b - blk * S;
-        float2 *p = sm + blk * Ls + i;
+    BflyWalk w(tid, nthr, S);
+    for (int b = tid; b < nb; b += nthr, w.next()) {
+        float2 *p = sm + w.blk * Ls + w.i;
         float2 v[R];
 #pragma unroll
         for (int j = 0; j < R; ++j) v[j] = p[j * S];
-        if (i) apply_tw<R>(v, cconj(twp[i]));
+        apply_tw_table<R, true>(v, twp, S, w.i);
         Dft<R, 1>::run(v);
 #pragma unroll
         for (int j = 0; j < R; ++j) p[j * S] = v[j];

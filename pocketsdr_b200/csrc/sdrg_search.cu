@@ -146,7 +146,7 @@ struct ConsArgs {
     const float2 *X;        // [n_bin][n_sum][R][M]
     const float2 *code;     // [n_prn][R][M] permuted conj code DFT
     int n_prn, n_bin, n_sum;
-    int prn0;               // first PRN of this launch (task = prn-major)
+    int prn0;               // first PRN of this launch (tasks are bin-major)
     float scale;            // 1/L^2 as the reference computes it in float
     int Nmax;               // grid columns kept
     size_t prn_stride;      // P stride between PRNs (elements)
@@ -186,10 +186,13 @@ __global__ void __launch_bounds__(512, 1) cons_kernel(ConsArgs a)
     float2 *tw = smem + a.pl.M;
     const int M = a.pl.M;
     const int c = (R > 1) ? (int)(blockIdx.x % R) : 0;
+    // bin-major tasks: the PRNs of one Doppler bin run side by side, so the
+    // bin's forward spectra are fetched from HBM once and then hit in L2
     const int task = blockIdx.x / R;
-    const int prn = a.prn0 + task / a.n_bin;
-    const int b = task % a.n_bin;
-    if (prn >= a.n_prn) return;   // uniform across the cluster
+    const int n_prn_l = a.n_prn - a.prn0;
+    const int prn = a.prn0 + task % n_prn_l;
+    const int b = task / n_prn_l;
+    if (b >= a.n_bin) return;     // uniform across the cluster
 
     load_twiddles(tw, a.tw, a.pl.twtot);
 
@@ -503,7 +506,8 @@ int sdrg_acq_profile(sdrg_acq_plan_t *plan, int enable)
 int sdrg_acq_profile_get(sdrg_acq_plan_t *plan, double *ms, int64_t *launches)
 {
     if (!plan || !ms || !launches) return set_error(SDRG_ERR_ARG, "sdrg_acq_profile_get: null");
-    for (int k = 0; k < 3; ++k) { ms[k] = 0.0; launches[k] = 0; }
+    const int nk = 3 * (int)plan->g.size();
+    for (int k = 0; k < nk; ++k) { ms[k] = 0.0; launches[k] = 0; }
     for (auto &u : plan->ev_used) {
         SDRG_CUDA(cudaEventSynchronize(u.second.second));
         float t = 0.0f;
@@ -678,16 +682,19 @@ sdrg_acq_plan_t *sdrg_acq_plan_new(const sdrg_acq_sig_t *sigs, int n_sig)
         ok = ok && cudaMalloc(&G.tab_dev, G.tab_words * 4) == cudaSuccess &&
              cudaMallocHost(&G.tab_host, G.tab_words * 4) == cudaSuccess &&
              cudaEventCreateWithFlags(&G.tab_ev, cudaEventDisableTiming) == cudaSuccess;
-        ok = ok && cudaMemcpy(nat, sigs[gi].code_fft, (size_t)s.n_prn * L * sizeof(float2),
-                              cudaMemcpyHostToDevice) == cudaSuccess;
-        ok = ok && perm_code(G.pl, nat, s.n_prn, G.code, st) == SDRG_OK &&
-             cudaStreamSynchronize(st) == cudaSuccess;
+        // Uploads are ordered on the thread's (non-blocking) stream: a plain
+        // cudaMemcpy from pageable memory may return before its DMA lands and
+        // runs on the legacy stream, which kernels on `st` do not wait for.
+        ok = ok && cudaMemcpyAsync(nat, sigs[gi].code_fft, (size_t)s.n_prn * L * sizeof(float2),
+                                   cudaMemcpyHostToDevice, st) == cudaSuccess;
+        ok = ok && perm_code(G.pl, nat, s.n_prn, G.code, st) == SDRG_OK;
         // Doppler bins as float on the device for the fine-Doppler fit
         if (ok) {
             float *fd_dev = (float *)(G.tab_dev + G.tab_words - s.len_fds);
-            ok = cudaMemcpy(fd_dev, G.fds.data(), s.len_fds * sizeof(float),
-                            cudaMemcpyHostToDevice) == cudaSuccess;
+            ok = cudaMemcpyAsync(fd_dev, G.fds.data(), s.len_fds * sizeof(float),
+                                 cudaMemcpyHostToDevice, st) == cudaSuccess;
         }
+        ok = ok && cudaStreamSynchronize(st) == cudaSuccess;
         if (nat) cudaFree(nat);
         if (!ok) {
             cuda_error(cudaGetLastError(), "sdrg_acq_plan_new allocation");
@@ -752,7 +759,8 @@ int sdrg_acq_run(sdrg_acq_plan_t *plan, const uint8_t *const *if_dev, const int 
     if ((e = ensure_device(&dev))) return e;
     cudaStream_t st = (cudaStream_t)stream;
     if (!st && (e = thread_stream(&st))) return e;
-    for (auto &G : plan->g) {
+    for (size_t gi = 0; gi < plan->g.size(); ++gi) {
+        GroupState &G = plan->g[gi];
         const sdrg_acq_sig_t &s = G.sig;
         if (len_if[s.buf] < s.L)
             return set_error(SDRG_ERR_ARG, "IF buffer %d shorter than L=%d", s.buf, s.L);
@@ -777,7 +785,7 @@ int sdrg_acq_run(sdrg_acq_plan_t *plan, const uint8_t *const *if_dev, const int 
         cudaEvent_t ev[2];
         if ((e = prof_begin(plan, st, ev))) return e;
         if ((e = launch_fwd<0>(G.pl, fa, nb * ns * G.pl->R, st))) return e;
-        if ((e = prof_end(plan, st, ev, 0))) return e;
+        if ((e = prof_end(plan, st, ev, 3 * (int)gi + 0))) return e;
         ConsArgs ca = {};
         ca.pl = G.pl->k; ca.tw = G.pl->tw_dev; ca.split = G.pl->split_dev; ca.X = G.X;
         ca.code = G.code; ca.n_prn = s.n_prn; ca.n_bin = nb; ca.n_sum = ns; ca.prn0 = 0;
@@ -786,13 +794,13 @@ int sdrg_acq_run(sdrg_acq_plan_t *plan, const uint8_t *const *if_dev, const int 
         ca.accumulate = 0; ca.P = G.P;
         if ((e = prof_begin(plan, st, ev))) return e;
         if ((e = launch_cons<0>(G.pl, ca, s.n_prn * nb, st))) return e;
-        if ((e = prof_end(plan, st, ev, 1))) return e;
+        if ((e = prof_end(plan, st, ev, 3 * (int)gi + 1))) return e;
         const float *fd_dev = (const float *)(G.tab_dev + G.tab_words - nb);
         if ((e = prof_begin(plan, st, ev))) return e;
         if ((e = launch_peaks(G.P, s.n_prn, nb, s.Nmax, s.Nmax, (size_t)nb * s.Nmax, s.T,
                               fd_dev, res_dev + G.res_off, st)))
             return e;
-        if ((e = prof_end(plan, st, ev, 2))) return e;
+        if ((e = prof_end(plan, st, ev, 3 * (int)gi + 2))) return e;
     }
     return SDRG_OK;
 }
