@@ -141,6 +141,30 @@ int sdrg_fft_supported(int N);
 /* Library version string. */
 const char *sdrg_version(void);
 
+/* ---- FFT correlator that allocates nothing --------------------------------
+ * No counterpart in the reference (an addition of this library).
+ * Same result as sdr_corr_fft (corr = IFFT(FFT(IQ * CSCALE) * code_fft / N^2))
+ * but for callers that cannot allocate device memory when they call: code
+ * running inside a CUDA stream capture, real-time receiver threads that must
+ * not hit cudaMalloc's implicit device synchronisation, or hosts whose memory
+ * comes from their own pool. Inputs and output are DEVICE pointers owned by
+ * the caller (IQ_dev: N mixed samples, code_fft_dev: N conjugated code-DFT
+ * values in natural order, corr_dev: N outputs); `stream` is a cudaStream_t
+ * (NULL = the legacy default stream); the call is asynchronous on it.
+ * All intermediate data (permuted code DFT, forward spectrum, FFT tables)
+ * live in one fixed device array of about 1.8 MB that every GPU loading the
+ * library holds until the process exits; N above SDRG_NOALLOC_MAX_N, or a
+ * length whose FFT plan does not fit that array, is rejected with
+ * SDRG_ERR_ARG. The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture. Every call shares the array and leaves its contents behind: calls
+ * that overlap on the GPU (other streams, other threads) race and must be
+ * serialised by the caller. Nothing needs clearing between calls (each call
+ * overwrites all it reads). Returns SDRG_OK or a negative status. */
+#define SDRG_NOALLOC_MAX_N 65536
+int sdrg_corr_fft_noalloc(const sdr_cpx16_t *IQ_dev, const sdr_cpx_t *code_fft_dev,
+    int N, sdr_cpx_t *corr_dev, void *stream);
+
 /* ---- batched parallel-code-phase acquisition ----------------------------
  * One signal group = one code family at one sampling setup: all its PRNs
  * share L, fs, fi, Doppler bins and sums, so the forward FFT of every

@@ -838,3 +838,131 @@ int sdrg_acq_run_host(sdrg_acq_plan_t *plan, const uint8_t *const *if_host, cons
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// FFT correlator that allocates nothing (sdrg_corr_fft_noalloc)
+// ---------------------------------------------------------------------------
+namespace sdrg {
+
+// Largest sub-transform held by one CTA, and the fixed scratch layout:
+// permuted code DFT (N) | forward spectrum (N) | twiddles (2 * kNaMaxM) |
+// digit-reversal map (kNaMaxM ints) | split twiddles (kNaMaxM).
+constexpr int kNaMaxN = SDRG_NOALLOC_MAX_N;
+constexpr int kNaMaxM = 28672;
+constexpr size_t kNaCode = 0;
+constexpr size_t kNaX = kNaCode + (size_t)kNaMaxN * sizeof(float2);
+constexpr size_t kNaTw = kNaX + (size_t)kNaMaxN * sizeof(float2);
+constexpr size_t kNaKperm = kNaTw + (size_t)2 * kNaMaxM * sizeof(float2);
+constexpr size_t kNaSplit = kNaKperm + (size_t)kNaMaxM * sizeof(int);
+constexpr size_t kNaBytes = kNaSplit + (size_t)kNaMaxM * sizeof(float2);
+
+// Every GPU that loads the library holds this array until the process exits.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+struct NoallocDev {
+    unsigned char *base = nullptr;   // device address of g_noalloc_scratch
+    int N = 0;                       // length whose tables the array holds
+    FftPlan pl;                      // plan whose pointers point into it
+};
+static std::mutex g_na_mtx;
+static NoallocDev g_na[64];
+// host staging for the tables (static, guarded by g_na_mtx: no heap use)
+static float2 g_na_tw_h[2 * kNaMaxM];
+static int g_na_kperm_h[kNaMaxM];
+static float2 g_na_split_h[kNaMaxM];
+
+// Host-side tables of a length-N plan (same construction as get_plan's) into
+// the static staging arrays, without touching device memory.
+static int noalloc_tables(int N, FftPlan *pl)
+{
+    int R, M;
+    FftPlanK k;
+    if (!plan_shape(N, &R, &M, &k) || M > kNaMaxM || k.twtot > 2 * kNaMaxM)
+        return set_error(SDRG_ERR_ARG, "sdrg_corr_fft_noalloc: length %d has no plan "
+                         "within the fixed scratch", N);
+    pl->L = N; pl->R = R; pl->M = M; pl->k = k;
+    int t = 32;
+    while (t < 512 && t * 8 < M) t *= 2;
+    pl->threads = t;
+    pl->smem = (size_t)M * sizeof(float2) + (size_t)k.twtot * sizeof(float2) + 512;
+    float2 *tw = g_na_tw_h;
+    int *kperm = g_na_kperm_h;
+    float2 *split = g_na_split_h;
+    for (int p = 0; p < k.npass; ++p) {
+        const int Ls = k.Ls[p], r = k.radix[p], S = Ls / r, jmax = (p == 0) ? 1 : r - 1;
+        for (int j = 1; j <= jmax; ++j)
+            for (int i = 0; i < S; ++i) {
+                const double a = -2.0 * M_PI * (double)((long)i * j % Ls) / Ls;
+                tw[k.twoff[p] + (j - 1) * S + i] = make_float2((float)cos(a), (float)sin(a));
+            }
+    }
+    for (int q = 0; q < M; ++q) {
+        int rem = q, blk = M, kk = 0, mul = 1;
+        for (int p = 0; p < k.npass; ++p) {
+            blk /= k.radix[p];
+            const int j = rem / blk;
+            rem %= blk;
+            kk += j * mul;
+            mul *= k.radix[p];
+        }
+        kperm[q] = kk;
+        const double a = 2.0 * M_PI * (double)kk / N;
+        split[q] = make_float2((float)cos(a), (float)sin(a));
+    }
+    return SDRG_OK;
+}
+
+} // namespace sdrg
+
+extern "C" int sdrg_corr_fft_noalloc(const sdr_cpx16_t *IQ_dev, const sdr_cpx_t *code_fft_dev,
+                                     int N, sdr_cpx_t *corr_dev, void *stream)
+{
+    if (N <= 0 || N > kNaMaxN)
+        return set_error(SDRG_ERR_ARG, "sdrg_corr_fft_noalloc: N=%d outside 1..%d", N, kNaMaxN);
+    if (!IQ_dev || !code_fft_dev || !corr_dev)
+        return set_error(SDRG_ERR_ARG, "sdrg_corr_fft_noalloc: null pointer");
+    cudaStream_t st = (cudaStream_t)stream;
+    int dev = 0;
+    SDRG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return set_error(SDRG_ERR_ARG, "device %d out of range", dev);
+    std::lock_guard<std::mutex> lk(g_na_mtx);
+    NoallocDev &S = g_na[dev];
+    if (!S.base) {
+        // set-up, once per device, with that device current
+        void *p = nullptr;
+        SDRG_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        S.base = (unsigned char *)p;
+    }
+    if (S.N != N) {
+        int e;
+        S.N = 0;
+        if ((e = noalloc_tables(N, &S.pl))) return e;
+        S.pl.tw_dev = (float2 *)(S.base + kNaTw);
+        S.pl.kperm_dev = (int *)(S.base + kNaKperm);
+        S.pl.split_dev = (float2 *)(S.base + kNaSplit);
+        const int M = S.pl.M, ntw = S.pl.k.twtot > 0 ? S.pl.k.twtot : 1;
+        // stream-ordered uploads from pageable memory: each call returns once
+        // the host data is staged, so the staging arrays may be reused
+        SDRG_CUDA(cudaMemcpyAsync(S.pl.tw_dev, g_na_tw_h, ntw * sizeof(float2),
+                                  cudaMemcpyHostToDevice, st));
+        SDRG_CUDA(cudaMemcpyAsync(S.pl.kperm_dev, g_na_kperm_h, M * sizeof(int),
+                                  cudaMemcpyHostToDevice, st));
+        SDRG_CUDA(cudaMemcpyAsync(S.pl.split_dev, g_na_split_h, M * sizeof(float2),
+                                  cudaMemcpyHostToDevice, st));
+        S.N = N;
+    }
+    const FftPlan *pl = &S.pl;
+    float2 *code_perm = (float2 *)(S.base + kNaCode);
+    float2 *X = (float2 *)(S.base + kNaX);
+    int e;
+    if ((e = perm_code(pl, (const float2 *)code_fft_dev, 1, code_perm, st))) return e;
+    FwdArgs fa = {};
+    fa.pl = pl->k; fa.tw = pl->tw_dev; fa.ctab = nullptr; fa.R = pl->R;
+    fa.n_bin = 1; fa.n_sum = 1; fa.cscale = kCScale; fa.iq = (const char2 *)IQ_dev; fa.X = X;
+    if ((e = launch_fwd<1>(pl, fa, pl->R, st))) return e;
+    ConsArgs ca = {};
+    ca.pl = pl->k; ca.tw = pl->tw_dev; ca.split = pl->split_dev; ca.X = X;
+    ca.code = code_perm; ca.n_prn = 1; ca.n_bin = 1; ca.n_sum = 1; ca.prn0 = 0;
+    ca.scale = 1.0f / N / N; ca.Nmax = N; ca.Y = (float2 *)corr_dev;
+    return launch_cons<1>(pl, ca, 1, st);
+}
