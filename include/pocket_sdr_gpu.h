@@ -223,8 +223,11 @@ int sdrg_acq_grid_host(const sdrg_acq_plan_t *plan, int g, float *dst);
  * stream around each kernel launch. sdrg_acq_profile_get waits for them and
  * returns, since the last get, the summed milliseconds and launch counts per
  * group g and kernel: index 3*g + 0 forward FFT, 3*g + 1 consumer (code
- * multiply + inverse FFT + power), 3*g + 2 peak reduction (arrays of
- * 3 * n_sig entries), then resets. */
+ * multiply + inverse FFT + power), 3*g + 2 peak reduction; then, at
+ * 3*n_sig + k, the per-run span of kernel kind k over all groups (earliest
+ * start to latest end; groups run concurrently on internal streams) summed
+ * over runs, with the number of runs. Arrays hold 3*n_sig + 3 entries.
+ * Resets after reading. */
 int sdrg_acq_profile(sdrg_acq_plan_t *plan, int enable);
 int sdrg_acq_profile_get(sdrg_acq_plan_t *plan, double *ms, int64_t *launches);
 

@@ -95,21 +95,22 @@ class AcqPlan:
         if lib.sdrg_acq_profile(self.handle, int(enable)):
             check("sdrg_acq_profile")
 
-    def profile_get(self, per_group: bool = False) -> dict:
-        """Summed kernel milliseconds and launch counts since the last call:
-        {'fwd': (ms, n), 'cons': (ms, n), 'peak': (ms, n)}; with per_group,
-        {(group, kind): (ms, n)}."""
+    def profile_get(self) -> dict:
+        """Kernel timing since the last call: {(group, kind): (ms, launches)}
+        per launch family, and {('span', kind): (ms, runs)}, the per-run span
+        of each kind over all (concurrent) groups; kind in fwd, cons, peak."""
         ng = len(self.groups)
-        ms = np.zeros(3 * ng, np.float64)
-        n = np.zeros(3 * ng, np.int64)
+        ms = np.zeros(3 * ng + 3, np.float64)
+        n = np.zeros(3 * ng + 3, np.int64)
         if lib.sdrg_acq_profile_get(self.handle, C.c_void_p(ms.ctypes.data),
                                     C.c_void_p(n.ctypes.data)):
             check("sdrg_acq_profile_get")
         kinds = ("fwd", "cons", "peak")
-        if per_group:
-            return {(g, kinds[k]): (float(ms[3 * g + k]), int(n[3 * g + k]))
-                    for g in range(ng) for k in range(3)}
-        return {kinds[k]: (float(ms[k::3].sum()), int(n[k::3].sum())) for k in range(3)}
+        out = {(g, kinds[k]): (float(ms[3 * g + k]), int(n[3 * g + k]))
+               for g in range(ng) for k in range(3)}
+        out.update({("span", kinds[k]): (float(ms[3 * ng + k]), int(n[3 * ng + k]))
+                    for k in range(3)})
+        return out
 
     def close(self) -> None:
         if getattr(self, "handle", None):

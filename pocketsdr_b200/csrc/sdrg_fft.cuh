@@ -256,43 +256,74 @@ __device__ __forceinline__ void apply_tw_table(float2 *v, const float2 *twp, int
     }
 }
 
-// One in-place DIF (forward) pass, p >= 1.
-template <int R>
-__device__ __forceinline__ void dif_pass(float2 *sm, int M, int Ls,
-                                         const float2 *twp, int tid, int nthr)
+// One in-place inner pass (p >= 1): DIF forward (FWD: DFT, then twiddles) or
+// DIT inverse (conjugate twiddles, then backward DFT). Radices up to 10 take
+// two butterflies per iteration (loads of both issued before either DFT) for
+// instruction-level parallelism; a pass with stride 1 has unit twiddles.
+template <int R, bool FWD>
+__device__ __forceinline__ void bfly_inner(float2 *v, const float2 *twp, int S, int i)
 {
+    if (FWD) {
+        Dft<R, -1>::run(v);
+        if (S > 1) apply_tw_table<R, false>(v, twp, S, i);
+    } else {
+        if (S > 1) apply_tw_table<R, true>(v, twp, S, i);
+        Dft<R, 1>::run(v);
+    }
+}
+
+template <int R, bool FWD>
+__device__ __forceinline__ void inner_pass(float2 *sm, int M, int Ls, const float2 *twp,
+                                           int tid, int nthr)
+{
+    constexpr int U = R <= 10 ? 2 : 1;
     const int S = Ls / R, nb = M / R;
     BflyWalk w(tid, nthr, S);
-    for (int b = tid; b < nb; b += nthr, w.next()) {
-        float2 *p = sm + w.blk * Ls + w.i;
+    int b = tid;
+    for (; b + (U - 1) * nthr < nb; b += U * nthr) {
+        float2 v[U][R];
+        float2 *p[U];
+        int ii[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            p[u] = sm + w.blk * Ls + w.i;
+            ii[u] = w.i;
+            w.next();
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int j = 0; j < R; ++j) v[u][j] = p[u][j * S];
+#pragma unroll
+        for (int u = 0; u < U; ++u) bfly_inner<R, FWD>(v[u], twp, S, ii[u]);
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int j = 0; j < R; ++j) p[u][j * S] = v[u][j];
+    }
+    for (; b < nb; b += nthr, w.next()) {
         float2 v[R];
+        float2 *p = sm + w.blk * Ls + w.i;
 #pragma unroll
         for (int j = 0; j < R; ++j) v[j] = p[j * S];
-        Dft<R, -1>::run(v);
-        apply_tw_table<R, false>(v, twp, S, w.i);
+        bfly_inner<R, FWD>(v, twp, S, w.i);
 #pragma unroll
         for (int j = 0; j < R; ++j) p[j * S] = v[j];
     }
 }
 
-// One in-place DIT (inverse) pass, p >= 1: conjugate twiddles, then the
-// backward DFT.
 template <int R>
-__device__ __forceinline__ void dit_pass(float2 *sm, int M, int Ls,
-                                         const float2 *twp, int tid, int nthr)
+__device__ __forceinline__ void dif_pass(float2 *sm, int M, int Ls, const float2 *twp,
+                                         int tid, int nthr)
 {
-    const int S = Ls / R, nb = M / R;
-    BflyWalk w(tid, nthr, S);
-    for (int b = tid; b < nb; b += nthr, w.next()) {
-        float2 *p = sm + w.blk * Ls + w.i;
-        float2 v[R];
-#pragma unroll
-        for (int j = 0; j < R; ++j) v[j] = p[j * S];
-        apply_tw_table<R, true>(v, twp, S, w.i);
-        Dft<R, 1>::run(v);
-#pragma unroll
-        for (int j = 0; j < R; ++j) p[j * S] = v[j];
-    }
+    inner_pass<R, true>(sm, M, Ls, twp, tid, nthr);
+}
+
+template <int R>
+__device__ __forceinline__ void dit_pass(float2 *sm, int M, int Ls, const float2 *twp,
+                                         int tid, int nthr)
+{
+    inner_pass<R, false>(sm, M, Ls, twp, tid, nthr);
 }
 
 // First DIF pass fused with the input: element m comes from load(m).
@@ -313,7 +344,9 @@ __device__ __forceinline__ void dif_pass0_load(float2 *sm, int M,
     }
 }
 
-// Last DIT pass fused with the output: store(m, y_m) for natural index m.
+// Last DIT pass fused with the output: store(m, y_m, old_m) for natural
+// index m, where old_m = store.pre(m) is fetched before the butterfly so a
+// global read-modify-write overlaps the shared-memory work.
 template <int R, class Store>
 __device__ __forceinline__ void dit_pass0_store(const float2 *sm, int M,
                                                 const float2 *twp, Store &store,
@@ -321,13 +354,16 @@ __device__ __forceinline__ void dit_pass0_store(const float2 *sm, int M,
 {
     const int S = M / R;
     for (int i = tid; i < S; i += nthr) {
+        typename Store::Old old[R];
+#pragma unroll
+        for (int j = 0; j < R; ++j) old[j] = store.pre(i + j * S);
         float2 v[R];
 #pragma unroll
         for (int j = 0; j < R; ++j) v[j] = sm[i + j * S];
         if (i) apply_tw<R>(v, cconj(twp[i]));
         Dft<R, 1>::run(v);
 #pragma unroll
-        for (int j = 0; j < R; ++j) store(i + j * S, v[j]);
+        for (int j = 0; j < R; ++j) store(i + j * S, v[j], old[j]);
     }
 }
 

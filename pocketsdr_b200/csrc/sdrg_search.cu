@@ -158,24 +158,32 @@ struct ConsArgs {
 
 template <int R>
 struct StorePower {
+    typedef float Old;
     float *row;       // P for this (prn, bin)
     int c, Nmax;
     bool add;
-    __device__ __forceinline__ void operator()(int m, float2 y) const
+    __device__ __forceinline__ float pre(int m) const
+    {
+        const int n = R * m + c;
+        return (add && n < Nmax) ? row[n] : 0.0f;
+    }
+    __device__ __forceinline__ void operator()(int m, float2 y, float old) const
     {
         const int n = R * m + c;
         if (n < Nmax) {
             const float pw = y.x * y.x + y.y * y.y;
-            row[n] = add ? row[n] + pw : pw;
+            row[n] = add ? old + pw : pw;
         }
     }
 };
 
 template <int R>
 struct StoreComplex {
+    typedef int Old;
     float2 *row;
     int c;
-    __device__ __forceinline__ void operator()(int m, float2 y) const { row[R * m + c] = y; }
+    __device__ __forceinline__ int pre(int) const { return 0; }
+    __device__ __forceinline__ void operator()(int m, float2 y, int) const { row[R * m + c] = y; }
 };
 
 template <int R, int MODE>
@@ -212,36 +220,58 @@ __global__ void __launch_bounds__(512, 1) cons_kernel(ConsArgs a)
         // all CTAs of the cluster are done with their shared memory
         if constexpr (R > 1) cg::this_cluster().sync(); else __syncthreads();
         const float2 *Xs = a.X + ((size_t)b * a.n_sum + s) * R * M;
-        for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
-            float2 g[R];
-            if constexpr (R == 1) {
-                const float2 z = cmul(Xs[q], code[q]);
-                dst[0][q] = make_float2(z.x * a.scale, z.y * a.scale);
-            } else {
-                const float2 t = a.split[q];
-                const float2 tc = cconj(t);
-                g[0] = Xs[q];
-                float2 w = tc;
+        // U positions per iteration: all their global loads are issued
+        // before any arithmetic or (remote) shared-memory store
+        constexpr int U = R <= 4 ? 2 : 1;
+        const int qstep = U * blockDim.x;
+        for (int q = q0 + threadIdx.x; q < q1; q += qstep) {
+            float2 xs[U][R], cs[U][R], ts[U];
+            bool ok[U];
 #pragma unroll
-                for (int r = 1; r < R; ++r) {
-                    g[r] = cmul(Xs[(size_t)r * M + q], w);
-                    if (r + 1 < R) w = cmul(w, tc);
+            for (int u = 0; u < U; ++u) {
+                const int qq = q + u * blockDim.x;
+                ok[u] = qq < q1;
+                const int ql = ok[u] ? qq : q;
+                ts[u] = R > 1 ? __ldg(a.split + ql) : make_float2(1.0f, 0.0f);
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    xs[u][r] = __ldg(Xs + (size_t)r * M + ql);
+                    cs[u][r] = __ldg(code + (size_t)r * M + ql);
                 }
-                Dft<R, -1>::run(g);                 // X[k + jM]
+            }
 #pragma unroll
-                for (int j = 0; j < R; ++j) {
-                    const float2 z = cmul(g[j], code[(size_t)j * M + q]);
-                    g[j] = make_float2(z.x * a.scale, z.y * a.scale);
+            for (int u = 0; u < U; ++u) {
+                if (!ok[u]) continue;
+                const int qq = q + u * blockDim.x;
+                float2 *g = xs[u];
+                if constexpr (R == 1) {
+                    const float2 z = cmul(g[0], cs[u][0]);
+                    dst[0][qq] = make_float2(z.x * a.scale, z.y * a.scale);
+                } else {
+                    const float2 t = ts[u];
+                    const float2 tc = cconj(t);
+                    float2 w = tc;
+#pragma unroll
+                    for (int r = 1; r < R; ++r) {
+                        g[r] = cmul(g[r], w);
+                        if (r + 1 < R) w = cmul(w, tc);
+                    }
+                    Dft<R, -1>::run(g);                 // X[k + jM]
+#pragma unroll
+                    for (int j = 0; j < R; ++j) {
+                        const float2 z = cmul(g[j], cs[u][j]);
+                        g[j] = make_float2(z.x * a.scale, z.y * a.scale);
+                    }
+                    Dft<R, 1>::run(g);                  // sum_j Z e^{+2 pi i c j/R}
+                    w = t;
+#pragma unroll
+                    for (int j = 1; j < R; ++j) {
+                        g[j] = cmul(g[j], w);
+                        if (j + 1 < R) w = cmul(w, t);
+                    }
+#pragma unroll
+                    for (int j = 0; j < R; ++j) dst[j][qq] = g[j];
                 }
-                Dft<R, 1>::run(g);                  // sum_j Z e^{+2 pi i c j/R}
-                w = t;
-#pragma unroll
-                for (int j = 1; j < R; ++j) {
-                    g[j] = cmul(g[j], w);
-                    if (j + 1 < R) w = cmul(w, t);
-                }
-#pragma unroll
-                for (int j = 0; j < R; ++j) dst[j][q] = g[j];
             }
         }
         if constexpr (R > 1) cg::this_cluster().sync(); else __syncthreads();
@@ -427,10 +457,18 @@ struct sdrg_acq_plan {
     std::vector<sdrg::GroupState> g;
     int n_res = 0;
     int64_t cells = 0;
+    // Signal groups run concurrently on internal streams forked from and
+    // joined back to the caller's stream: a group whose clusters cannot use
+    // every SM (8-CTA clusters fit 120 of 148) leaves room for the others.
+    std::vector<cudaStream_t> streams;
+    cudaEvent_t ev_fork = nullptr;
+    std::vector<cudaEvent_t> ev_join;
     // kernel timing (sdrg_acq_profile): event pairs recorded around launches
+    struct Rec { int kind, run; cudaEvent_t a, b; };
     bool prof = false;
+    int run = 0;
     std::vector<cudaEvent_t> ev_pool;
-    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_used;
+    std::vector<Rec> ev_used;
 };
 
 namespace sdrg {
@@ -486,7 +524,7 @@ static int prof_end(sdrg_acq_plan *plan, cudaStream_t st, cudaEvent_t *ev, int k
 {
     if (!plan->prof) return SDRG_OK;
     SDRG_CUDA(cudaEventRecord(ev[1], st));
-    plan->ev_used.push_back({kind, {ev[0], ev[1]}});
+    plan->ev_used.push_back({kind, plan->run, ev[0], ev[1]});
     return SDRG_OK;
 }
 
@@ -506,16 +544,41 @@ int sdrg_acq_profile(sdrg_acq_plan_t *plan, int enable)
 int sdrg_acq_profile_get(sdrg_acq_plan_t *plan, double *ms, int64_t *launches)
 {
     if (!plan || !ms || !launches) return set_error(SDRG_ERR_ARG, "sdrg_acq_profile_get: null");
-    const int nk = 3 * (int)plan->g.size();
-    for (int k = 0; k < nk; ++k) { ms[k] = 0.0; launches[k] = 0; }
+    const int ng = (int)plan->g.size(), nk = 3 * ng;
+    for (int k = 0; k < nk + 3; ++k) { ms[k] = 0.0; launches[k] = 0; }
+    // per-run union span of each kernel kind (launches of different groups
+    // overlap on the internal streams): [earliest start, latest end]
+    std::vector<double> lo(3), hi(3);
+    int cur = -1;
+    cudaEvent_t ref = nullptr;
+    auto flush = [&]() {
+        for (int k = 0; k < 3; ++k)
+            if (hi[k] > lo[k]) { ms[nk + k] += hi[k] - lo[k]; launches[nk + k] += 1; }
+    };
     for (auto &u : plan->ev_used) {
-        SDRG_CUDA(cudaEventSynchronize(u.second.second));
-        float t = 0.0f;
-        SDRG_CUDA(cudaEventElapsedTime(&t, u.second.first, u.second.second));
-        ms[u.first] += t;
-        launches[u.first] += 1;
-        plan->ev_pool.push_back(u.second.first);
-        plan->ev_pool.push_back(u.second.second);
+        SDRG_CUDA(cudaEventSynchronize(u.b));
+        if (u.kind < 0) {   // reference event of a run, recorded before the fork
+            if (cur >= 0) flush();
+            cur = u.run;
+            ref = u.a;
+            for (int k = 0; k < 3; ++k) { lo[k] = 1e300; hi[k] = -1e300; }
+            continue;
+        }
+        float t = 0.0f, t0 = 0.0f, t1 = 0.0f;
+        SDRG_CUDA(cudaEventElapsedTime(&t, u.a, u.b));
+        ms[u.kind] += t;
+        launches[u.kind] += 1;
+        if (!ref) continue;
+        SDRG_CUDA(cudaEventElapsedTime(&t0, ref, u.a));
+        SDRG_CUDA(cudaEventElapsedTime(&t1, ref, u.b));
+        const int k = u.kind % 3;
+        lo[k] = t0 < lo[k] ? t0 : lo[k];
+        hi[k] = t1 > hi[k] ? t1 : hi[k];
+    }
+    if (cur >= 0) flush();
+    for (auto &u : plan->ev_used) {
+        plan->ev_pool.push_back(u.a);
+        if (u.b != u.a) plan->ev_pool.push_back(u.b);
     }
     plan->ev_used.clear();
     return SDRG_OK;
@@ -654,6 +717,19 @@ sdrg_acq_plan_t *sdrg_acq_plan_new(const sdrg_acq_sig_t *sigs, int n_sig)
     if (ensure_device(&dev) || thread_stream(&st)) return nullptr;
     sdrg_acq_plan_t *plan = new sdrg_acq_plan_t();
     plan->g.resize(n_sig);
+    const int n_streams = n_sig < 4 ? n_sig : 4;
+    plan->streams.resize(n_streams, nullptr);
+    plan->ev_join.resize(n_streams, nullptr);
+    bool sok = cudaEventCreateWithFlags(&plan->ev_fork, cudaEventDisableTiming) == cudaSuccess;
+    for (int i = 0; i < n_streams && sok; ++i) {
+        sok = cudaStreamCreateWithFlags(&plan->streams[i], cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&plan->ev_join[i], cudaEventDisableTiming) == cudaSuccess;
+    }
+    if (!sok) {
+        cuda_error(cudaGetLastError(), "sdrg_acq_plan_new streams");
+        sdrg_acq_plan_free(plan);
+        return nullptr;
+    }
     int res_off = 0;
     for (int gi = 0; gi < n_sig; ++gi) {
         GroupState &G = plan->g[gi];
@@ -712,10 +788,17 @@ sdrg_acq_plan_t *sdrg_acq_plan_new(const sdrg_acq_sig_t *sigs, int n_sig)
 void sdrg_acq_plan_free(sdrg_acq_plan_t *plan)
 {
     if (!plan) return;
+    for (cudaStream_t s : plan->streams) {
+        if (!s) continue;
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+    }
+    for (auto ev : plan->ev_join) if (ev) cudaEventDestroy(ev);
+    if (plan->ev_fork) cudaEventDestroy(plan->ev_fork);
     for (auto ev : plan->ev_pool) cudaEventDestroy(ev);
     for (auto &u : plan->ev_used) {
-        cudaEventDestroy(u.second.first);
-        cudaEventDestroy(u.second.second);
+        cudaEventDestroy(u.a);
+        if (u.b != u.a) cudaEventDestroy(u.b);
     }
     for (auto &G : plan->g) {
         if (G.code) cudaFree(G.code);
@@ -757,13 +840,26 @@ int sdrg_acq_run(sdrg_acq_plan_t *plan, const uint8_t *const *if_dev, const int 
     Device *dev;
     int e;
     if ((e = ensure_device(&dev))) return e;
-    cudaStream_t st = (cudaStream_t)stream;
-    if (!st && (e = thread_stream(&st))) return e;
+    cudaStream_t caller = (cudaStream_t)stream;
+    if (!caller && (e = thread_stream(&caller))) return e;
+    for (size_t gi = 0; gi < plan->g.size(); ++gi) {
+        const sdrg_acq_sig_t &s = plan->g[gi].sig;
+        if (len_if[s.buf] < s.L)
+            return set_error(SDRG_ERR_ARG, "IF buffer %d shorter than L=%d", s.buf, s.L);
+    }
+    // fork: every internal stream starts after the caller's prior work
+    if (plan->prof) {
+        cudaEvent_t r[2];
+        if ((e = prof_begin(plan, caller, r))) return e;   // records r[0]
+        plan->ev_pool.push_back(r[1]);
+        plan->ev_used.push_back({-1, plan->run, r[0], r[0]});
+    }
+    SDRG_CUDA(cudaEventRecord(plan->ev_fork, caller));
+    for (cudaStream_t s2 : plan->streams) SDRG_CUDA(cudaStreamWaitEvent(s2, plan->ev_fork, 0));
     for (size_t gi = 0; gi < plan->g.size(); ++gi) {
         GroupState &G = plan->g[gi];
         const sdrg_acq_sig_t &s = G.sig;
-        if (len_if[s.buf] < s.L)
-            return set_error(SDRG_ERR_ARG, "IF buffer %d shorter than L=%d", s.buf, s.L);
+        cudaStream_t st = plan->streams[gi % plan->streams.size()];
         if (G.last_len != len_if[s.buf] || G.last_ix != ix[s.buf]) {
             SDRG_CUDA(cudaEventSynchronize(G.tab_ev));   // previous upload done
             group_tables(G, len_if, ix);
@@ -802,6 +898,12 @@ int sdrg_acq_run(sdrg_acq_plan_t *plan, const uint8_t *const *if_dev, const int 
             return e;
         if ((e = prof_end(plan, st, ev, 3 * (int)gi + 2))) return e;
     }
+    // join: the caller's stream continues after every group
+    for (size_t i = 0; i < plan->streams.size(); ++i) {
+        SDRG_CUDA(cudaEventRecord(plan->ev_join[i], plan->streams[i]));
+        SDRG_CUDA(cudaStreamWaitEvent(caller, plan->ev_join[i], 0));
+    }
+    plan->run++;
     return SDRG_OK;
 }
 
