@@ -386,10 +386,116 @@ def _measured_hbm():
         return 6650.0
 
 
+TRACK_METRIC = "tracking correlator channel-epochs/s (mix + 44-tap corr_std per channel code period)"
+
+
+def _track_setup(args, rank):
+    import torch
+    from pocketsdr_b200 import synth
+    wl = synth.track_24mhz(seed=5 + rank)
+    uniq = {}
+    banks = synth.track_banks(wl)
+    ptrs = []
+    for c, bk in zip(wl.channels, banks):
+        key = (c.sig, c.prn)
+        if key not in uniq:
+            uniq[key] = torch.from_numpy(bk).cuda()
+        ptrs.append(uniq[key].data_ptr())
+    return wl, uniq, ptrs
+
+
+def cpu_track_rate(wl, specs_list, banks_host, max_jobs=600):
+    """Reference CPU rate (jobs/s): sdr_mix_carr + sdr_corr_std per job (the
+    reference's own C build), one thread per job chunk over all host cores."""
+    import concurrent.futures as cf
+    from oracle import oracle
+    R = oracle.best()
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    jobs = [s for specs in specs_list for s in specs][:max_jobs]
+
+    def one(s):
+        IQ = R.mix_carr(wl.bufs[s["buf"]], s["ix"], s["N"], s["fs"], s["fc"], s["phi"])
+        R.corr_std(IQ, banks_host[s["ch"]], s["coff"], s["pos"], False)
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=cores) as ex:
+        list(ex.map(one, jobs))
+    dt = time.perf_counter() - t0
+    return len(jobs) / dt, cores, R.kind, f"{len(jobs)} channel-epochs of the same stream"
+
+
+def run_track(args):
+    """Tracking-correlator workload: every step is one 1 ms epoch of the
+    24 MHz 8-antenna stream, i.e. one correlator job per channel whose code
+    period starts at that epoch (L1CA/L5I every ms, E1B every 4 ms)."""
+    import torch
+    from pocketsdr_b200 import synth, track
+    rank, world, local = dist_info()
+    torch.cuda.set_device(local)
+    wl, uniq, ptrs = _track_setup(args, rank)
+    st = torch.cuda.Stream()
+    torch.cuda.set_stream(st)
+    bufs_d = [torch.from_numpy(b).cuda() for b in wl.bufs]
+    lens = [len(b) for b in wl.bufs]
+    n_ep = args.warmup + args.steps
+    specs_list = []
+    for e in range(n_ep):
+        sp = wl.jobs_at(e * 1e-3, ptrs)
+        for s, c in zip(sp, [c for c in wl.channels if abs(round(e * 1e-3 / c.T) * c.T - e * 1e-3) < 1e-9]):
+            s["ch"] = wl.channels.index(c)
+        specs_list.append(sp)
+    jobs_list = [track.make_jobs(sp) for sp in specs_list]
+    max_j = max(len(s) for s in specs_list)
+    corr = torch.empty(max_j * track.SDR_MAX_CORR * 2, dtype=torch.float32, device="cuda")
+    Cb = torch.empty(max_j * 4, dtype=torch.float32, device="cuda")
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    ptr_b = [b.data_ptr() for b in bufs_d]
+
+    def step(e):
+        track.corr_batch(jobs_list[e], ptr_b, lens, corr.data_ptr(), Cb.data_ptr(), st.cuda_stream)
+
+    for e in range(args.warmup):
+        step(e)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    clk = ClockSampler(local)
+    clk.start()
+    for k in range(args.steps):
+        flush.fill_(k & 0xFF)
+        ev[k][0].record(st)
+        step(args.warmup + k)
+        ev[k][1].record(st)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    n_jobs = sum(len(specs_list[args.warmup + k]) for k in range(args.steps))
+    value = n_jobs / (ms / 1e3)
+    taps = sum(len(s["pos"]) * s["N"] for k in range(args.steps) for s in specs_list[args.warmup + k])
+    line = {"metric": TRACK_METRIC, "value": value, "unit": "channel-epochs/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8",
+            "data": "synthetic",
+            "config": {"workload": "track_24mhz", "channels": len(wl.channels),
+                       "antennas": len(wl.bufs), "taps": 44,
+                       "l2": "flushed between timed steps (512 MB write outside the events)"},
+            "tap_samples_per_s": taps / (ms / 1e3), "clocks": clocks,
+            "gpu_launches": 3 * args.steps}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        banks_host = synth.track_banks(wl)
+        rate, cores, kind, desc = cpu_track_rate(wl, specs_list, banks_host)
+        line["cpu_baseline"] = {"value": rate, "unit": "channel-epochs/s", "cores": cores,
+                                "kind": kind, "sample": desc}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "track_24mhz":
+        return run_track(args)
     return run_ours(args)
 
 

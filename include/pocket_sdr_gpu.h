@@ -231,6 +231,31 @@ int sdrg_acq_grid_host(const sdrg_acq_plan_t *plan, int g, float *dst);
 int sdrg_acq_profile(sdrg_acq_plan_t *plan, int enable);
 int sdrg_acq_profile_get(sdrg_acq_plan_t *plan, double *ms, int64_t *launches);
 
+/* ---- batched tracking correlators ------------------------------------------
+ * One job = what src/sdr_ch.c:725-733 does for one channel and one code
+ * period: sdr_mix_carr(buff[buf], ix, N, fs, fc, phi, IQ) followed by
+ * sdr_corr_std (or sdr_corr_std_cpx_code when cpx_code) on that IQ with the
+ * channel's SDR_N_CODES x N code bank, code offset coff (samples) and n tap
+ * positions pos (samples). Results are bit-identical to those two calls. */
+typedef struct {
+    int buf;                    /* IF buffer index */
+    int ix;                     /* first sample in the circular buffer */
+    int N;                      /* samples (one code period) */
+    double fs, fc, phi;         /* sdr_mix_carr arguments */
+    double coff;                /* sdr_corr_std code offset (samples) */
+    const sdr_cpx16_t *code;    /* DEVICE pointer: code bank [SDR_N_CODES][N] */
+    int cpx_code;               /* 1: complex-code correlator */
+    int n;                      /* taps (1..SDR_MAX_CORR) */
+    const double *pos;          /* HOST pointer: n tap positions (samples) */
+} sdrg_corr_job_t;
+
+/* Runs n_job jobs on `stream` (NULL = the calling thread's stream); if_dev /
+ * len_if describe the device IF buffers. corr_dev receives
+ * [n_job][SDR_MAX_CORR] correlations, C_dev (may be NULL) [n_job][2] boundary
+ * partials, both DEVICE pointers. Asynchronous. */
+int sdrg_corr_batch(const sdrg_corr_job_t *jobs, int n_job, const uint8_t *const *if_dev,
+    const int *len_if, sdr_cpx_t *corr_dev, sdr_cpx_t *C_dev, void *stream);
+
 /* Host convenience: copies IF buffers to the device, runs, and copies the
  * n_prn-total results back (synchronous). if_host[b] are HOST pointers. */
 int sdrg_acq_run_host(sdrg_acq_plan_t *plan, const uint8_t *const *if_host,

@@ -65,6 +65,7 @@ SIGNATURES = {
     "sdrg_acq_profile": ([_p, _i], _i),
     "sdrg_acq_profile_get": ([_p, _p, _p], _i),
     "sdrg_acq_run_host": ([_p, _p, _p, _p, _p], _i),
+    "sdrg_corr_batch": ([_p, _i, _p, _p, _p, _p, _p], _i),
 }
 
 

@@ -244,3 +244,236 @@ void sdr_corr_std_cpx(const sdr_cpx_t *buff, int len_buff, int ix, int N, double
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// batched tracking correlators (sdrg_corr_batch)
+// ---------------------------------------------------------------------------
+namespace sdrg {
+
+struct CorrJobDev {
+    const uint8_t *buf;
+    int len, ix, N, nsplit;
+    uint32_t p0a, p0b, step;
+    int cpx, tap0, n;
+    size_t iq_off;              // first sample of this job in the IQ scratch
+    const char2 *code;          // bank [SDR_N_CODES][N]
+};
+
+struct TapDev { int job, j, k, pad; };
+
+__device__ __forceinline__ char2 mix_byte_b(uint8_t byte, uint32_t phase, const char2 *ctab)
+{
+    const int I = (int)(int8_t)(uint8_t)(byte << 4) >> 4;
+    const int Q = (int)(int8_t)byte >> 4;
+    const char2 c = ctab[phase >> 24];
+    char2 o;
+    o.x = (signed char)(I * c.x - Q * c.y);
+    o.y = (signed char)(I * c.y + Q * c.x);
+    return o;
+}
+
+// grid (chunks, jobs): carrier wipe-off of every job's window into the IQ
+// scratch, with the reference's phase restart at the buffer wrap
+__global__ void mixb_kernel(const CorrJobDev *__restrict__ jobs, const char2 *__restrict__ ctab_g,
+                            char2 *__restrict__ iq)
+{
+    __shared__ char2 ctab[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) ctab[i] = ctab_g[i];
+    __syncthreads();
+    const CorrJobDev J = jobs[blockIdx.y];
+    char2 *out = iq + J.iq_off;
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < J.N; n += gridDim.x * blockDim.x) {
+        int pos = J.ix + n;
+        if (pos >= J.len) pos -= J.len;
+        const uint32_t ph = n < J.nsplit ? J.p0a + J.step * (uint32_t)n
+                                         : J.p0b + J.step * (uint32_t)(n - J.nsplit);
+        out[n] = mix_byte_b(__ldg(J.buf + pos), ph, ctab);
+    }
+}
+
+// sign-product partial sums of one half-dot over [0, main_len) (integer)
+template <bool CPX>
+__device__ __forceinline__ void half_main(const char2 *__restrict__ x, const char2 *__restrict__ y,
+                                          int main_len, int &sr, int &si)
+{
+    for (int i = threadIdx.x; i < main_len; i += blockDim.x) {
+        const char2 a = x[i], c = __ldg(y + i);
+        if (CPX) {
+            sr += sgn_mul8(a.x, c.x) + sgn_mul8(a.y, c.y);
+            si += sgn_mul8(a.y, c.x) + sgn_mul8(a.x, neg8(c.y));
+        } else {
+            sr += sgn_mul8(a.x, c.x);
+            si += sgn_mul8(a.y, c.y);
+        }
+    }
+}
+
+// one block (128 threads) per tap: both half-dots of src/sdr_func.c:990-991
+__global__ void __launch_bounds__(128) tapb_kernel(const TapDev *__restrict__ taps,
+                                                   const CorrJobDev *__restrict__ jobs,
+                                                   const char2 *__restrict__ iq, float cs,
+                                                   float2 *__restrict__ c12)
+{
+    const TapDev T = taps[blockIdx.x];
+    const CorrJobDev J = jobs[T.job];
+    const int N = J.N, j = T.j;
+    const char2 *IQ = iq + J.iq_off;
+    const char2 *bank = J.code + (size_t)T.k * N;
+    __shared__ int red[2][2][4];
+    int sum[2][2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int len = h == 0 ? j : N - j;
+        const char2 *x = IQ + (h == 0 ? 0 : j);
+        const char2 *y = bank + (h == 0 ? N - j : 0);
+        int sr = 0, si = 0;
+        if (J.cpx) half_main<true>(x, y, (len / 16) * 16, sr, si);
+        else half_main<false>(x, y, (len / 16) * 16, sr, si);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            sr += __shfl_xor_sync(0xffffffffu, sr, o);
+            si += __shfl_xor_sync(0xffffffffu, si, o);
+        }
+        sum[h][0] = sr;
+        sum[h][1] = si;
+    }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        red[0][0][w] = sum[0][0]; red[0][1][w] = sum[0][1];
+        red[1][0][w] = sum[1][0]; red[1][1][w] = sum[1][1];
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        const int h = threadIdx.x;
+        const int len = h == 0 ? j : N - j;
+        const char2 *x = IQ + (h == 0 ? 0 : j);
+        const char2 *y = bank + (h == 0 ? N - j : 0);
+        int tr = 0, ti = 0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) { tr += red[h][0][i]; ti += red[h][1][i]; }
+        float fr = (float)tr, fi = (float)ti;
+        for (int i = (len / 16) * 16; i < len; ++i) {
+            const char2 a = x[i], c = y[i];
+            if (J.cpx) {
+                fr = __fadd_rn(fr, (float)(a.x * c.x + a.y * c.y));
+                fi = __fadd_rn(fi, (float)(a.y * c.x - a.x * c.y));
+            } else {
+                fr = __fadd_rn(fr, (float)(a.x * c.x));
+                fi = __fadd_rn(fi, (float)(a.y * c.y));
+            }
+        }
+        c12[2 * blockIdx.x + h] = make_float2(__fmul_rn(fr, cs), __fmul_rn(fi, cs));
+    }
+}
+
+// one warp per job: polarity test and outputs (src/sdr_func.c:993-1007)
+__global__ void finb_kernel(const CorrJobDev *__restrict__ jobs, const float2 *__restrict__ c12,
+                            float2 *__restrict__ corr, float2 *__restrict__ C)
+{
+    const CorrJobDev J = jobs[blockIdx.x];
+    const float2 *cc = c12 + 2 * (size_t)J.tap0;
+    float dot = 0.0f;
+    for (int i = 0; i < 3 && i < J.n; ++i) {
+        const float2 a = cc[2 * i], b = cc[2 * i + 1];
+        dot = __fadd_rn(dot, __fmaf_rn(a.x, b.x, __fmul_rn(a.y, b.y)));
+    }
+    const float sign = dot < 0.0f ? -1.0f : 1.0f;
+    const float fN = (float)J.N;
+    float2 *out = corr + (size_t)blockIdx.x * SDR_MAX_CORR;
+    for (int i = threadIdx.x; i < J.n; i += blockDim.x) {
+        const float2 a = cc[2 * i], b = cc[2 * i + 1];
+        out[i] = make_float2(__fdiv_rn(__fadd_rn(a.x, __fmul_rn(sign, b.x)), fN),
+                             __fdiv_rn(__fadd_rn(a.y, __fmul_rn(sign, b.y)), fN));
+    }
+    if (C && threadIdx.x == 0 && J.n > 0) {
+        C[2 * (size_t)blockIdx.x] = cc[0];
+        C[2 * (size_t)blockIdx.x + 1] = cc[1];
+    }
+}
+
+static inline uint32_t phase_b(double phi) { return (uint32_t)((phi - floor(phi)) * 4294967296.0); }
+static inline uint32_t step_b(double step) { return (uint32_t)(int)(step * 4294967296.0); }
+
+} // namespace sdrg
+
+extern "C" int sdrg_corr_batch(const sdrg_corr_job_t *jobs, int n_job, const uint8_t *const *if_dev,
+                               const int *len_if, sdr_cpx_t *corr_dev, sdr_cpx_t *C_dev, void *stream)
+{
+    if (n_job <= 0) return SDRG_OK;
+    if (!jobs || !if_dev || !len_if || !corr_dev)
+        return set_error(SDRG_ERR_ARG, "sdrg_corr_batch: null argument");
+    Device *dev;
+    int e;
+    if ((e = ensure_device(&dev))) return e;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!st && (e = thread_stream(&st))) return e;
+    ThreadCtx &c = tctx();
+    // table sizes
+    size_t n_tap = 0, n_iq = 0;
+    for (int i = 0; i < n_job; ++i) {
+        const sdrg_corr_job_t &J = jobs[i];
+        if (J.N <= 0 || J.n <= 0 || J.n > SDR_MAX_CORR || !J.code || !J.pos || J.buf < 0 ||
+            J.ix < 0 || J.ix >= len_if[J.buf] || J.N > len_if[J.buf] || J.fs <= 0)
+            return set_error(SDRG_ERR_ARG, "sdrg_corr_batch: bad job %d", i);
+        n_tap += J.n;
+        n_iq += ((size_t)J.N + 15) / 16 * 16;
+    }
+    const size_t jb = sizeof(CorrJobDev) * n_job, tb = sizeof(TapDev) * n_tap;
+    const size_t tab_bytes = (jb + tb + 255) / 256 * 256;
+    const size_t dev_bytes = tab_bytes + n_iq * sizeof(char2) + 2 * n_tap * sizeof(float2) + 512;
+    if (!c.cb_ev) {
+        SDRG_CUDA(cudaEventCreateWithFlags(&c.cb_ev, cudaEventDisableTiming));
+        SDRG_CUDA(cudaEventCreateWithFlags(&c.cb_done, cudaEventDisableTiming));
+    }
+    // the previous call's upload from the host staging has finished, and this
+    // call's device work follows the previous call's (which may be on another
+    // stream) because both use this thread's scratch
+    SDRG_CUDA(cudaEventSynchronize(c.cb_ev));
+    SDRG_CUDA(cudaStreamWaitEvent(st, c.cb_done, 0));
+    c.cb_host.pinned = true;
+    if (dev_bytes > c.cb_dev.size) SDRG_CUDA(cudaStreamSynchronize(st));
+    if ((e = c.cb_host.reserve(tab_bytes)) || (e = c.cb_dev.reserve(dev_bytes))) return e;
+    CorrJobDev *jh = (CorrJobDev *)c.cb_host.ptr;
+    TapDev *th = (TapDev *)((char *)c.cb_host.ptr + jb);
+    size_t tap = 0, iq_off = 0;
+    std::vector<int2> jk(SDR_MAX_CORR);
+    for (int i = 0; i < n_job; ++i) {
+        const sdrg_corr_job_t &J = jobs[i];
+        const int len = len_if[J.buf];
+        // the reference's tap arithmetic (src/sdr_func.c:988-990), in double
+        if (!tap_params(J.N, J.coff, J.pos, J.n, SDR_N_CODES, jk.data()))
+            return set_error(SDRG_ERR_ARG, "sdrg_corr_batch: job %d tap outside one wrap", i);
+        // sdr_mix_carr's phase arithmetic and wrap split (src/sdr_func.c:772-836)
+        const double step = J.fc / J.fs;
+        const int n1 = (J.ix + J.N <= len) ? J.N : len - J.ix;
+        CorrJobDev d;
+        d.buf = if_dev[J.buf]; d.len = len; d.ix = J.ix; d.N = J.N; d.nsplit = n1;
+        d.p0a = phase_b(J.phi);
+        d.p0b = n1 < J.N ? phase_b(J.phi + step * n1) : 0;
+        d.step = step_b(step);
+        d.cpx = J.cpx_code ? 1 : 0; d.tap0 = (int)tap; d.n = J.n;
+        d.iq_off = iq_off;
+        d.code = (const char2 *)J.code;
+        jh[i] = d;
+        for (int t = 0; t < J.n; ++t) th[tap + t] = TapDev{i, jk[t].x, jk[t].y, 0};
+        tap += J.n;
+        iq_off += ((size_t)J.N + 15) / 16 * 16;
+    }
+    char *db = (char *)c.cb_dev.ptr;
+    CorrJobDev *jd = (CorrJobDev *)db;
+    TapDev *td = (TapDev *)(db + jb);
+    char2 *iq = (char2 *)(db + tab_bytes);
+    float2 *c12 = (float2 *)(db + tab_bytes + ((n_iq * sizeof(char2) + 255) / 256) * 256);
+    SDRG_CUDA(cudaMemcpyAsync(db, c.cb_host.ptr, jb + tb, cudaMemcpyHostToDevice, st));
+    SDRG_CUDA(cudaEventRecord(c.cb_ev, st));
+    int maxN = 0;
+    for (int i = 0; i < n_job; ++i) maxN = jobs[i].N > maxN ? jobs[i].N : maxN;
+    dim3 mg((unsigned)((maxN + 255) / 256 < 64 ? (maxN + 255) / 256 : 64), (unsigned)n_job);
+    mixb_kernel<<<mg, 256, 0, st>>>(jd, dev->ctab_dev, iq);
+    SDRG_CUDA(cudaGetLastError());
+    tapb_kernel<<<(unsigned)n_tap, 128, 0, st>>>(td, jd, iq, kCScale, c12);
+    SDRG_CUDA(cudaGetLastError());
+    finb_kernel<<<(unsigned)n_job, 32, 0, st>>>(jd, c12, (float2 *)corr_dev, (float2 *)C_dev);
+    SDRG_CUDA(cudaGetLastError());
+    SDRG_CUDA(cudaEventRecord(c.cb_done, st));
+    return SDRG_OK;
+}

@@ -409,6 +409,100 @@ __device__ void fft_inverse(float2 *sm, const float2 *tw, const FftPlanK &pl,
     }
 }
 
+// ---- compile-time plans -------------------------------------------------------
+// A 4-pass plan fixed at compile time: every stride, table offset, loop trip
+// count and divisor is a constant, so shared-memory addresses take immediate
+// offsets and the butterfly loops unroll. The table layout is the runtime
+// plan's (pass 0: S0 entries; pass p >= 1: S_p * (r_p - 1) entries), so a
+// matching runtime plan's tables serve it unchanged.
+template <int M_, int NT_, int R0_, int R1_, int R2_, int R3_>
+struct StaticPlan4 {
+    static constexpr int M = M_, NT = NT_;
+    static constexpr int R0 = R0_, R1 = R1_, R2 = R2_, R3 = R3_;
+    static constexpr int S0 = M / R0, S1 = S0 / R1, S2 = S1 / R2, S3 = S2 / R3;
+    static constexpr int O0 = 0, O1 = S0, O2 = O1 + S1 * (R1 - 1), O3 = O2 + S2 * (R2 - 1);
+    static constexpr int TWTOT = O3 + S3 * (R3 - 1);
+    static_assert(S3 == 1 && R0 * R1 * R2 * R3 == M, "plan must cover M");
+    static bool matches(const FftPlanK &k, int threads)
+    {
+        return k.M == M && k.npass == 4 && k.radix[0] == R0 && k.radix[1] == R1 &&
+               k.radix[2] == R2 && k.radix[3] == R3 && k.twtot == TWTOT && threads == NT;
+    }
+};
+
+// The plan of every 24 000-point sub-transform (L = 24 000 x {1, 2, 8}: the
+// 12 and 24 MHz searches of 1 ms and 4 ms codes).
+using Plan24000 = StaticPlan4<24000, 512, 16, 10, 10, 15>;
+
+// inner pass with compile-time radix R, stride S (sub-length R*S)
+template <int R, int S, int M, int NT, bool FWD>
+__device__ __forceinline__ void s_inner(float2 *sm, const float2 *twp)
+{
+    constexpr int NB = M / R, LS = R * S, IT = (NB + NT - 1) / NT;
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int b = threadIdx.x + it * NT;
+        if (b < NB) {
+            const int blk = b / S, i = b - blk * S;
+            float2 *p = sm + blk * LS + i;
+            float2 v[R];
+#pragma unroll
+            for (int j = 0; j < R; ++j) v[j] = p[j * S];
+            if (FWD) {
+                Dft<R, -1>::run(v);
+                if (S > 1) {
+#pragma unroll
+                    for (int j = 1; j < R; ++j) v[j] = cmul(v[j], twp[(j - 1) * S + i]);
+                }
+            } else {
+                if (S > 1) {
+#pragma unroll
+                    for (int j = 1; j < R; ++j) v[j] = cmul(v[j], cconj(twp[(j - 1) * S + i]));
+                }
+                Dft<R, 1>::run(v);
+            }
+#pragma unroll
+            for (int j = 0; j < R; ++j) p[j * S] = v[j];
+        }
+    }
+}
+
+// last inverse pass (radix R, stride S = M / R) handing outputs to store()
+template <int R, int S, int NT, class Store>
+__device__ __forceinline__ void s_pass0_store(const float2 *sm, const float2 *twp, Store &store)
+{
+    constexpr int IT = (S + NT - 1) / NT;
+#pragma unroll 1
+    for (int it = 0; it < IT; ++it) {
+        const int i = threadIdx.x + it * NT;
+        if (i < S) {
+            typename Store::Old old[R];
+#pragma unroll
+            for (int j = 0; j < R; ++j) old[j] = store.pre(i + j * S);
+            float2 v[R];
+#pragma unroll
+            for (int j = 0; j < R; ++j) v[j] = sm[i + j * S];
+            if (i) apply_tw<R>(v, cconj(twp[i]));
+            Dft<R, 1>::run(v);
+#pragma unroll
+            for (int j = 0; j < R; ++j) store(i + j * S, v[j], old[j]);
+        }
+    }
+}
+
+// Inverse transform with a compile-time plan (same contract as fft_inverse).
+template <class P, class Store>
+__device__ __forceinline__ void fft_inverse_static(float2 *sm, const float2 *tw, Store &store)
+{
+    s_inner<P::R3, P::S3, P::M, P::NT, false>(sm, tw + P::O3);
+    __syncthreads();
+    s_inner<P::R2, P::S2, P::M, P::NT, false>(sm, tw + P::O2);
+    __syncthreads();
+    s_inner<P::R1, P::S1, P::M, P::NT, false>(sm, tw + P::O1);
+    __syncthreads();
+    s_pass0_store<P::R0, P::S0, P::NT>(sm, tw + P::O0, store);
+}
+
 // Copies the per-pass twiddle tables from global to shared memory.
 __device__ __forceinline__ void load_twiddles(float2 *tw_sm, const float2 *tw_g,
                                               int n)

@@ -49,6 +49,10 @@ struct ThreadCtx {
     cudaStream_t stream = nullptr;
     Scratch dev[6];      // device scratch slots
     Scratch host[3];     // pinned host staging slots
+    // batched correlators (asynchronous): their own slots and the event of
+    // the last upload from cb_host
+    Scratch cb_dev, cb_host;
+    cudaEvent_t cb_ev = nullptr, cb_done = nullptr;
     int error = 0;
     std::string msg;
 };

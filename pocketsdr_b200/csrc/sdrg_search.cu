@@ -186,13 +186,13 @@ struct StoreComplex {
     __device__ __forceinline__ void operator()(int m, float2 y, int) const { row[R * m + c] = y; }
 };
 
-template <int R, int MODE>
+template <int R, int MODE, int SP>
 __global__ void __launch_bounds__(512, 1) cons_kernel(ConsArgs a)
 {
     extern __shared__ float2 smem[];
     float2 *sm = smem;
     float2 *tw = smem + a.pl.M;
-    const int M = a.pl.M;
+    const int M = SP ? Plan24000::M : a.pl.M;   // SP: compile-time plan
     const int c = (R > 1) ? (int)(blockIdx.x % R) : 0;
     // bin-major tasks: the PRNs of one Doppler bin run side by side, so the
     // bin's forward spectra are fetched from HBM once and then hit in L2
@@ -279,11 +279,13 @@ __global__ void __launch_bounds__(512, 1) cons_kernel(ConsArgs a)
         if (MODE == 0) {
             float *row = a.P + (size_t)(prn) * a.prn_stride + (size_t)b * a.bin_stride;
             StorePower<R> st{row, c, a.Nmax, a.accumulate || s > 0};
-            fft_inverse(sm, tw, a.pl, st);
+            if constexpr (SP == 1) fft_inverse_static<Plan24000>(sm, tw, st);
+            else fft_inverse(sm, tw, a.pl, st);
         } else {
             float2 *row = a.Y + (size_t)b * (size_t)R * M;
             StoreComplex<R> st{row, c};
-            fft_inverse(sm, tw, a.pl, st);
+            if constexpr (SP == 1) fft_inverse_static<Plan24000>(sm, tw, st);
+            else fft_inverse(sm, tw, a.pl, st);
         }
     }
     // keep remote shared memory alive until every CTA has finished reading
@@ -323,16 +325,16 @@ static int launch_fwd(const FftPlan *pl, const FwdArgs &a, int n_blocks, cudaStr
     return SDRG_OK;
 }
 
-template <int R, int MODE>
-static int launch_cons_R(const FftPlan *pl, const ConsArgs &a, int n_tasks, cudaStream_t st)
+template <int R, int MODE, int SP>
+static int launch_cons_RS(const FftPlan *pl, const ConsArgs &a, int n_tasks, cudaStream_t st)
 {
     static bool attr_set = false;
     if (!attr_set) {
-        SDRG_CUDA(cudaFuncSetAttribute(cons_kernel<R, MODE>,
+        SDRG_CUDA(cudaFuncSetAttribute(cons_kernel<R, MODE, SP>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)(g_smem_limit())));
         if (R > 1) {
-            SDRG_CUDA(cudaFuncSetAttribute(cons_kernel<R, MODE>,
+            SDRG_CUDA(cudaFuncSetAttribute(cons_kernel<R, MODE, SP>,
                                            cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
         }
         attr_set = true;
@@ -349,8 +351,20 @@ static int launch_cons_R(const FftPlan *pl, const ConsArgs &a, int n_tasks, cuda
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = R > 1 ? 1 : 0;
-    SDRG_CUDA(cudaLaunchKernelEx(&cfg, cons_kernel<R, MODE>, a));
+    SDRG_CUDA(cudaLaunchKernelEx(&cfg, cons_kernel<R, MODE, SP>, a));
     return SDRG_OK;
+}
+
+// the compile-time 24 000-point plan where it applies (R = 1, 2, 8), the
+// runtime plan otherwise
+template <int R, int MODE>
+static int launch_cons_R(const FftPlan *pl, const ConsArgs &a, int n_tasks, cudaStream_t st)
+{
+    if constexpr (R == 1 || R == 2 || R == 8) {
+        if (Plan24000::matches(pl->k, pl->threads))
+            return launch_cons_RS<R, MODE, 1>(pl, a, n_tasks, st);
+    }
+    return launch_cons_RS<R, MODE, 0>(pl, a, n_tasks, st);
 }
 
 template <int MODE>

@@ -177,6 +177,99 @@ def acq_multi_24mhz(seed: int = 2, prn_limit: int | None = None, t_sum: float = 
     return Workload("acq_multi_24mhz", fs, True, bufs, groups, sats, [0] * n_buf)
 
 
+@dataclass
+class TrackChannel:
+    sig: str
+    prn: int
+    ant: int              # antenna (IF buffer)
+    fd0: float            # Doppler at t = 0 (Hz)
+    rate: float           # Doppler rate (Hz/s)
+    coff0: float          # code offset at t = 0 (s)
+    N: int                # samples per code period
+    T: float              # code period (s)
+
+
+@dataclass
+class TrackWorkload:
+    """Tracking-correlator batch: n_ant antenna streams, channels with their
+    own code bank, open-loop carrier / code trajectories."""
+    fs: float
+    fi: float
+    bufs: list
+    channels: list
+    pos: dict             # per signal: tap positions (samples)
+
+    def jobs_at(self, t: float, banks_ptr: list) -> list:
+        """Job specs for every channel whose code period starts at time t
+        (multiple of its period), following src/sdr_ch.c:692-733: carrier at
+        fi + fd(t), phase = integral of the carrier, code offset drifting with
+        the carrier-aided rate."""
+        out = []
+        for c, ptr in zip(self.channels, banks_ptr):
+            k = int(round(t / c.T))
+            if abs(k * c.T - t) > 1e-9:
+                continue
+            fd = c.fd0 + c.rate * t
+            fc = self.fi + fd
+            phi = self.fi * t + c.fd0 * t + 0.5 * c.rate * t * t
+            coff = c.coff0 - (c.fd0 * t + 0.5 * c.rate * t * t) / CARRIER[c.sig]
+            L = len(self.bufs[c.ant])
+            ix = int(round(t * self.fs)) % L
+            out.append(dict(buf=c.ant, ix=ix, N=c.N, fs=self.fs, fc=fc, phi=phi - np.floor(phi),
+                            coff=(coff % c.T) * self.fs, cpx_code=False, pos=self.pos[c.sig],
+                            code_ptr=ptr))
+        return out
+
+
+TRACK_SIGS = (("L1CA", 0.375), ("E1B", 0.25), ("L5I", 0.375))
+
+
+def track_24mhz(seed: int = 5, n_ch: int = 256, n_ant: int = 8, t_buf: float = 0.1) -> TrackWorkload:
+    """24 MHz complex IQ, 3-bit, n_ant antenna streams of t_buf seconds
+    (replayed cyclically for longer runs); n_ch channels mixing L1 C/A, E1-B
+    and L5-I with Doppler rates U[0, 2] Hz/s; taps P/E/L at +-0.5 chip, the
+    noise tap at -120 samples and 40 taps at 0.05-chip spacing (44 taps)."""
+    fs, fi, bits = 24e6, 3.0e6, 3
+    rng = np.random.default_rng(seed)
+    chans = []
+    counts = [int(round(f * n_ch)) for _, f in TRACK_SIGS]
+    counts[-1] = n_ch - sum(counts[:-1])
+    for (sig, _), cnt in zip(TRACK_SIGS, counts):
+        prns = list(codes.PRN_SETS[sig])
+        T = codes.code_cyc(sig)
+        for i in range(cnt):
+            chans.append(TrackChannel(sig, prns[i % len(prns)], i % n_ant,
+                                      float(rng.uniform(-4000, 4000)), float(rng.uniform(0, 2)),
+                                      float(rng.uniform(0, T)), int(round(fs * T)), T))
+    pos = {}
+    for sig, _ in TRACK_SIGS:
+        L, T = codes.SIGNALS[sig]
+        sc = T / (L if sig != "E1B" else L // 2) * fs      # samples per chip
+        pos[sig] = np.concatenate([[0.0, -0.5 * sc, 0.5 * sc, -120.0],
+                                   np.arange(-20, 20) * 0.05 * sc])
+    n = int(round(t_buf * fs))
+    bufs = []
+    for a in range(n_ant):
+        sats = [Sat(c.sig, c.prn, (1 - c.coff0 / c.T) * codes.SIGNALS[c.sig][0], c.fd0, 0.0, 45.0, a)
+                for c in chans if c.ant == a][:12]
+        bufs.append(gen_if(n, fs, {s: fi for s, _ in TRACK_SIGS}, sats, iq=True, bits=bits,
+                           seed=seed * 100 + a))
+    return TrackWorkload(fs, fi, bufs, chans, pos)
+
+
+def track_banks(wl: TrackWorkload) -> list:
+    """Per channel code bank (int8 [10 N, 2]) as the receiver builds it."""
+    from .track import code_bank
+    cache = {}
+    out = []
+    for c in wl.channels:
+        key = (c.sig, c.prn)
+        if key not in cache:
+            cache[key] = code_bank(codes.gen_code(c.sig, c.prn), c.T, wl.fs, c.N)
+        out.append(cache[key])
+    return out
+
+
 def group_code_ffts(g: Group) -> np.ndarray:
     """[n_prn, L] complex64 conjugated code DFTs of a group."""
     out = np.empty((len(g.prns), g.L), np.complex64)

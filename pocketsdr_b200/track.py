@@ -1,0 +1,74 @@
+"""Batched tracking correlators on the GPU (sdrg_corr_batch C ABI).
+
+One job is the per-channel, per-code-period work of the reference's tracking
+loop (src/sdr_ch.c:725-733): carrier wipe-off of the channel's IF window
+(sdr_mix_carr) and the multi-tap standard correlator (sdr_corr_std, or
+sdr_corr_std_cpx_code for complex codes) against the channel's resampled code
+bank. A batch runs every channel of an epoch in three launches; outputs are
+bit-identical to the reference's two calls per channel.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import check, lib
+
+SDR_N_CODES = 10
+SDR_MAX_CORR = 107
+
+
+class CorrJob(C.Structure):
+    """sdrg_corr_job_t."""
+    _fields_ = [("buf", C.c_int), ("ix", C.c_int), ("N", C.c_int),
+                ("fs", C.c_double), ("fc", C.c_double), ("phi", C.c_double),
+                ("coff", C.c_double), ("code", C.c_void_p), ("cpx_code", C.c_int),
+                ("n", C.c_int), ("pos", C.POINTER(C.c_double))]
+
+
+lib.sdrg_corr_batch.argtypes = [C.POINTER(CorrJob), C.c_int, C.c_void_p, C.c_void_p,
+                                C.c_void_p, C.c_void_p, C.c_void_p]
+lib.sdrg_corr_batch.restype = C.c_int
+
+
+def make_jobs(specs) -> tuple:
+    """specs: iterable of dicts with keys buf, ix, N, fs, fc, phi, coff,
+    code_ptr (device pointer of the bank), cpx_code, pos (sequence of floats).
+    Returns (ctypes job array, keep-alive list)."""
+    specs = list(specs)
+    arr = (CorrJob * len(specs))()
+    keep = []
+    for j, s in zip(arr, specs):
+        pos = np.ascontiguousarray(s["pos"], np.float64)
+        keep.append(pos)
+        j.buf, j.ix, j.N = int(s["buf"]), int(s["ix"]), int(s["N"])
+        j.fs, j.fc, j.phi, j.coff = float(s["fs"]), float(s["fc"]), float(s["phi"]), float(s["coff"])
+        j.code = C.c_void_p(int(s["code_ptr"]))
+        j.cpx_code = int(bool(s.get("cpx_code", False)))
+        j.n = len(pos)
+        j.pos = pos.ctypes.data_as(C.POINTER(C.c_double))
+    return arr, keep
+
+
+def corr_batch(jobs, if_ptrs, lens, corr_ptr: int, C_ptr: int = 0, stream: int = 0) -> None:
+    """Asynchronous batch on device buffers: jobs from make_jobs; if_ptrs /
+    lens: device IF buffers; corr_ptr: [n_job][107] complex64 device buffer;
+    C_ptr: [n_job][2] complex64 device buffer or 0."""
+    arr, _ = jobs if isinstance(jobs, tuple) else (jobs, None)
+    n = len(if_ptrs)
+    ptrs = (C.c_void_p * n)(*if_ptrs)
+    ls = (C.c_int * n)(*lens)
+    st = lib.sdrg_corr_batch(arr, len(arr), ptrs, ls, C.c_void_p(corr_ptr),
+                             C.c_void_p(C_ptr or None), C.c_void_p(stream or None))
+    if st:
+        check("sdrg_corr_batch")
+
+
+def code_bank(code, T, fs, N, code_Q=None) -> np.ndarray:
+    """The receiver's fractional-phase code bank (src/sdr_ch.c:265-272):
+    bank k is the code resampled with offset -k / fs / SDR_N_CODES, as
+    int8 [SDR_N_CODES * N, 2]."""
+    from .codes import res_code
+    banks = [res_code(code, T, -k / fs / SDR_N_CODES, fs, N, 0, code_Q) for k in range(SDR_N_CODES)]
+    return np.concatenate(banks)
