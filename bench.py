@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--prn-limit", type=int, default=None,
                     help="fewer PRNs per group (profiling runs)")
+    ap.add_argument("--scaling", choices=("weak", "strong"), default="weak",
+                    help="weak: one IF block per rank; strong: PRNs dealt over ranks")
     ap.add_argument("--t-sum", type=float, default=20e-3,
                     help="non-coherent time per group (s)")
     return ap.parse_args()
@@ -233,19 +235,23 @@ def run_ours(args):
     import torch
     rank, world, local = dist_info()
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
     from pocketsdr_b200 import acquire, synth
-    from pocketsdr_b200._lib import lib
+    from pocketsdr_b200 import dist as D
+    dist = D.init(backend="nccl", device=torch.device("cuda", local))
+    strong = args.scaling == "strong" and world > 1
 
-    wl = make_workload(args.workload, 2 + rank, args.prn_limit, args.t_sum)
+    # weak: every rank searches its own IF block; strong: one IF block, the
+    # PRNs of every group dealt over the ranks
+    wl = make_workload(args.workload, 2 + (0 if strong else rank), args.prn_limit, args.t_sum)
+    full_groups = wl.groups
+    shard_index = None
+    if strong:
+        wl.groups, shard_index = D.shard_groups(full_groups, rank, world)
     cfs = [synth.group_code_ffts(g) for g in wl.groups]
     plan = acquire.AcqPlan(wl.groups, cfs)
     cells = plan.cells
+    job_cells = sum(len(g.prns) * len(g.fds) * g.Nmax for g in full_groups) if strong \
+        else cells * world
     st = torch.cuda.Stream()          # every launch of ours and every event on it
     torch.cuda.set_stream(st)
     bufs_d = [torch.from_numpy(b).cuda() for b in wl.bufs]
@@ -286,12 +292,8 @@ def run_ours(args):
                 sum(v[1] for (g, kk), v in prof_g.items() if kk == k))
             for k in ("fwd", "cons", "peak")}
     plan.profile(False)
-    total_ms = sum(step_ms)
-    if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = cells * args.steps * world / (total_ms / 1e3)
+    total_ms = D.max_over_ranks(sum(step_ms), dist)
+    value = job_cells * args.steps / (total_ms / 1e3)
 
     # ---- end to end through the public API: host IF -> device -> results -> host
     bufs_h = [torch.from_numpy(b).pin_memory() for b in wl.bufs]
@@ -316,13 +318,11 @@ def run_ours(args):
         e2e_step()
         e2e_ev[k][1].record(st)
     torch.cuda.synchronize()
-    e2e_ms = sum(a.elapsed_time(b) for a, b in e2e_ev)
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = cells * args.steps * world / (e2e_ms / 1e3)
+    e2e_ms = D.max_over_ranks(sum(a.elapsed_time(b) for a, b in e2e_ev), dist)
+    e2e_value = job_cells * args.steps / (e2e_ms / 1e3)
     res = np.frombuffer(res_h.numpy().tobytes(), dtype=acquire.RESULT_DTYPE)
+    if strong:   # the per-PRN results of every rank, once (32 B per PRN)
+        res = np.concatenate(D.gather_results(res, shard_index, full_groups, world, dist))
 
     # ---- roofline of the dominant kernel (consumer: code product + inverse FFT + power)
     cons_ms, cons_n = prof["cons"]
@@ -352,12 +352,14 @@ def run_ours(args):
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": args.workload, "cells_per_step": cells,
+            "scaling": "strong" if strong else "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": args.workload, "cells_per_step": job_cells // (1 if strong else world),
                        "groups": [f"{g.sig}:{len(g.prns)}prn x {len(g.fds)}bin x {g.Nmax}off x "
-                                  f"{g.n_sum}sum L={g.L}" for g in wl.groups],
+                                  f"{g.n_sum}sum L={g.L}" for g in full_groups],
                        "l2": "flushed between timed steps (512 MB write outside the events)",
-                       "parallelism": f"replica x{world} (one IF block per rank)"},
+                       "parallelism": (f"PRNs dealt over {world} ranks, results all-gathered once"
+                                       if strong else f"replica x{world} (one IF block per rank)")},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": sum(n for _, n in prof.values()),
