@@ -181,7 +181,9 @@ static const size_t kSmemDefault = 232448;
 
 bool plan_shape(int L, int *Rout, int *Mout, FftPlanK *kout)
 {
-    static const int Rs[] = {1, 2, 3, 4, 5, 6, 8};
+    // R <= 8: one thread-block cluster per transform; R in 10..20: staged
+    // through an L2-resident scratch (a cluster cannot exceed 8 portably)
+    static const int Rs[] = {1, 2, 3, 4, 5, 6, 8, 10, 12, 15, 16, 20};
     size_t smax = g_dev.id >= 0 ? g_dev.smem_optin : kSmemDefault;
     for (int R : Rs) {
         if (L % R) continue;
@@ -231,7 +233,7 @@ static int build_plan(int L, FftPlan *pl)
     FftPlanK k;
     if (!plan_shape(L, &R, &M, &k)) {
         return set_error(SDRG_ERR_ARG,
-                         "FFT length %d unsupported (needs L = R*M, R in {1..6,8}, "
+                         "FFT length %d unsupported (needs L = R*M, R in {1..6,8,10,12,15,16,20}, "
                          "M 2-3-5-smooth and fitting one CTA)", L);
     }
     pl->L = L; pl->R = R; pl->M = M; pl->k = k;

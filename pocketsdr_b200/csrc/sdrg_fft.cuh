@@ -186,6 +186,7 @@ template <int DIR> struct Dft<10, DIR> : DftCT<2, 5, DIR> {};
 template <int DIR> struct Dft<12, DIR> : DftCT<4, 3, DIR> {};
 template <int DIR> struct Dft<15, DIR> : DftCT<3, 5, DIR> {};
 template <int DIR> struct Dft<16, DIR> : DftCT<4, 4, DIR> {};
+template <int DIR> struct Dft<20, DIR> : DftCT<4, 5, DIR> {};   // staged splits only
 
 // ---- kernel-side plan --------------------------------------------------------
 struct FftPlanK {

@@ -292,6 +292,117 @@ __global__ void __launch_bounds__(512, 1) cons_kernel(ConsArgs a)
     if constexpr (R > 1) cg::this_cluster().sync();
 }
 
+// ---------------------------------------------------------------------------
+// staged consumer for splits R > 8 (L up to 20 * M, e.g. 480 000 = 20 x 24 000):
+// the combine writes the R sub-spectra w_c of a chunk of tasks to an
+// L2-resident scratch W, then R independent CTAs per task run the length-M
+// inverse transforms. Same arithmetic as cons_kernel's cluster exchange.
+// ---------------------------------------------------------------------------
+struct StageArgs {
+    const float2 *split, *X, *code;
+    int R, M, n_prn, n_bin, n_sum;
+    int task0, s;            // first task of the chunk, sum index
+    float scale;
+    float2 *W;               // [chunk][R][M]
+};
+
+template <int R>
+__global__ void __launch_bounds__(256) stage_combine_kernel(StageArgs a)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= a.M) return;
+    const int tl = blockIdx.y, task = a.task0 + tl;
+    const int prn = task % a.n_prn, b = task / a.n_prn;
+    const size_t M = a.M;
+    const float2 *Xs = a.X + ((size_t)b * a.n_sum + a.s) * R * M;
+    const float2 *code = a.code + (size_t)prn * R * M;
+    const float2 t = __ldg(a.split + q), tc = cconj(t);
+    float2 g[R];
+    g[0] = __ldg(Xs + q);
+    float2 w = tc;
+#pragma unroll
+    for (int r = 1; r < R; ++r) {
+        g[r] = cmul(__ldg(Xs + r * M + q), w);
+        if (r + 1 < R) w = cmul(w, tc);
+    }
+    Dft<R, -1>::run(g);                     // X[k + jM]
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+        const float2 z = cmul(g[j], __ldg(code + j * M + q));
+        g[j] = make_float2(z.x * a.scale, z.y * a.scale);
+    }
+    Dft<R, 1>::run(g);                      // sum_j Z e^{+2 pi i c j / R}
+    w = t;
+#pragma unroll
+    for (int j = 1; j < R; ++j) {
+        g[j] = cmul(g[j], w);
+        if (j + 1 < R) w = cmul(w, t);
+    }
+    float2 *Wt = a.W + (size_t)tl * R * M;
+#pragma unroll
+    for (int j = 0; j < R; ++j) Wt[j * M + q] = g[j];
+}
+
+struct StorePowerRt {
+    typedef float Old;
+    float *row;
+    int c, R, Nmax;
+    bool add;
+    __device__ __forceinline__ float pre(int m) const
+    {
+        const int n = R * m + c;
+        return (add && n < Nmax) ? row[n] : 0.0f;
+    }
+    __device__ __forceinline__ void operator()(int m, float2 y, float old) const
+    {
+        const int n = R * m + c;
+        if (n < Nmax) {
+            const float pw = y.x * y.x + y.y * y.y;
+            row[n] = add ? old + pw : pw;
+        }
+    }
+};
+
+struct StoreComplexRt {
+    typedef int Old;
+    float2 *row;
+    int c, R;
+    __device__ __forceinline__ int pre(int) const { return 0; }
+    __device__ __forceinline__ void operator()(int m, float2 y, int) const { row[R * m + c] = y; }
+};
+
+// grid (R, chunk tasks): CTA c of a task inverts w_c
+template <int MODE, int SP>
+__global__ void __launch_bounds__(512, 1) stage_ifft_kernel(ConsArgs ca, StageArgs a)
+{
+    extern __shared__ float2 smem[];
+    float2 *sm = smem;
+    float2 *tw = smem + ca.pl.M;
+    const int M = SP ? Plan24000::M : ca.pl.M;
+    const int c = blockIdx.x, tl = blockIdx.y, task = a.task0 + tl;
+    const int prn = task % a.n_prn, b = task / a.n_prn;
+    load_twiddles(tw, ca.tw, ca.pl.twtot);
+    const float2 *src = a.W + ((size_t)tl * a.R + c) * M;
+    if ((M & 1) == 0) {
+        const float4 *s4 = (const float4 *)src;
+        float4 *d4 = (float4 *)sm;
+        for (int i = threadIdx.x; i < M / 2; i += blockDim.x) d4[i] = __ldg(s4 + i);
+    } else {
+        for (int i = threadIdx.x; i < M; i += blockDim.x) sm[i] = __ldg(src + i);
+    }
+    __syncthreads();
+    if (MODE == 0) {
+        float *row = ca.P + (size_t)prn * ca.prn_stride + (size_t)b * ca.bin_stride;
+        StorePowerRt st{row, c, a.R, ca.Nmax, ca.accumulate || a.s > 0};
+        if constexpr (SP == 1) fft_inverse_static<Plan24000>(sm, tw, st);
+        else fft_inverse(sm, tw, ca.pl, st);
+    } else {
+        StoreComplexRt st{ca.Y + (size_t)b * a.R * M, c, a.R};
+        if constexpr (SP == 1) fft_inverse_static<Plan24000>(sm, tw, st);
+        else fft_inverse(sm, tw, ca.pl, st);
+    }
+}
+
 // out[p][j][q] = code_nat[p][k(q) + j M] (permuted order of the DIF output)
 __global__ void perm_code_kernel(const float2 *code_nat, const int *kperm, int M,
                                  int R, int n_prn, float2 *out)
@@ -382,6 +493,75 @@ static int launch_cons(const FftPlan *pl, const ConsArgs &a, int n_tasks, cudaSt
     }
 }
 
+template <int MODE, int SP>
+static int set_stage_attr()
+{
+    static bool done = false;
+    if (!done) {
+        SDRG_CUDA(cudaFuncSetAttribute(stage_ifft_kernel<MODE, SP>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(g_smem_limit())));
+        done = true;
+    }
+    return SDRG_OK;
+}
+
+// Tasks of a staged split (R > 8) in chunks of w_tasks, each chunk through
+// the scratch W (w_tasks * L complex), sum by sum.
+template <int MODE>
+static int launch_staged(const FftPlan *pl, const ConsArgs &ca, int n_tasks, cudaStream_t st,
+                         float2 *W, int w_tasks)
+{
+    if (!W || w_tasks <= 0) return set_error(SDRG_ERR_ARG, "staged FFT split without scratch");
+    const bool sp = Plan24000::matches(pl->k, pl->threads);
+    int e;
+    if ((e = sp ? set_stage_attr<MODE, 1>() : set_stage_attr<MODE, 0>())) return e;
+    StageArgs sa = {};
+    sa.split = pl->split_dev; sa.X = ca.X; sa.code = ca.code;
+    sa.R = pl->R; sa.M = pl->M; sa.n_prn = ca.n_prn - ca.prn0; sa.n_bin = ca.n_bin;
+    sa.n_sum = ca.n_sum; sa.scale = ca.scale; sa.W = W;
+    for (int t0 = 0; t0 < n_tasks; t0 += w_tasks) {
+        const int n = n_tasks - t0 < w_tasks ? n_tasks - t0 : w_tasks;
+        for (int s = 0; s < ca.n_sum; ++s) {
+            sa.task0 = t0;
+            sa.s = s;
+            const dim3 gc((unsigned)((pl->M + 255) / 256), (unsigned)n);
+            switch (pl->R) {
+            case 10: stage_combine_kernel<10><<<gc, 256, 0, st>>>(sa); break;
+            case 12: stage_combine_kernel<12><<<gc, 256, 0, st>>>(sa); break;
+            case 15: stage_combine_kernel<15><<<gc, 256, 0, st>>>(sa); break;
+            case 16: stage_combine_kernel<16><<<gc, 256, 0, st>>>(sa); break;
+            case 20: stage_combine_kernel<20><<<gc, 256, 0, st>>>(sa); break;
+            default: return set_error(SDRG_ERR_ARG, "unsupported staged split %d", pl->R);
+            }
+            SDRG_CUDA(cudaGetLastError());
+            const dim3 gi((unsigned)pl->R, (unsigned)n);
+            if (sp) stage_ifft_kernel<MODE, 1><<<gi, pl->threads, pl->smem, st>>>(ca, sa);
+            else stage_ifft_kernel<MODE, 0><<<gi, pl->threads, pl->smem, st>>>(ca, sa);
+            SDRG_CUDA(cudaGetLastError());
+        }
+    }
+    return SDRG_OK;
+}
+
+// the consumer for any plan: cluster exchange for R <= 8, staged otherwise
+template <int MODE>
+static int launch_consumer(const FftPlan *pl, const ConsArgs &ca, int n_tasks, cudaStream_t st,
+                           float2 *W, int w_tasks)
+{
+    if (pl->R <= 8) return launch_cons<MODE>(pl, ca, n_tasks, st);
+    return launch_staged<MODE>(pl, ca, n_tasks, st, W, w_tasks);
+}
+
+// scratch tasks for a staged split: about 256 MB of L2/HBM-resident sub-spectra
+static int staged_chunk(const FftPlan *pl, int n_tasks)
+{
+    if (pl->R <= 8) return 0;
+    long c = (256L << 20) / ((long)pl->L * (long)sizeof(float2));
+    if (c < 1) c = 1;
+    return (int)(c < n_tasks ? c : n_tasks);
+}
+
 static int perm_code(const FftPlan *pl, const float2 *nat, int n_prn, float2 *out,
                      cudaStream_t st)
 {
@@ -439,7 +619,10 @@ static int corr_fft_device(const char2 *iq_dev, const sdr_cpx_t *code_host, int 
     ca.pl = pl->k; ca.tw = pl->tw_dev; ca.split = pl->split_dev; ca.X = X;
     ca.code = code_perm; ca.n_prn = 1; ca.n_bin = 1; ca.n_sum = 1; ca.prn0 = 0;
     ca.scale = 1.0f / N / N; ca.Nmax = N; ca.Y = Y;
-    if ((e = launch_cons<1>(pl, ca, 1, st))) return e;
+    const int wt = staged_chunk(pl, 1);
+    if (wt && (e = c.dev[5].reserve((size_t)wt * cb))) return e;
+    if ((e = launch_consumer<1>(pl, ca, 1, st, wt ? (float2 *)c.dev[5].ptr : nullptr, wt)))
+        return e;
     SDRG_CUDA(cudaMemcpyAsync(c.host[0].ptr, Y, cb, cudaMemcpyDeviceToHost, st));
     SDRG_CUDA(cudaStreamSynchronize(st));
     memcpy(corr_host, c.host[0].ptr, cb);
@@ -457,6 +640,8 @@ struct GroupState {
     float2 *code = nullptr;             // [n_prn][R][M]
     float2 *X = nullptr;                // [n_bin][n_sum][R][M]
     float *P = nullptr;                 // [n_prn][n_bin][Nmax]
+    float2 *W = nullptr;                // staged splits: [w_tasks][R][M] sub-spectra
+    int w_tasks = 0;
     uint32_t *tab_dev = nullptr;        // phstep | ph0a | ph0b | (int) ix | nsplit
     uint32_t *tab_host = nullptr;       // pinned mirror
     size_t tab_words = 0;
@@ -710,7 +895,10 @@ void sdr_search_code(const sdr_cpx_t *code_fft, double T, const sdr_buff_t *buff
     ca.n_prn = 1; ca.n_bin = len_fds; ca.n_sum = 1; ca.prn0 = 0;
     ca.scale = 1.0f / N / N; ca.Nmax = N; ca.prn_stride = 0; ca.bin_stride = N;
     ca.accumulate = 1; ca.P = P_d;
-    if ((e = launch_cons<0>(pl, ca, len_fds, st))) return;
+    const int wt = staged_chunk(pl, len_fds);
+    if (wt && (e = c.dev[5].reserve((size_t)wt * cb))) return;
+    if ((e = launch_consumer<0>(pl, ca, len_fds, st, wt ? (float2 *)c.dev[5].ptr : nullptr, wt)))
+        return;
     if (cudaMemcpyAsync(c.host[2].ptr, P_d, pb, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess) {
         cuda_error(cudaGetLastError(), "sdr_search_code D2H");
@@ -768,6 +956,9 @@ sdrg_acq_plan_t *sdrg_acq_plan_new(const sdrg_acq_sig_t *sigs, int n_sig)
                   cudaMalloc(&nat, (size_t)s.n_prn * L * sizeof(float2)) == cudaSuccess &&
                   cudaMalloc(&G.X, (size_t)s.len_fds * s.n_sum * L * sizeof(float2)) == cudaSuccess &&
                   cudaMalloc(&G.P, (size_t)s.n_prn * s.len_fds * s.Nmax * sizeof(float)) == cudaSuccess;
+        G.w_tasks = staged_chunk(G.pl, s.n_prn * s.len_fds);
+        ok = ok && (!G.w_tasks ||
+                    cudaMalloc(&G.W, (size_t)G.w_tasks * L * sizeof(float2)) == cudaSuccess);
         G.tab_words = 2 * (size_t)s.len_fds + (size_t)s.len_fds * s.n_sum + 2 * (size_t)s.n_sum + s.len_fds;
         ok = ok && cudaMalloc(&G.tab_dev, G.tab_words * 4) == cudaSuccess &&
              cudaMallocHost(&G.tab_host, G.tab_words * 4) == cudaSuccess &&
@@ -818,6 +1009,7 @@ void sdrg_acq_plan_free(sdrg_acq_plan_t *plan)
         if (G.code) cudaFree(G.code);
         if (G.X) cudaFree(G.X);
         if (G.P) cudaFree(G.P);
+        if (G.W) cudaFree(G.W);
         if (G.tab_dev) cudaFree(G.tab_dev);
         if (G.tab_host) cudaFreeHost(G.tab_host);
         if (G.tab_ev) cudaEventDestroy(G.tab_ev);
@@ -903,7 +1095,7 @@ int sdrg_acq_run(sdrg_acq_plan_t *plan, const uint8_t *const *if_dev, const int 
         ca.prn_stride = (size_t)nb * s.Nmax; ca.bin_stride = s.Nmax;
         ca.accumulate = 0; ca.P = G.P;
         if ((e = prof_begin(plan, st, ev))) return e;
-        if ((e = launch_cons<0>(G.pl, ca, s.n_prn * nb, st))) return e;
+        if ((e = launch_consumer<0>(G.pl, ca, s.n_prn * nb, st, G.W, G.w_tasks))) return e;
         if ((e = prof_end(plan, st, ev, 3 * (int)gi + 1))) return e;
         const float *fd_dev = (const float *)(G.tab_dev + G.tab_words - nb);
         if ((e = prof_begin(plan, st, ev))) return e;

@@ -177,6 +177,56 @@ def acq_multi_24mhz(seed: int = 2, prn_limit: int | None = None, t_sum: float = 
     return Workload("acq_multi_24mhz", fs, True, bufs, groups, sats, [0] * n_buf)
 
 
+def long_replica_fft(sig: str, prn: int, fs: float, t_coh: float, L: int) -> np.ndarray:
+    """Conjugated DFT of a t_coh-second replica for long coherent integration:
+    the primary code repeated over t_coh with a seeded +-1 overlay per primary
+    period (standing in for a secondary code such as L5's NH sequences) and,
+    for codes longer than t_coh allows to repeat whole, simply truncated."""
+    chips = codes.gen_code(sig, prn).astype(np.float64)
+    Lc, T = codes.SIGNALS[sig]
+    n = int(round(fs * t_coh))
+    t = np.arange(n, dtype=np.float64)
+    per = np.floor(t * (1.0 / (T * fs))).astype(np.int64)            # primary period index
+    idx = (np.floor(t * (Lc / (T * fs))).astype(np.int64)) % Lc
+    ov = np.random.default_rng(sum(map(ord, sig)) * 7 + prn).choice([-1.0, 1.0], per.max() + 1)
+    x = np.zeros(L, np.complex128)
+    x[:n] = chips[idx] * ov[per]
+    return np.conj(np.fft.fft(x)).astype(np.complex64)
+
+
+def acq_long_48mhz(seed: int = 6, prn_limit: int | None = None, n_sum: int = 20,
+                   bins: np.ndarray | None = None) -> Workload:
+    """Weak-signal long coherent search: 48 MHz complex IQ, 3-bit, GPS L5-Q
+    (stand-in codes, 1 ms primary with a per-ms overlay) and QZSS L6D (stand-in
+    TDM code, 4 ms) at C/N0 25-32 dB-Hz; 10 ms coherent (480 000-sample FFTs)
+    x n_sum non-coherent sums over +-10 kHz in 50 Hz bins."""
+    fs, bits, t_coh = 48e6, 3, 10e-3
+    fi_of = {"L5Q": 0.0, "L6D": 5.0e6}
+    rng = np.random.default_rng(seed)
+    L = int(round(fs * t_coh))
+    fds = np.arange(-10000, 10001, 50, dtype=np.float32) if bins is None else np.asarray(bins, np.float32)
+    sats, groups = [], []
+    for sig in ("L5Q", "L6D"):
+        prns = list(codes.PRN_SETS[sig])
+        if prn_limit:
+            prns = prns[:prn_limit]
+        vis = sorted(rng.choice(prns, min(4, len(prns)), replace=False).tolist())
+        for p in vis:
+            sats.append(Sat(sig, int(p), float(rng.uniform(0, codes.SIGNALS[sig][0])),
+                            float(rng.uniform(-9000, 9000)), float(rng.uniform(0, 1)),
+                            float(rng.uniform(25, 32)), 0))
+        groups.append(Group(sig, prns, fs, fi_of[sig], t_coh, L, L, L, n_sum, fds, 0))
+    buf = gen_if(L * (n_sum + 1), fs, fi_of, sats, iq=True, bits=bits, seed=seed * 10)
+    return Workload("acq_long_48mhz", fs, True, [buf], groups, sats, [0])
+
+
+def long_code_ffts(g: Group) -> np.ndarray:
+    out = np.empty((len(g.prns), g.L), np.complex64)
+    for i, p in enumerate(g.prns):
+        out[i] = long_replica_fft(g.sig, p, g.fs, g.T, g.L)
+    return out
+
+
 @dataclass
 class TrackChannel:
     sig: str
