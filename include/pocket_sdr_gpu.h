@@ -263,6 +263,76 @@ int sdrg_corr_batch(const sdrg_corr_job_t *jobs, int n_job, const uint8_t *const
 int sdrg_acq_run_host(sdrg_acq_plan_t *plan, const uint8_t *const *if_host,
     const int *len_if, const int *ix, sdrg_acq_result_t *res_host);
 
+/* ---- differentiable refinement (no reference counterpart) ------------------
+ * The reference stops at the acquisition grid (peak, C/N0 and the three-bin
+ * Doppler quadratic of src/sdr_func.c:709-744). These calls refine code
+ * delay, Doppler and carrier phase of many signals at once from that peak.
+ * Model of one signal over samples n of a packed IF buffer, t = n / fs:
+ *   psi(t) / 2 pi = fi t + fd (t - t_ref) + phi
+ *   u(t) = rate (t - t_ref) + rate_nom (t_ref - tau) - 1/2   (chips)
+ *   replica = chips linearly interpolated at u (through the chip centres)
+ * theta = {tau (s), fd (Hz), phi (cycles at t_ref)} per signal, in double;
+ * `rate` (chips/s) per signal is the code rate the model uses and is not
+ * differentiated. The span is K blocks of Nb samples from ix0; t_ref =
+ * (ix0 + K Nb / 2) / fs. Per (signal, block k) the FP32 sums are
+ *   {Re C, Im C, Re D, Im D, Re E, Im E, Q, Qt, Qtt, R, P, 0}
+ *   C = sum x c e^{-j psi}, D = sum x dc e^{-j psi}, E = sum t' x c e^{-j psi},
+ *   Q = sum c^2, Qt = sum t' c^2, Qtt = sum t'^2 c^2, R = sum c dc,
+ *   P = sum dc^2, with dc = chip[i+1] - chip[i] and t' the time from the
+ *   block centre; so dC/dtau = -rate_nom D, dC/dphi = -2 pi j C and
+ *   dC/dfd = -2 pi j (E + (t_k - t_ref) C), t_k = block centre. */
+typedef struct {
+    const int8_t *chips;   /* HOST: Lc chip values (+-1 or 0), copied */
+    int Lc;                /* chips per code period (2..65536) */
+    double rate;           /* nominal chip rate (chips/s) */
+    double fi;             /* IF (Hz) */
+    double fc;             /* RF carrier (Hz) for a carrier-aided code rate; 0: none */
+} sdrg_refine_sig_t;
+
+typedef struct sdrg_refine_plan sdrg_refine_plan_t;
+
+/* Uploads the signals' chips; iq: 1 complex samples, 0 real (Q nibble
+ * ignored). Returns NULL on error (see sdr_gpu_last_error). */
+sdrg_refine_plan_t *sdrg_refine_plan_new(const sdrg_refine_sig_t *sigs, int n_sig,
+    double fs, int iq, int Nb, int K);
+void sdrg_refine_plan_free(sdrg_refine_plan_t *plan);
+
+/* out4 = {n_sig, K, Nb, CTAs per block}. */
+int sdrg_refine_plan_info(const sdrg_refine_plan_t *plan, int *out4);
+
+/* Block sums on `stream` (a cudaStream_t; NULL = the legacy default stream,
+ * for every sdrg_refine_* call), all DEVICE
+ * pointers: if_dev (len_if samples; the span must lie inside, no wrap),
+ * theta_dev [n_sig][3] and rate_dev [n_sig] doubles; mode 0 writes C only
+ * (out_dev [n_sig][K][2] floats), mode 1 all twelve ([n_sig][K][12]).
+ * Asynchronous; allocates nothing. */
+int sdrg_refine_sums(sdrg_refine_plan_t *plan, const uint8_t *if_dev, int len_if, int ix0,
+    const double *theta_dev, const double *rate_dev, int mode, float *out_dev, void *stream);
+
+/* Vector-Jacobian product of the block correlations: grad_dev[n_sig][3]
+ * (double) = d/dtheta sum_k Re(conj(g_k) C_k), from mode-1 sums and g_dev
+ * [n_sig][K][2] floats (the upstream gradient of (Re C_k, Im C_k)). */
+int sdrg_refine_vjp(sdrg_refine_plan_t *plan, const float *sums_dev, const float *g_dev,
+    double *grad_dev, void *stream);
+
+/* n_step Gauss-Newton steps, step i in model models[i] (HOST array):
+ *   0  correlation-power loss: complex amplitude per block (carrier phase
+ *      not observable; only tau and fd move);
+ *   1  coherent: one real amplitude and a common carrier phase;
+ *   2  coherent with a real amplitude per block (data-bit signs).
+ * Each step recomputes the mode-1 sums, folds the closed-form carrier phase
+ * into phi, eliminates the least-squares amplitudes, solves the 3x3 normal
+ * equations of (tau, fd, phi) in FP64, clamps the step to +-0.5 chip and
+ * +-fs / (4 Nb) Hz, and sets rate = rate_nom (1 + fd / fc) when fc > 0.
+ * theta_dev and rate_dev are updated in place; info_dev (may be NULL)
+ * receives [n_step][n_sig][5] doubles {power sum_k |C_k|^2 before the step,
+ * d tau (chips), d fd (Hz), d phi (cycles), 1 if the system was solved}.
+ * Asynchronous, two kernel launches per step, no allocation and no host
+ * synchronisation (capturable in a CUDA graph). */
+int sdrg_refine_gn(sdrg_refine_plan_t *plan, const uint8_t *if_dev, int len_if, int ix0,
+    double *theta_dev, double *rate_dev, const int *models, int n_step, double *info_dev,
+    void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -82,6 +82,8 @@ class Restatement:
         L.orc_dop_bins.argtypes = [_d, _f, _f, _p]
         L.orc_res_code.argtypes = [_p, _p, _i, _d, _d, _d, _i, _i, _p]
         L.orc_gen_code_fft.argtypes = [_p, _p, _i, _d, _d, _d, _i, _i, _p]
+        L.orc_refine_sums.argtypes = [_p, _i, _d, _d, _d, _p, _p, _i, _d, _i, _i, _i, _p]
+        L.orc_refine_step.argtypes = [_p, _i, _i, _d, _d, _d, _i, _p, _p, _p]
         L.orc_init()
 
     def mix_table(self) -> np.ndarray:
@@ -183,6 +185,68 @@ class Restatement:
         self.lib.orc_gen_code_fft(_ptr(code_I), None if cq is None else _ptr(cq),
                                   len(code_I), T, coff, fs, N, Nz, _ptr(out))
         return out
+
+    # ---- refinement model (refine_oracle.c; FP64, no reference counterpart) --
+
+    REFINE_W = 12
+
+    def refine_sums(self, chips, rate_nom, rate, fi, theta, buf, iq, fs, ix0, Nb, K):
+        """float64 [K, 12] block sums of one signal (see refine_oracle.c)."""
+        chips = np.ascontiguousarray(chips, np.int8)
+        buf = np.ascontiguousarray(buf, np.uint8)
+        th = np.ascontiguousarray(theta, np.float64)
+        if ix0 < 0 or ix0 + K * Nb > len(buf):
+            raise ValueError("refine span outside the buffer")
+        out = np.zeros((K, self.REFINE_W), np.float64)
+        self.lib.orc_refine_sums(_ptr(chips), len(chips), rate_nom, rate, fi, _ptr(th),
+                                 _ptr(buf), int(iq), fs, ix0, Nb, K, _ptr(out))
+        return out
+
+    def refine_step(self, sums, Nb, fs, rate_nom, fc, theta, rate, model=1):
+        """One Gauss-Newton step (model 0 power, 1 coherent, 2 coherent with
+        per-block signs): returns (theta', rate', info[5])."""
+        sums = np.ascontiguousarray(sums, np.float64)
+        th = np.array(theta, np.float64)
+        r = np.array([rate], np.float64)
+        info = np.zeros(5, np.float64)
+        self.lib.orc_refine_step(_ptr(sums), sums.shape[0], Nb, fs, rate_nom, fc,
+                                 int(model), _ptr(th), _ptr(r), _ptr(info))
+        return th, float(r[0]), info
+
+    @staticmethod
+    def refine_corr(sums):
+        """Complex C_k of block sums."""
+        return sums[:, 0] + 1j * sums[:, 1]
+
+    @staticmethod
+    def refine_vjp(sums, g, rate_nom, Nb, fs):
+        """FP64 vector-Jacobian product: d/dtheta of sum_k Re(conj(g_k) C_k)
+        for upstream gradients g_k (complex) - the analytic gradient the GPU
+        backward computes, from FP64 sums. dC/dtau = -rate_nom D,
+        dC/dfd = -2 pi j (E + dt_k C), dC/dphi = -2 pi j C."""
+        K = sums.shape[0]
+        Cc = sums[:, 0] + 1j * sums[:, 1]
+        D = sums[:, 2] + 1j * sums[:, 3]
+        E = sums[:, 4] + 1j * sums[:, 5]
+        dt = (np.arange(K) + 0.5 - 0.5 * K) * Nb / fs
+        g = np.asarray(g, np.complex128)
+        d_tau = np.sum(np.real(np.conj(g) * (-rate_nom * D)))
+        d_fd = np.sum(np.real(np.conj(g) * (-2j * np.pi * (E + dt * Cc))))
+        d_phi = np.sum(np.real(np.conj(g) * (-2j * np.pi * Cc)))
+        return np.array([d_tau, d_fd, d_phi])
+
+    def refine_gn(self, chips, rate_nom, fc, fi, theta, buf, iq, fs, ix0, Nb, K, models):
+        """Gauss-Newton steps from theta, one per entry of `models` (the model
+        of each step); the code rate follows the carrier. Returns
+        (theta, rate, [info per step])."""
+        th = np.array(theta, np.float64)
+        rate = rate_nom * (1.0 + th[1] / fc) if fc > 0 else rate_nom
+        infos = []
+        for m in models:
+            s = self.refine_sums(chips, rate_nom, rate, fi, th, buf, iq, fs, ix0, Nb, K)
+            th, rate, info = self.refine_step(s, Nb, fs, rate_nom, fc, th, rate, model=m)
+            infos.append(info)
+        return th, rate, infos
 
 
 class Reference:

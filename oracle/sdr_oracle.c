@@ -3,6 +3,8 @@
  * correlation hot path. See sdr_oracle.h. This file is test infrastructure:
  * the shipped library (pocketsdr_b200) never links or calls it.
  *
+ * The refinement model (no reference counterpart) lives in refine_oracle.c.
+ *
  * Built with -ffp-contract=off so that every fused multiply-add below is an
  * explicit fma() call, written where the reference build (gcc -O3 -mfma,
  * GNU C default -ffp-contract=fast) contracts the same expression.

@@ -89,6 +89,26 @@ void orc_gen_code_fft(const int8_t *code_I, const int8_t *code_Q,
                       int len_code, double T, double coff, double fs, int N,
                       int Nz, float *code_fft);
 
+/* ---- refinement model (refine_oracle.c; no reference counterpart) ------- */
+#define ORC_REFINE_W 12    /* sums per block */
+
+/* FP64 per-block sums for one signal: out[k * 12 + i] =
+ * {Re C, Im C, Re D, Im D, Re E, Im E, Q, Qt, Qtt, R, P, 0} with
+ * C = sum x c e^{-j psi}, D = sum x dc e^{-j psi}, E = sum t' x c e^{-j psi},
+ * Q = sum c^2, Qt = sum t' c^2, Qtt = sum t'^2 c^2, R = sum c dc,
+ * P = sum dc^2; dc = chip[i+1] - chip[i]; theta = {tau (s), fd (Hz),
+ * phi (cycles at t_ref)}. */
+void orc_refine_sums(const int8_t *chips, int Lc, double rate_nom, double rate,
+                     double fi, const double *theta, const uint8_t *buf, int iq,
+                     double fs, int ix0, int Nb, int K, double *out);
+
+/* One Gauss-Newton step from the block sums (model 0: power loss with
+ * complex block amplitudes; 1: one real amplitude and a common carrier phase;
+ * 2: real block amplitudes and a common carrier phase); updates theta and
+ * rate, info[5] = {power, d tau (chips), d fd (Hz), d phi (cycles), solved}. */
+void orc_refine_step(const double *sums, int K, int Nb, double fs, double rate_nom,
+                     double fc, int model, double *theta, double *rate, double *info);
+
 #ifdef __cplusplus
 }
 #endif

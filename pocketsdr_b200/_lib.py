@@ -36,6 +36,11 @@ class AcqResult(C.Structure):
                 ("pave", _d), ("fd", _d)]
 
 
+class RefineSig(C.Structure):
+    """sdrg_refine_sig_t."""
+    _fields_ = [("chips", _p), ("Lc", _i), ("rate", _d), ("fi", _d), ("fc", _d)]
+
+
 # every exported entry point and its signature; tests check the library
 # exports exactly these names
 SIGNATURES = {
@@ -66,6 +71,12 @@ SIGNATURES = {
     "sdrg_acq_profile_get": ([_p, _p, _p], _i),
     "sdrg_acq_run_host": ([_p, _p, _p, _p, _p], _i),
     "sdrg_corr_batch": ([_p, _i, _p, _p, _p, _p, _p], _i),
+    "sdrg_refine_plan_new": ([C.POINTER(RefineSig), _i, _d, _i, _i, _i], _p),
+    "sdrg_refine_plan_free": ([_p], None),
+    "sdrg_refine_plan_info": ([_p, _p], _i),
+    "sdrg_refine_sums": ([_p, _p, _i, _i, _p, _p, _i, _p, _p], _i),
+    "sdrg_refine_vjp": ([_p, _p, _p, _p, _p], _i),
+    "sdrg_refine_gn": ([_p, _p, _i, _i, _p, _p, _p, _i, _p, _p], _i),
 }
 
 

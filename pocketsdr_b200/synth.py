@@ -220,6 +220,105 @@ def acq_long_48mhz(seed: int = 6, prn_limit: int | None = None, n_sum: int = 20,
     return Workload("acq_long_48mhz", fs, True, [buf], groups, sats, [0])
 
 
+@dataclass
+class RefineSat:
+    sig: str
+    prn: int
+    tau: float            # code delay (s): code phase rate_nom (t_ref - tau) at t_ref
+    doppler: float        # Hz
+    phase: float          # carrier phase at t_ref (cycles)
+    cn0: float            # dB-Hz
+
+
+@dataclass
+class RefineWorkload:
+    """Delay / Doppler / phase refinement: one IF record, the satellites in
+    it, the acquisition groups that give the starting grid peaks and the
+    refinement span (K blocks of Nb samples from ix0)."""
+    name: str
+    fs: float
+    fi: float
+    iq: bool
+    buf: np.ndarray
+    sats: list
+    groups: list
+    Nb: int
+    K: int
+    ix0: int = 0
+
+    @property
+    def t_ref(self) -> float:
+        return (self.ix0 + 0.5 * self.K * self.Nb) / self.fs
+
+
+def code_rate(sig: str) -> float:
+    L, T = codes.SIGNALS[sig]
+    return L / T
+
+
+def refine_signal(sig: str, prn: int, fs: float, fi: float, n: int, tau: float, fd: float,
+                  phi: float, t_ref: float) -> np.ndarray:
+    """Unit-amplitude complex signal of one satellite: rectangular chips at
+    the carrier-aided code rate, chip phase rate_nom (t_ref - tau) at t_ref,
+    carrier phase fi t + fd (t - t_ref) + phi cycles."""
+    chips = codes.gen_code(sig, prn).astype(np.float64)
+    Lc = len(chips)
+    rn = code_rate(sig)
+    rate = rn * (1.0 + fd / CARRIER[sig])
+    t = np.arange(n, dtype=np.float64) / fs
+    u = rate * (t - t_ref) + rn * (t_ref - tau)
+    idx = np.floor(u).astype(np.int64) % Lc
+    cyc = fi * t + fd * (t - t_ref) + phi
+    return chips[idx] * np.exp(2j * np.pi * (cyc - np.floor(cyc)))
+
+
+def refine_12mhz(seed: int = 4, n_l1ca: int = 32, n_e1b: int = 32,
+                 cn0=(30.0, 45.0)) -> RefineWorkload:
+    """12 MHz real IF at 3 MHz, 2-bit, GPS L1 C/A and Galileo E1-B (stand-in
+    codes, BOC(1,1)) satellites at C/N0 U[30, 45] dB-Hz with off-grid delay
+    and Doppler (U[-4500, 4500] Hz); refinement over 10 ms coherent x 4
+    blocks. Starting grid: L1 C/A 10 ms coherent (N = 120 000, 2N FFT) x 4
+    sums in 50 Hz bins, E1-B 8 ms (two code periods, N = 96 000) x 5 sums in
+    62.5 Hz bins (coherent windows must advance by whole code periods), both
+    over +-5 kHz. No data-bit modulation."""
+    fs, fi, bits = 12e6, 3e6, 2
+    Nb, K = 120000, 4
+    rng = np.random.default_rng(seed)
+    n = 5 * Nb
+    t_ref = 0.5 * K * Nb / fs
+    sats = []
+    for sig, cnt in (("L1CA", n_l1ca), ("E1B", n_e1b)):
+        T = codes.code_cyc(sig)
+        for p in list(codes.PRN_SETS[sig])[:cnt]:
+            sats.append(RefineSat(sig, int(p), float(rng.uniform(0, T)),
+                                  float(rng.uniform(-4500, 4500)), float(rng.uniform(0, 1)),
+                                  float(rng.uniform(*cn0))))
+    x = rng.standard_normal(n)
+    n0 = 2.0 / fs
+    for s in sats:
+        amp = np.sqrt(2 * 10 ** (s.cn0 / 10) * n0)
+        x += amp * refine_signal(s.sig, s.prn, fs, fi, n, s.tau, s.doppler, s.phase, t_ref).real
+    buf = pack(_quant(x, bits), None)
+    groups = []
+    for sig, T, n_sum in (("L1CA", 10e-3, 4), ("E1B", 8e-3, 5)):
+        prns = [s.prn for s in sats if s.sig == sig]
+        if not prns:
+            continue
+        N = int(round(fs * T))
+        groups.append(Group(sig, prns, fs, fi, T, N, 2 * N, N, n_sum, dop_bins(T, 0.0, 5000.0), 0))
+    return RefineWorkload("refine_12mhz", fs, fi, False, buf, sats, groups, Nb, K, 0)
+
+
+def periodic_code_ffts(g: Group) -> np.ndarray:
+    """Conjugated DFTs of the code repeated over the group's N samples
+    (nearest-chip resampling wraps modulo the code length), zero padded to L."""
+    out = np.empty((len(g.prns), g.L), np.complex64)
+    for i, p in enumerate(g.prns):
+        out[i] = codes.gen_code_fft(codes.gen_code(g.sig, p), codes.code_cyc(g.sig), 0.0,
+                                    g.fs, g.N, g.L - g.N)
+    return out
+
+
 def long_code_ffts(g: Group) -> np.ndarray:
     out = np.empty((len(g.prns), g.L), np.complex64)
     for i, p in enumerate(g.prns):
