@@ -109,32 +109,50 @@ def test_refine_vjp_matches_fp64_gradient(orc, wl):
         assert np.all(np.abs(grad[i] - gr) <= tol), (grad[i], gr, tol)
 
 
+def _central(f, theta, j, h):
+    import torch
+    st = torch.zeros_like(theta)
+    st[:, j] = torch.from_numpy(np.asarray(h, np.float64)).cuda()
+    return ((f(theta + st) - f(theta - st)) / (2 * st[:, j])).cpu().numpy()
+
+
 def test_autograd_backward_matches_gpu_central_differences():
     """torch.autograd through CorrBlocks against central differences of the
-    GPU forward itself, for a random linear functional of the C_k (every
-    theta component, carrier phase included)."""
+    GPU forward itself: the correlation-power loss for delay and Doppler, a
+    random linear functional of the C_k for Doppler and carrier phase (the
+    power loss has no phase gradient). The delay step is small against the
+    chip (the model is piecewise linear in tau) and the signals strong, so
+    that chip-centre crossings inside the step stay far below 2 %."""
     import torch
-    from pocketsdr_b200.refine import corr_blocks
+    from pocketsdr_b200.refine import corr_blocks, corr_power
     w1 = synth.refine_12mhz(seed=32, n_l1ca=2, n_e1b=2, cn0=(44.0, 45.0))
     rng = np.random.default_rng(3)
     th = _perturbed(w1, rng, 0.3, 15.0, lo=0.4)
     plan, buf, theta, rate = _setup(w1, th)
+    rn = np.array([synth.code_rate(s.sig) for s in w1.sats])
+
+    x = theta.clone().requires_grad_(True)
+    corr_power(plan, buf, w1.ix0, x, rate).sum().backward()
+    grad = x.grad.cpu().numpy()
+
+    def power(t):
+        with torch.no_grad():
+            return corr_power(plan, buf, w1.ix0, t, rate).double()
+
+    np.testing.assert_allclose(grad[:, 0], _central(power, theta, 0, 5e-5 / rn), rtol=0.02)
+    np.testing.assert_allclose(grad[:, 1], _central(power, theta, 1, [0.05] * plan.n), rtol=0.01)
+
     g = torch.from_numpy(rng.standard_normal((plan.n, plan.K, 2)).astype(np.float32)).cuda()
     x = theta.clone().requires_grad_(True)
     (corr_blocks(plan, buf, w1.ix0, x, rate) * g).sum().backward()
     grad = x.grad.cpu().numpy()
 
-    def f(t):
+    def lin(t):
         with torch.no_grad():
             return (corr_blocks(plan, buf, w1.ix0, t, rate).double() * g.double()).sum(dim=(1, 2))
 
-    for j, h in ((0, None), (1, 0.05), (2, 1e-3)):
-        step = np.zeros((plan.n, 3))
-        for i, s in enumerate(w1.sats):
-            step[i, j] = (2e-4 / synth.code_rate(s.sig)) if j == 0 else h
-        st = torch.from_numpy(step).cuda()
-        fd = ((f(theta + st) - f(theta - st)) / (2 * st[:, j])).cpu().numpy()
-        np.testing.assert_allclose(grad[:, j], fd, rtol=0.02)
+    np.testing.assert_allclose(grad[:, 1], _central(lin, theta, 1, [0.05] * plan.n), rtol=0.01)
+    np.testing.assert_allclose(grad[:, 2], _central(lin, theta, 2, [1e-3] * plan.n), rtol=0.01)
 
 
 def test_power_loss_phase_gradient_is_zero(wl):
