@@ -2,7 +2,12 @@
 """Benchmark: batched multi-GNSS acquisition cells/s on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload acq_multi_24mhz|acq_l1ca_12mhz]
+                    [--workload acq_multi_24mhz|acq_l1ca_12mhz|track_24mhz|refine_12mhz]
+
+Besides the default acquisition workload: track_24mhz times the batched
+tracking correlators (channel-epochs/s) and refine_12mhz the grid search plus
+Gauss-Newton refinement of 64 signals (signals/s, with the refinement's cost
+against the grid and its agreement with the FP64 oracle).
 
 A step is one full search of the workload: every PRN of every signal group x
 every Doppler bin x every code offset, accumulated over all non-coherent sums,
@@ -492,12 +497,201 @@ def run_track(args):
     return 0
 
 
+REFINE_METRIC = ("refined signals/s: grid search + 5 Gauss-Newton steps of (tau, fd, phi), "
+                 "10 ms coherent x 4 blocks")
+REFINE_FLOPS_PER_SAMPLE = 60   # mode-1 sums: sincos ~20, mixing 4, code 3, 11 accumulators ~33
+
+
+def _fp64_refine(wl, th0, models):
+    """The FP64 oracle's Gauss-Newton from th0 for every signal, threads over
+    signals (the C oracle releases the GIL). Returns (theta [n, 3], wall s,
+    threads)."""
+    import concurrent.futures as cf
+    from oracle.oracle import Restatement
+    from pocketsdr_b200 import codes, synth
+    orc = Restatement()
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+
+    def one(i):
+        s = wl.sats[i]
+        th, _, _ = orc.refine_gn(codes.gen_code(s.sig, s.prn), synth.code_rate(s.sig),
+                                 synth.CARRIER[s.sig], wl.fi, th0[i], wl.buf, wl.iq, wl.fs,
+                                 wl.ix0, wl.Nb, wl.K, models)
+        return th
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=cores) as ex:
+        out = np.array(list(ex.map(one, range(len(wl.sats)))))
+    return out, time.perf_counter() - t0, cores
+
+
+def run_refine(args):
+    """Differentiable-refinement workload: 64 GPS L1 C/A + Galileo E1-B
+    signals at 12 MHz (C/N0 30-45 dB-Hz, off-grid delay and Doppler). A step
+    is the plain grid search (10 ms / 8 ms coherent, +-5 kHz) of all 64 PRNs
+    followed by 5 Gauss-Newton steps from its peaks; the line reports both
+    parts, their cost ratio and the refinement's agreement with the FP64
+    oracle and with the truth."""
+    import torch
+    from pocketsdr_b200 import acquire, codes, synth
+    from pocketsdr_b200.refine import RefinePlan, RefineSpec
+    rank, world, local = dist_info()
+    torch.cuda.set_device(local)
+    wl = synth.refine_12mhz(seed=4 + rank)
+    n = len(wl.sats)
+    models = [1] * 5
+    acq = acquire.AcqPlan(wl.groups, [synth.periodic_code_ffts(g) for g in wl.groups])
+    specs = [RefineSpec(codes.gen_code(s.sig, s.prn), synth.code_rate(s.sig), wl.fi,
+                        synth.CARRIER[s.sig]) for s in wl.sats]
+    plan = RefinePlan(specs, wl.fs, wl.iq, wl.Nb, wl.K)
+    st = torch.cuda.Stream()
+    torch.cuda.set_stream(st)
+    buf_d = torch.from_numpy(wl.buf).cuda()
+    res_d = torch.empty(n * acquire.RESULT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    theta = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
+    rate = torch.zeros(n, dtype=torch.float64, device="cuda")
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+
+    def grid():
+        acq.run_device([buf_d.data_ptr()], [buf_d.numel()], [0], res_d.data_ptr(), st.cuda_stream)
+
+    def refine():
+        plan.from_peaks(res_d, 0, wl.ix0, theta, rate)
+        plan.gn(buf_d, wl.ix0, theta, rate, models, info=False)
+
+    for _ in range(args.warmup):
+        grid()
+        refine()
+    torch.cuda.synchronize()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    clk = ClockSampler(local)
+    clk.start()
+    for k in range(args.steps):
+        flush.fill_(k & 0xFF)
+        ev[k][0].record(st)
+        grid()
+        ev[k][1].record(st)
+        refine()
+        ev[k][2].record(st)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    grid_ms = sum(e[0].elapsed_time(e[1]) for e in ev) / args.steps
+    ref_ms = sum(e[1].elapsed_time(e[2]) for e in ev) / args.steps
+    # the sums kernel alone (mode 1), for its roofline
+    s_ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    flush.fill_(1)
+    s_ev[0].record(st)
+    for _ in range(10):
+        plan.sums(buf_d, wl.ix0, theta, rate, mode=1)
+    s_ev[1].record(st)
+    torch.cuda.synchronize()
+    sums_ms = s_ev[0].elapsed_time(s_ev[1]) / 10
+    step_ms = grid_ms + ref_ms
+    value = n / (step_ms / 1e3)
+
+    # end to end: host IF -> device, grid + refinement, theta -> host
+    buf_h = torch.from_numpy(wl.buf).pin_memory()
+    th_h = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+    e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.fill_((k + 1) & 0xFF)
+        e2e_ev[k][0].record(st)
+        buf_d.copy_(buf_h, non_blocking=True)
+        grid()
+        refine()
+        th_h.copy_(theta, non_blocking=True)
+        e2e_ev[k][1].record(st)
+    torch.cuda.synchronize()
+    e2e_ms = sum(a.elapsed_time(b) for a, b in e2e_ev) / args.steps
+
+    # parity with the FP64 oracle from the same starting peaks, and the truth
+    res = np.frombuffer(res_d.cpu().numpy().tobytes(), dtype=acquire.RESULT_DTYPE)
+    plan.from_peaks(res_d, 0, wl.ix0, theta, rate)
+    th0 = theta.cpu().numpy()
+    plan.gn(buf_d, wl.ix0, theta, rate, models, info=False)
+    th = theta.cpu().numpy()
+    line_extra = {}
+    if rank == 0 and not args.no_cpu_baseline:
+        th_ref, cpu_gn_s, cores = _fp64_refine(wl, th0, models)
+        div = np.array([2.0 if s.sig == "E1B" else 1.0 for s in wl.sats])
+        rn = np.array([synth.code_rate(s.sig) for s in wl.sats])
+        T = np.array([codes.code_cyc(s.sig) for s in wl.sats])
+        tau_t = np.array([s.tau for s in wl.sats])
+        fd_t = np.array([s.doppler for s in wl.sats])
+        e_tau = ((th[:, 0] - tau_t + T / 2) % T - T / 2) * rn / div
+        e0_tau = ((th0[:, 0] - tau_t + T / 2) % T - T / 2) * rn / div
+        line_extra["vs_fp64_oracle"] = {
+            "max_dtau_chip": float(np.max(np.abs(th[:, 0] - th_ref[:, 0]) * rn / div)),
+            "max_dfd_hz": float(np.max(np.abs(th[:, 1] - th_ref[:, 1]))),
+            "bar": "0.01 chip, 5 Hz"}
+        # truth statistics over the signals the grid acquired (peak within
+        # one chip and one 10 ms Doppler bin of the truth)
+        ok = (np.abs(e0_tau) < 1.0) & (np.abs(th0[:, 1] - fd_t) < 50.0)
+        line_extra["vs_truth"] = {
+            "acquired": int(ok.sum()),
+            "rms_dtau_chip": float(np.sqrt(np.mean(e_tau[ok] ** 2))),
+            "rms_dfd_hz": float(np.sqrt(np.mean((th[ok, 1] - fd_t[ok]) ** 2))),
+            "within_5hz": int(np.sum(np.abs(th[ok, 1] - fd_t[ok]) < 5.0)),
+            "start_rms_dtau_chip": float(np.sqrt(np.mean(e0_tau[ok] ** 2))),
+            "start_rms_dfd_hz": float(np.sqrt(np.mean((th0[ok, 1] - fd_t[ok]) ** 2)))}
+        if world == 1:
+            class _W:   # the grid's groups / buffers in cpu_reference_rate's shape
+                groups, bufs = wl.groups, [wl.buf]
+            rate_c, cores_c, kind, desc = cpu_reference_rate(_W, budget_prn=4)
+            cells = sum(len(g.prns) * len(g.fds) * g.Nmax for g in wl.groups)
+            cpu_grid_s = cells / rate_c          # both legs use every host core
+            cpu_s = cpu_grid_s + cpu_gn_s
+            line_extra["cpu_baseline"] = {
+                "value": n / cpu_s, "unit": "signals/s", "cores": cores_c,
+                "kind": kind + " grid + port FP64 Gauss-Newton",
+                "sample": desc + f"; Gauss-Newton: all {n} signals x 5 steps in the FP64 oracle "
+                                 f"({cpu_gn_s:.1f} s on {cores} threads)",
+                "grid_s": cpu_grid_s, "gn_s": cpu_gn_s}
+    samples = n * wl.K * wl.Nb
+    achieved = REFINE_FLOPS_PER_SAMPLE * samples / (sums_ms / 1e3) / 1e12
+    line = {"metric": REFINE_METRIC, "value": value, "unit": "signals/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "refine_12mhz", "signals": n, "coherent_ms": 10, "blocks": wl.K,
+                       "gn_steps": len(models), "model": "coherent (one real amplitude)",
+                       "grid": [f"{g.sig}:{len(g.prns)}prn x {len(g.fds)}bin x {g.Nmax}off x "
+                                f"{g.n_sum}sum L={g.L}" for g in wl.groups],
+                       "l2": "flushed between timed steps (512 MB write outside the events)"},
+            "grid_ms": grid_ms, "refine_ms": ref_ms, "cost_vs_grid": step_ms / grid_ms,
+            "sums_kernel_ms": sums_ms,
+            "e2e": {"value": n / (e2e_ms / 1e3), "unit": "signals/s",
+                    "h2d_bytes_per_step": int(buf_h.numel()), "d2h_bytes_per_step": n * 24},
+            "gpu_launches": None,
+            "roofline": {"kernel": "refine_sums_kernel<1> (per-sample model, derivatives, 11 sums)",
+                         "bound": "fp32", "achieved": achieved, "peak": FP32_NOMINAL_TFLOPS,
+                         "unit": "TFLOP/s", "frac": achieved / FP32_NOMINAL_TFLOPS,
+                         "flops_per_sample": REFINE_FLOPS_PER_SAMPLE, "samples": samples,
+                         "traffic": None},
+            "clocks": clocks, "detected": int(np.sum(res["cn0"] >= 30.0))}
+    line.update(line_extra)
+    acq.profile(True)
+    acq.profile_get()
+    grid()
+    torch.cuda.synchronize()
+    line["gpu_launches"] = (sum(v[1] for k, v in acq.profile_get().items() if k[0] != "span")
+                            + 1 + 2 * len(models)) * args.steps
+    acq.profile(False)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    plan.close()
+    acq.close()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "track_24mhz":
         return run_track(args)
+    if args.workload == "refine_12mhz":
+        return run_refine(args)
     return run_ours(args)
 
 

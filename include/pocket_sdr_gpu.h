@@ -315,6 +315,13 @@ int sdrg_refine_sums(sdrg_refine_plan_t *plan, const uint8_t *if_dev, int len_if
 int sdrg_refine_vjp(sdrg_refine_plan_t *plan, const float *sums_dev, const float *g_dev,
     double *grad_dev, void *stream);
 
+/* Starting theta / rate from acquisition results (DEVICE array of n_sig
+ * sdrg_acq_result_t in the plan's signal order, e.g. written by
+ * sdrg_acq_run): code phase 0 at sample ix_grid + offset, fd = the fine
+ * Doppler, phi = 0, carrier-aided code rate; t_ref from ix0. */
+int sdrg_refine_from_peaks(sdrg_refine_plan_t *plan, const sdrg_acq_result_t *res_dev,
+    int ix_grid, int ix0, double *theta_dev, double *rate_dev, void *stream);
+
 /* n_step Gauss-Newton steps, step i in model models[i] (HOST array):
  *   0  correlation-power loss: complex amplitude per block (carrier phase
  *      not observable; only tau and fd move);

@@ -77,6 +77,7 @@ SIGNATURES = {
     "sdrg_refine_sums": ([_p, _p, _i, _i, _p, _p, _i, _p, _p], _i),
     "sdrg_refine_vjp": ([_p, _p, _p, _p, _p], _i),
     "sdrg_refine_gn": ([_p, _p, _i, _i, _p, _p, _p, _i, _p, _p], _i),
+    "sdrg_refine_from_peaks": ([_p, _p, _i, _i, _p, _p, _p], _i),
 }
 
 

@@ -508,6 +508,40 @@ extern "C" int sdrg_refine_gn(sdrg_refine_plan *p, const uint8_t *if_dev, int le
     return SDRG_OK;
 }
 
+namespace sdrg {
+// theta / rate from acquisition peaks: code phase 0 at sample ix_grid + offset
+// (a sdr_search_code lag), fd = the fine Doppler, phase 0
+__global__ void refine_from_peaks_kernel(const RefineSigDev *sigs, int n,
+                                         const sdrg_acq_result_t *res, int ix_grid, double fs,
+                                         double t_ref, double *theta, double *rate)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double t0 = (double)((long long)ix_grid + res[i].offset) / fs;
+    const double fd = res[i].fd, fc = sigs[i].fc;
+    const double sc = fc > 0.0 ? fd / fc : 0.0;
+    theta[3 * i] = t0 + sc * (t0 - t_ref);      // carrier-aided code rate over t0 .. t_ref
+    theta[3 * i + 1] = fd;
+    theta[3 * i + 2] = 0.0;
+    rate[i] = sigs[i].rate_nom * (1.0 + sc);
+}
+} // namespace sdrg
+
+extern "C" int sdrg_refine_from_peaks(sdrg_refine_plan *p, const sdrg_acq_result_t *res_dev,
+                                      int ix_grid, int ix0, double *theta_dev, double *rate_dev,
+                                      void *stream)
+{
+    if (!p || !res_dev || !theta_dev || !rate_dev)
+        return set_error(SDRG_ERR_ARG, "sdrg_refine_from_peaks: null argument");
+    cudaStream_t st = (cudaStream_t)stream;   // NULL: the legacy default stream
+    const double t_ref = (ix0 + 0.5 * p->K * (double)p->Nb) / p->fs;
+    refine_from_peaks_kernel<<<(p->n + 127) / 128, 128, 0, st>>>(p->sigs_dev, p->n, res_dev,
+                                                                 ix_grid, p->fs, t_ref,
+                                                                 theta_dev, rate_dev);
+    SDRG_CUDA(cudaGetLastError());
+    return SDRG_OK;
+}
+
 extern "C" int sdrg_refine_plan_info(const sdrg_refine_plan *p, int *out4)
 {
     if (!p || !out4) return set_error(SDRG_ERR_ARG, "sdrg_refine_plan_info: null argument");

@@ -117,6 +117,17 @@ class RefinePlan:
             check("sdrg_refine_vjp")
         return grad
 
+    def from_peaks(self, res: torch.Tensor, ix_grid: int, ix0: int, theta: torch.Tensor,
+                   rate: torch.Tensor) -> None:
+        """theta / rate (in place) from device acquisition results (the
+        sdrg_acq_result_t bytes an AcqPlan.run_device wrote), signal order =
+        plan order."""
+        if not res.is_cuda or res.numel() < 32 * self.n:
+            raise ValueError("res: device buffer of n_sig acquisition results expected")
+        if lib.sdrg_refine_from_peaks(self.handle, _dptr(res), int(ix_grid), int(ix0),
+                                      _dptr(theta), _dptr(rate), _stream()):
+            check("sdrg_refine_from_peaks")
+
     def gn(self, buf: torch.Tensor, ix0: int, theta: torch.Tensor, rate: torch.Tensor,
            models=(MODEL_COHERENT,) * 5, info: bool = True):
         """Gauss-Newton steps in place on theta / rate (one per entry of
