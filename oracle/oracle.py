@@ -38,11 +38,14 @@ _d = C.c_double
 _f = C.c_float
 
 
+REF_ROOT = os.environ.get("POCKETSDR_REF", "/root/reference")
+
+
 def build(ref: bool = True) -> None:
     """Compile the restatement, and the reference library when its sources
     are present on this machine."""
     targets = ["oracle"]
-    if ref and os.path.isdir(os.environ.get("POCKETSDR_REF", "/root/reference") + "/src"):
+    if ref and os.path.isdir(REF_ROOT + "/src"):
         targets.append("ref")
     subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
 

@@ -117,6 +117,32 @@ def main() -> int:
                         params=np.array([fs, fi, T]))
     meta["code_fft_numpy_vs_ref_rel"] = float(np.abs(code_fft - code_fft_ref).max() /
                                               np.abs(code_fft_ref).max())
+    # ---- real front-end data: the reference's own L1 sample -----------------
+    # sample/L1_20211125_004000_12MHz_I.bin (12 MHz, IF 3 MHz, INT8 real, 2-bit
+    # values). 20 ms of it, packed as the reference's sdr_read_data does
+    # (src/sdr_func.c:451-505: SDR_CPX8(raw, 0)), searched for GPS L1 C/A
+    # PRN 1-32 with 4 ms coherent x 5 sums (48 000-point circular correlation
+    # of the code tiled x4), +-5 kHz in 250 Hz bins, by the reference's
+    # sdr_search_code / sdr_corr_max / sdr_fine_dop.
+    src = os.path.join(oracle.REF_ROOT, "sample", "L1_20211125_004000_12MHz_I.bin")
+    raw = np.fromfile(src, np.int8)[:5 * 48000]
+    real_buf = (raw.astype(np.uint8) & 0x0F).astype(np.uint8)
+    fs, fi, T, N = 12e6, 3e6, 4e-3, 48000
+    fds = np.arange(-5000, 5001, 250, dtype=np.float32)
+    res = []
+    for prn in range(1, 33):
+        cf = R.gen_code_fft(np.tile(codes.gen_code("L1CA", prn), 4), None, T, 0.0, fs, N, 0)
+        P = np.zeros((len(fds), N), np.float32)
+        for s in range(5):
+            R.search_code(cf, real_buf, s * N, N, fs, fi, fds, P, T)
+        cn0, pk = R.corr_max(P, N, N, len(fds), T)
+        res.append((prn, pk[0], pk[1], cn0, float(P[pk[0], pk[1]]), R.fine_dop(P, N, fds, pk)))
+    res = np.array(res, dtype=[("prn", np.int32), ("bin", np.int32), ("offset", np.int32),
+                               ("cn0", np.float32), ("pmax", np.float32), ("fd", np.float64)])
+    np.savez_compressed(os.path.join(HERE, "real_l1ca.npz"), buf=real_buf, fds=fds, res=res,
+                        params=np.array([fs, fi, T, N, 5]))
+    meta["real_l1ca_detected_38dbhz"] = [int(r["prn"]) for r in res if r["cn0"] >= 38.0]
+
     # Doppler bins: exact floats
     meta["dop_bins"] = {f"{T}_{d}_{m}": R.dop_bins(T, d, m).tolist()
                         for T, d, m in ((1e-3, 0.0, 5000.0), (4e-3, 0.0, 5000.0),

@@ -240,6 +240,35 @@ def test_batched_grid_matches_search_code(gpu):
         assert_power_close(G[p], P[:, :g.Nmax])
 
 
+def test_real_front_end_data_vs_reference_fixture(gpu, golden):
+    """Real data: 20 ms of the reference's own L1 sample (12 MHz, IF 3 MHz,
+    2-bit) searched for GPS L1 C/A PRN 1-32, 4 ms coherent (code tiled x4,
+    48 000-point circular correlation) x 5 sums, against the reference's
+    sdr_search_code / sdr_corr_max / sdr_fine_dop results stored in the
+    fixture. Detected PRNs (the reference finds 2, 5, 11, 13, 15, 18, 20, 29,
+    30 at >= 38 dB-Hz): same Doppler bin, same code offset modulo the 1 ms
+    period (the tiled replica makes the four maxima exactly equal), C/N0
+    within 0.1 dB. Every PRN: peak power within 1e-4 and C/N0 within 0.1 dB."""
+    from pocketsdr_b200.acquire import AcqPlan
+    d = golden("real_l1ca.npz")
+    fs, fi, T, N, n_sum = d["params"]
+    N, n_sum = int(N), int(n_sum)
+    g = synth.Group("L1CA", list(range(1, 33)), fs, fi, T, N, N, N, n_sum, d["fds"], 0, tile=4)
+    plan = AcqPlan([g], [synth.group_code_ffts(g)])
+    res = plan.run_host([d["buf"]], [0])
+    ref_res = d["res"]
+    det = [int(r["prn"]) for r in ref_res if r["cn0"] >= 38.0]
+    assert det == [2, 5, 11, 13, 15, 18, 20, 29, 30]
+    period = N // 4
+    for r, e in zip(res, ref_res):
+        assert abs(float(r["cn0"]) - float(e["cn0"])) < 0.1, (int(e["prn"]), r, e)
+        assert float(r["pmax"]) == pytest.approx(float(e["pmax"]), rel=1e-4)
+        if e["cn0"] >= 38.0:
+            assert int(r["bin"]) == int(e["bin"]), (int(e["prn"]), r, e)
+            assert int(r["offset"]) % period == int(e["offset"]) % period, (int(e["prn"]), r, e)
+            assert float(r["fd"]) == pytest.approx(float(e["fd"]), abs=0.5)
+
+
 def test_acq_l1ca_12mhz_peaks(gpu, ref):
     """The 12 MHz real-IF L1 C/A search (4 ms coherent x 5 sums) on the
     visible PRNs and a few absent ones: identical peaks, C/N0 within 0.1 dB."""

@@ -96,6 +96,28 @@ def test_search_golden(orc, golden):
     assert np.max(np.abs(corr - g["corr"])) <= 1e-5 * np.max(np.abs(g["corr"]))
 
 
+def test_search_real_data_golden(orc, golden):
+    """The restatement on the reference's real L1 sample: for two detected
+    PRNs, the peak over the reference's peak bin and its neighbours is the
+    reference's (offset modulo the 1 ms period of the x4 tiled code) with the
+    same power."""
+    from pocketsdr_b200 import codes
+    d = golden("real_l1ca.npz")
+    fs, fi, T, N, n_sum = d["params"]
+    N, n_sum = int(N), int(n_sum)
+    for e in d["res"][[12, 28]]:                  # PRN 13 (47.8 dB-Hz), 29 (38.4)
+        b = int(e["bin"])
+        fds = d["fds"][b - 1: b + 2]
+        cf = orc.gen_code_fft(np.tile(codes.gen_code("L1CA", int(e["prn"])), 4), None, T, 0.0,
+                              fs, N, 0)
+        P = np.zeros((3, N), np.float32)
+        for s in range(n_sum):
+            orc.search_code(cf, d["buf"], s * N, N, fs, fi, fds, P)
+        i, j = np.unravel_index(int(np.argmax(P)), P.shape)
+        assert i == 1 and j % (N // 4) == int(e["offset"]) % (N // 4)
+        assert float(P[i, j]) == pytest.approx(float(e["pmax"]), rel=1e-5)
+
+
 def test_search_accumulates(orc):
     # test/src/test_sdr_func.c:237-242: zero code DFT leaves P at 1.0
     buf = np.array([pack_cpx8(i + 1, -i) for i in range(4)], np.uint8)
