@@ -2,9 +2,13 @@
 """Benchmark: batched multi-GNSS acquisition cells/s on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload acq_multi_24mhz|acq_l1ca_12mhz|track_24mhz|refine_12mhz]
+                    [--workload acq_multi_24mhz|acq_l1ca_12mhz|acq_long_48mhz|track_24mhz|
+                                refine_12mhz]
 
-Besides the default acquisition workload: track_24mhz times the batched
+Besides the default acquisition workload: acq_l1ca_12mhz is the plain 12 MHz
+GPS L1 C/A search (32 PRNs x 41 bins x 5 x 4 ms), acq_long_48mhz the weak-signal
+long coherent search (48 MHz, GPS L5-Q and QZSS L6D, 10 ms coherent =
+480 000-point FFTs x 20 sums, 401 bins of 50 Hz), track_24mhz times the batched
 tracking correlators (channel-epochs/s) and refine_12mhz the grid search plus
 Gauss-Newton refinement of 64 signals (signals/s, with the refinement's cost
 against the grid and its agreement with the FP64 oracle).
@@ -131,7 +135,17 @@ def make_workload(name: str, seed: int, prn_limit=None, t_sum=20e-3):
         return synth.acq_multi_24mhz(seed=seed, prn_limit=prn_limit, t_sum=t_sum)
     if name == "acq_l1ca_12mhz":
         return synth.acq_l1ca_12mhz(seed=seed)
+    if name == "acq_long_48mhz":
+        return synth.acq_long_48mhz(seed=seed, prn_limit=prn_limit)
     raise SystemExit(f"unknown workload {name}")
+
+
+def workload_code_ffts(wl, g):
+    """Conjugated code DFTs [n_prn, L] of group g of a workload."""
+    from pocketsdr_b200 import synth
+    if wl.name == "acq_long_48mhz":
+        return synth.long_code_ffts(g)
+    return synth.group_code_ffts(g)
 
 
 def cons_flops(groups) -> float:
@@ -172,13 +186,15 @@ def load_traffic() -> dict:
 
 
 # ---------------------------------------------------------------------------
-def cpu_reference_rate(wl, max_threads: int | None = None, budget_prn: int | None = None):
+def cpu_reference_rate(wl, max_threads: int | None = None, budget_prn: int | None = None,
+                       max_bins: int | None = None):
     """Reference CPU throughput (cells/s) of the whole workload on this host,
     estimated from a bounded sample: for each group, up to `threads` PRN
-    searches (every bin, every sum, the reference's own sdr_search_code built
-    from source, or the oracle restatement when that build is absent) run in
-    parallel threads; core-seconds per PRN scale to the full PRN set, spread
-    over all cores."""
+    searches (every sum, the reference's own sdr_search_code built from
+    source, or the oracle restatement when that build is absent) run in
+    parallel threads, over every Doppler bin or the first `max_bins` (the
+    search cost is the same per bin); core-seconds per PRN scale to the full
+    bin and PRN sets, spread over all cores."""
     import concurrent.futures as cf
     from oracle import oracle
     from pocketsdr_b200 import synth
@@ -188,16 +204,21 @@ def cpu_reference_rate(wl, max_threads: int | None = None, budget_prn: int | Non
     total_core_s, total_cells, sample_desc = 0.0, 0, []
     for g in wl.groups:
         n = min(len(g.prns), threads, budget_prn or threads)
-        cfs = [synth.tiled_code_fft(g.sig, p, g.fs, g.tile, g.N, g.L - g.N) for p in g.prns[:n]]
+        if wl.name == "acq_long_48mhz":
+            cfs = [synth.long_replica_fft(g.sig, p, g.fs, g.T, g.L) for p in g.prns[:n]]
+        else:
+            cfs = [synth.tiled_code_fft(g.sig, p, g.fs, g.tile, g.N, g.L - g.N) for p in g.prns[:n]]
         buf = wl.bufs[g.buf]
+        nb = min(len(g.fds), max_bins or len(g.fds))
+        fds = np.ascontiguousarray(g.fds[:nb])
 
         def one(c):
-            P = np.zeros((len(g.fds), g.L), np.float32)
+            P = np.zeros((nb, g.L), np.float32)
             t0 = time.perf_counter()
             for s in range(g.n_sum):
-                R.search_code(c, buf, (s * g.N) % len(buf), g.L, g.fs, g.fi, g.fds, P, g.T)
-            R.corr_max(P, g.L, g.Nmax, len(g.fds), g.T)
-            return time.perf_counter() - t0
+                R.search_code(c, buf, (s * g.N) % len(buf), g.L, g.fs, g.fi, fds, P, g.T)
+            R.corr_max(P, g.L, g.Nmax, nb, g.T)
+            return (time.perf_counter() - t0) * len(g.fds) / nb
         t0 = time.perf_counter()
         with cf.ThreadPoolExecutor(max_workers=n) as ex:
             per = list(ex.map(one, cfs))
@@ -205,10 +226,18 @@ def cpu_reference_rate(wl, max_threads: int | None = None, budget_prn: int | Non
         core_s_per_prn = sum(per) / n
         total_core_s += core_s_per_prn * len(g.prns)
         total_cells += len(g.prns) * len(g.fds) * g.Nmax
-        sample_desc.append(f"{g.sig}:{n}/{len(g.prns)} PRN ({wall:.1f}s)")
+        sample_desc.append(f"{g.sig}:{n}/{len(g.prns)} PRN" +
+                           (f" x {nb}/{len(g.fds)} bins" if nb < len(g.fds) else "") +
+                           f" ({wall:.1f}s)")
     rate = total_cells / (total_core_s / threads)
     return rate, threads, R.kind, "; ".join(sample_desc) + \
-        f"; full PRN sets extrapolated from core-seconds per PRN over {threads} threads"
+        f"; full PRN (and bin) sets extrapolated from core-seconds per PRN over {threads} threads"
+
+
+def _bin_budget(wl):
+    """Doppler bins per sampled PRN search on the CPU: all of them, except for
+    the 480 000-point searches (401 bins x 20 sums would take minutes per PRN)."""
+    return 2 if wl.name == "acq_long_48mhz" else None
 
 
 # ---------------------------------------------------------------------------
@@ -220,7 +249,7 @@ def run_reference(args):
     vals = []
     desc = ""
     for k in range(args.warmup + args.steps):
-        rate, cores, kind, desc = cpu_reference_rate(wl, budget_prn=4)
+        rate, cores, kind, desc = cpu_reference_rate(wl, budget_prn=4, max_bins=_bin_budget(wl))
         if k >= args.warmup:
             vals.append(rate)
     v = statistics.median(vals)
@@ -252,7 +281,7 @@ def run_ours(args):
     shard_index = None
     if strong:
         wl.groups, shard_index = D.shard_groups(full_groups, rank, world)
-    cfs = [synth.group_code_ffts(g) for g in wl.groups]
+    cfs = [workload_code_ffts(wl, g) for g in wl.groups]
     plan = acquire.AcqPlan(wl.groups, cfs)
     cells = plan.cells
     job_cells = sum(len(g.prns) * len(g.fds) * g.Nmax for g in full_groups) if strong \
@@ -373,7 +402,7 @@ def run_ours(args):
             "roofline": roofline, "clocks": clocks,
             "detected": int(sum(1 for r in res if r["cn0"] >= 38.0))}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, cores, kind, desc = cpu_reference_rate(wl)
+        rate, cores, kind, desc = cpu_reference_rate(wl, max_bins=_bin_budget(wl))
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
                                 "sample": desc}
     if rank == 0:
@@ -430,10 +459,16 @@ def cpu_track_rate(wl, specs_list, banks_host, max_jobs=600):
     return len(jobs) / dt, cores, R.kind, f"{len(jobs)} channel-epochs of the same stream"
 
 
+TRACK_EPOCHS_PER_STEP = 100   # one step = 100 ms of the stream
+
+
 def run_track(args):
-    """Tracking-correlator workload: every step is one 1 ms epoch of the
-    24 MHz 8-antenna stream, i.e. one correlator job per channel whose code
-    period starts at that epoch (L1CA/L5I every ms, E1B every 4 ms)."""
+    """Tracking-correlator workload: every step is 100 ms of the 24 MHz
+    8-antenna stream, 100 consecutive 1 ms epochs; each epoch is one batch
+    (sdrg_corr_batch) of a correlator job per channel whose code period
+    starts there (L1CA/L5I every ms, E1B every 4 ms). Open-loop trajectories,
+    so the epochs' jobs are known in advance; still one batch per epoch, as a
+    receiver closing its loops each epoch would run them."""
     import torch
     from pocketsdr_b200 import synth, track
     rank, world, local = dist_info()
@@ -443,7 +478,8 @@ def run_track(args):
     torch.cuda.set_stream(st)
     bufs_d = [torch.from_numpy(b).cuda() for b in wl.bufs]
     lens = [len(b) for b in wl.bufs]
-    n_ep = args.warmup + args.steps
+    E = TRACK_EPOCHS_PER_STEP
+    n_ep = (args.warmup + args.steps) * E
     specs_list = []
     for e in range(n_ep):
         sp = wl.jobs_at(e * 1e-3, ptrs)
@@ -452,16 +488,19 @@ def run_track(args):
         specs_list.append(sp)
     jobs_list = [track.make_jobs(sp) for sp in specs_list]
     max_j = max(len(s) for s in specs_list)
-    corr = torch.empty(max_j * track.SDR_MAX_CORR * 2, dtype=torch.float32, device="cuda")
-    Cb = torch.empty(max_j * 4, dtype=torch.float32, device="cuda")
+    per_ep = max_j * track.SDR_MAX_CORR * 2          # floats of one epoch's correlations
+    corr = torch.empty(E * per_ep, dtype=torch.float32, device="cuda")
+    Cb = torch.empty(E * max_j * 4, dtype=torch.float32, device="cuda")
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
     ptr_b = [b.data_ptr() for b in bufs_d]
 
-    def step(e):
-        track.corr_batch(jobs_list[e], ptr_b, lens, corr.data_ptr(), Cb.data_ptr(), st.cuda_stream)
+    def step(k):
+        for i in range(E):
+            track.corr_batch(jobs_list[k * E + i], ptr_b, lens, corr.data_ptr() + 4 * i * per_ep,
+                             Cb.data_ptr() + 16 * i * max_j, st.cuda_stream)
 
-    for e in range(args.warmup):
-        step(e)
+    for k in range(args.warmup):
+        step(k)
     torch.cuda.synchronize()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
@@ -475,18 +514,47 @@ def run_track(args):
     torch.cuda.synchronize()
     clocks = clk.stop()
     ms = sum(a.elapsed_time(b) for a, b in ev)
-    n_jobs = sum(len(specs_list[args.warmup + k]) for k in range(args.steps))
+    timed = [specs_list[e] for e in range(args.warmup * E, n_ep)]
+    n_jobs = sum(len(sp) for sp in timed)
     value = n_jobs / (ms / 1e3)
-    taps = sum(len(s["pos"]) * s["N"] for k in range(args.steps) for s in specs_list[args.warmup + k])
+    taps = sum(len(s["pos"]) * s["N"] for sp in timed for s in sp)
+
+    # end to end: the step's 100 ms of IF (every antenna) from pinned host
+    # memory into the device buffers, the batches, every correlation back
+    bufs_h = [torch.from_numpy(b).pin_memory() for b in wl.bufs]
+    corr_h = torch.empty(corr.numel(), dtype=torch.float32).pin_memory()
+    h2d = sum(b.numel() for b in bufs_h)
+    d2h = corr_h.numel() * 4
+
+    def e2e_step(k):
+        for bh, bd in zip(bufs_h, bufs_d):
+            bd.copy_(bh, non_blocking=True)
+        step(k)
+        corr_h.copy_(corr, non_blocking=True)
+
+    e2e_step(0)
+    torch.cuda.synchronize()
+    e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.fill_((k + 1) & 0xFF)
+        e2e_ev[k][0].record(st)
+        e2e_step(args.warmup + k)
+        e2e_ev[k][1].record(st)
+    torch.cuda.synchronize()
+    e2e_ms = sum(a.elapsed_time(b) for a, b in e2e_ev)
+
     line = {"metric": TRACK_METRIC, "value": value, "unit": "channel-epochs/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8",
             "data": "synthetic",
             "config": {"workload": "track_24mhz", "channels": len(wl.channels),
-                       "antennas": len(wl.bufs), "taps": 44,
+                       "antennas": len(wl.bufs), "taps": 44, "epochs_per_step": E,
                        "l2": "flushed between timed steps (512 MB write outside the events)"},
+            "e2e": {"value": n_jobs / (e2e_ms / 1e3), "unit": "channel-epochs/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "tap_samples_per_s": taps / (ms / 1e3), "clocks": clocks,
-            "gpu_launches": 3 * args.steps}
+            "gpu_launches": 3 * E * args.steps}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         banks_host = synth.track_banks(wl)
         rate, cores, kind, desc = cpu_track_rate(wl, specs_list, banks_host)

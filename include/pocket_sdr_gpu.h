@@ -113,6 +113,22 @@ double sdr_fine_dop(const float *P, int N, const float *fds, int len_fds,
  * sdr_free is free()). */
 float *sdr_dop_bins(double T, float dop, float max_dop, int *len_fds);
 
+/* Replaces src/sdr_code.c:2556-2568 (sdr_res_code, src/pocket_sdr.h:462-463).
+ * Nearest-chip resampling: sample i < N takes chip
+ * (int)((coff*fs + i) * (len_code/T/fs)) % len_code (Q = code_Q's chip, or
+ * code_I's for a real code), samples N..N+Nz-1 are 0. Bit-identical to the
+ * reference. A code offset that would index before the code (the reference
+ * reads out of bounds there) is rejected. */
+void sdr_res_code(const int8_t *code_I, const int8_t *code_Q, int len_code,
+    double T, double coff, double fs, int N, int Nz, sdr_cpx16_t *code_res);
+
+/* Replaces src/sdr_code.c:2589-2608 (sdr_gen_code_fft, src/pocket_sdr.h:464-465).
+ * Conjugated DFT (natural order, N+Nz points) of the resampled replica
+ * zero padded by Nz (replica Q = code_Q's chips, or 0 for a real code). FP32
+ * mixed-radix FFT on the GPU: N+Nz must be supported (sdrg_fft_supported). */
+void sdr_gen_code_fft(const int8_t *code_I, const int8_t *code_Q, int len_code,
+    double T, double coff, double fs, int N, int Nz, sdr_cpx_t *code_fft);
+
 /* =========================================================================
  * Part 2: additive entry points (no reference counterpart)
  * ========================================================================= */
@@ -180,7 +196,8 @@ typedef struct {
     int len_fds;           /* Doppler bins */
     double fs, fi, T;      /* sampling rate, IF (Hz), coherent time (s) */
     const float *fds;      /* [len_fds] Doppler bins (Hz), HOST */
-    const sdr_cpx_t *code_fft; /* [n_prn][L] conjugated code DFTs, HOST */
+    const sdr_cpx_t *code_fft; /* [n_prn][L] conjugated code DFTs, HOST, or
+                              NULL (zeros until sdrg_acq_set_codes) */
     int buf;               /* index of the IF buffer this group reads */
 } sdrg_acq_sig_t;
 
@@ -257,6 +274,40 @@ typedef struct {
  * partials, both DEVICE pointers. Asynchronous. */
 int sdrg_corr_batch(const sdrg_corr_job_t *jobs, int n_job, const uint8_t *const *if_dev,
     const int *len_if, sdr_cpx_t *corr_dev, sdr_cpx_t *C_dev, void *stream);
+
+/* ---- replicas on the device ------------------------------------------------
+ * Batched forms of sdr_res_code / sdr_gen_code_fft (src/sdr_code.c:2556-2608)
+ * for n_code codes of len_code chips each, stored back to back
+ * (code_I_dev[c * len_code + i]; code_Q_dev likewise, or NULL for real
+ * codes). All pointers are DEVICE pointers; `stream` is a cudaStream_t
+ * (NULL = the legacy default stream); asynchronous.
+ *
+ * sdrg_res_code writes code_res_dev[(c * n_bank + b) * (N + Nz) + i] =
+ * sdr_res_code(code c, coff - b / fs / n_bank)[i] for b < n_bank <= 32; with
+ * coff = 0 and n_bank = SDR_N_CODES these are a tracking channel's
+ * fractional-phase code banks (src/sdr_ch.c:265-272), bit-identical.
+ *
+ * sdrg_gen_code_fft writes code_fft_dev[c * (N + Nz) + k] =
+ * sdr_gen_code_fft(code c, coff)[k]; its sub-spectra scratch is
+ * stream-ordered (cudaMallocAsync / cudaFreeAsync on `stream`). */
+int sdrg_res_code(const int8_t *code_I_dev, const int8_t *code_Q_dev, int len_code,
+    int n_code, double T, double coff, double fs, int N, int Nz, int n_bank,
+    sdr_cpx16_t *code_res_dev, void *stream);
+int sdrg_gen_code_fft(const int8_t *code_I_dev, const int8_t *code_Q_dev, int len_code,
+    int n_code, double T, double coff, double fs, int N, int Nz,
+    sdr_cpx_t *code_fft_dev, void *stream);
+
+/* Sets the code DFTs of plan group g on the device from chips, replacing
+ * what sdrg_acq_plan_new uploaded (a plan may also be created with
+ * code_fft = NULL for a group and get its codes only from here): PRN p of
+ * the group takes code_I_dev[p * len_code ...] (n_prn codes, DEVICE), code
+ * period T, offset coff, an N-sample replica zero padded to the group's L
+ * (the receiver's acquisition uses N = L / 2, src/sdr_ch.c:197). Same values
+ * as sdr_gen_code_fft, written directly in the plan's internal layout.
+ * `stream` NULL = the calling thread's stream; asynchronous; a later
+ * sdrg_acq_run on the same stream sees the new codes. */
+int sdrg_acq_set_codes(sdrg_acq_plan_t *plan, int g, const int8_t *code_I_dev,
+    const int8_t *code_Q_dev, int len_code, double T, double coff, int N, void *stream);
 
 /* Host convenience: copies IF buffers to the device, runs, and copies the
  * n_prn-total results back (synchronous). if_host[b] are HOST pointers. */

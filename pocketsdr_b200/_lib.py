@@ -55,6 +55,8 @@ SIGNATURES = {
     "sdr_corr_max": ([_p, _i, _i, _i, _d, _p], _f),
     "sdr_fine_dop": ([_p, _i, _p, _i, _p], _d),
     "sdr_dop_bins": ([_d, _f, _f, C.POINTER(_i)], C.POINTER(_f)),
+    "sdr_res_code": ([_p, _p, _i, _d, _d, _d, _i, _i, _p], None),
+    "sdr_gen_code_fft": ([_p, _p, _i, _d, _d, _d, _i, _i, _p], None),
     "sdr_gpu_last_error": ([C.c_char_p, _i], _i),
     "sdr_gpu_clear_error": ([], None),
     "sdrg_init": ([_i], _i),
@@ -71,6 +73,9 @@ SIGNATURES = {
     "sdrg_acq_profile_get": ([_p, _p, _p], _i),
     "sdrg_acq_run_host": ([_p, _p, _p, _p, _p], _i),
     "sdrg_corr_batch": ([_p, _i, _p, _p, _p, _p, _p], _i),
+    "sdrg_res_code": ([_p, _p, _i, _i, _d, _d, _d, _i, _i, _i, _p, _p], _i),
+    "sdrg_gen_code_fft": ([_p, _p, _i, _i, _d, _d, _d, _i, _i, _p, _p], _i),
+    "sdrg_acq_set_codes": ([_p, _i, _p, _p, _i, _d, _d, _i, _p], _i),
     "sdrg_refine_plan_new": ([C.POINTER(RefineSig), _i, _d, _i, _i, _i], _p),
     "sdrg_refine_plan_free": ([_p], None),
     "sdrg_refine_plan_info": ([_p, _p], _i),

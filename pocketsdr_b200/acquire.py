@@ -24,23 +24,25 @@ assert RESULT_DTYPE.itemsize == C.sizeof(AcqResult)
 class AcqPlan:
     def __init__(self, groups, code_ffts):
         """groups: sequence of synth.Group-like objects (sig, prns, fs, fi, T, N,
-        L, Nmax, n_sum, fds, buf); code_ffts: per group complex64 [n_prn, L]."""
+        L, Nmax, n_sum, fds, buf); code_ffts: per group complex64 [n_prn, L],
+        or None for a group whose codes come from set_codes (device chips)."""
         self.groups = list(groups)
         n = len(self.groups)
         sigs = (AcqSig * n)()
         self._keep = []
         for i, (g, cf) in enumerate(zip(self.groups, code_ffts)):
-            cf = np.ascontiguousarray(cf, np.complex64)
             fds = np.ascontiguousarray(g.fds, np.float32)
-            if cf.shape != (len(g.prns), g.L):
-                raise ValueError(f"group {i}: code_fft shape {cf.shape} != {(len(g.prns), g.L)}")
+            if cf is not None:
+                cf = np.ascontiguousarray(cf, np.complex64)
+                if cf.shape != (len(g.prns), g.L):
+                    raise ValueError(f"group {i}: code_fft shape {cf.shape} != {(len(g.prns), g.L)}")
             self._keep += [cf, fds]
             s = sigs[i]
             s.L, s.N, s.Nmax, s.n_sum = g.L, g.N, g.Nmax, g.n_sum
             s.n_prn, s.len_fds = len(g.prns), len(fds)
             s.fs, s.fi, s.T = g.fs, g.fi, g.T
             s.fds = fds.ctypes.data_as(C.POINTER(C.c_float))
-            s.code_fft = C.c_void_p(cf.ctypes.data)
+            s.code_fft = C.c_void_p(cf.ctypes.data) if cf is not None else None
             s.buf = g.buf
         self.handle = lib.sdrg_acq_plan_new(sigs, n)
         if not self.handle:
@@ -49,6 +51,19 @@ class AcqPlan:
         self._keep = None      # the plan copied everything
         self.n_res = sum(len(g.prns) for g in self.groups)
         self.offsets = np.cumsum([0] + [len(g.prns) for g in self.groups])[:-1]
+
+    def set_codes(self, g: int, chips, T: float, coff: float = 0.0, N: int | None = None,
+                  code_Q=None) -> None:
+        """Computes group g's code DFTs on the device (sdrg_acq_set_codes) from
+        chips [n_prn, len_code] (one code per PRN, group order): the N-sample
+        replica (default: the group's N) of code period T, zero padded to L.
+        Asynchronous on torch's current stream, like run_device."""
+        from . import replica
+        gr = self.groups[g]
+        ci = replica.device_chips(chips)
+        if ci.shape[0] != len(gr.prns):
+            raise ValueError(f"group {g}: {ci.shape[0]} codes for {len(gr.prns)} PRNs")
+        replica.set_plan_codes(self.handle, g, ci, T, coff, gr.N if N is None else N, code_Q)
 
     @property
     def cells(self) -> int:

@@ -90,4 +90,16 @@ struct IfWindow {
 int mix_cpx_device(const sdr_cpx_t *buff, int len_buff, int ix, int N, double fs,
                    double fc, double phi, char2 *iq_dev, cudaStream_t st);
 
+// Replica generation (sdrg_code.cu), asynchronous on st, DEVICE pointers.
+// res_code_device: out[c][b][N+Nz] = sdr_res_code(code c, coff - b/fs/n_bank);
+// code_fft_device: conjugated DFT of each code's N-sample replica zero padded
+// to L, natural order ([c][L]) or the acquisition layout ([c][R][M] at the
+// forward transform's digit-reversed positions).
+int res_code_device(const int8_t *ci, const int8_t *cq, int len_code, int n_code, double T,
+                    double coff, double fs, int N, int Nz, int n_bank, char2 *out,
+                    cudaStream_t st);
+int code_fft_device(const int8_t *ci, const int8_t *cq, int len_code, int n_code, double T,
+                    double coff, double fs, int N, int L, int natural, float2 *out,
+                    cudaStream_t st);
+
 } // namespace sdrg

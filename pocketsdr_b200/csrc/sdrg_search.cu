@@ -938,7 +938,7 @@ sdrg_acq_plan_t *sdrg_acq_plan_new(const sdrg_acq_sig_t *sigs, int n_sig)
         G.sig = sigs[gi];
         const sdrg_acq_sig_t &s = G.sig;
         if (s.L <= 0 || s.N <= 0 || s.Nmax <= 0 || s.Nmax > s.L || s.n_sum <= 0 ||
-            s.n_prn <= 0 || s.len_fds <= 0 || !s.fds || !s.code_fft || s.fs <= 0) {
+            s.n_prn <= 0 || s.len_fds <= 0 || !s.fds || s.fs <= 0) {
             set_error(SDRG_ERR_ARG, "sdrg_acq_plan_new: bad parameters for group %d", gi);
             sdrg_acq_plan_free(plan);
             return nullptr;
@@ -966,9 +966,15 @@ sdrg_acq_plan_t *sdrg_acq_plan_new(const sdrg_acq_sig_t *sigs, int n_sig)
         // Uploads are ordered on the thread's (non-blocking) stream: a plain
         // cudaMemcpy from pageable memory may return before its DMA lands and
         // runs on the legacy stream, which kernels on `st` do not wait for.
-        ok = ok && cudaMemcpyAsync(nat, sigs[gi].code_fft, (size_t)s.n_prn * L * sizeof(float2),
-                                   cudaMemcpyHostToDevice, st) == cudaSuccess;
-        ok = ok && perm_code(G.pl, nat, s.n_prn, G.code, st) == SDRG_OK;
+        if (sigs[gi].code_fft) {
+            ok = ok && cudaMemcpyAsync(nat, sigs[gi].code_fft, (size_t)s.n_prn * L * sizeof(float2),
+                                       cudaMemcpyHostToDevice, st) == cudaSuccess;
+            ok = ok && perm_code(G.pl, nat, s.n_prn, G.code, st) == SDRG_OK;
+        } else {
+            // codes come later from sdrg_acq_set_codes; zero until then
+            ok = ok && cudaMemsetAsync(G.code, 0, (size_t)s.n_prn * L * sizeof(float2), st) ==
+                           cudaSuccess;
+        }
         // Doppler bins as float on the device for the fine-Doppler fit
         if (ok) {
             float *fd_dev = (float *)(G.tab_dev + G.tab_words - s.len_fds);
@@ -1036,6 +1042,25 @@ int sdrg_acq_grid_host(const sdrg_acq_plan_t *plan, int g, float *dst)
     SDRG_CUDA(cudaMemcpy(dst, plan->g[g].P, (size_t)s.n_prn * s.len_fds * s.Nmax * sizeof(float),
                          cudaMemcpyDeviceToHost));
     return SDRG_OK;
+}
+
+int sdrg_acq_set_codes(sdrg_acq_plan_t *plan, int g, const int8_t *code_I_dev,
+                       const int8_t *code_Q_dev, int len_code, double T, double coff, int N,
+                       void *stream)
+{
+    if (!plan || g < 0 || g >= (int)plan->g.size())
+        return set_error(SDRG_ERR_ARG, "sdrg_acq_set_codes: no group %d", g);
+    GroupState &G = plan->g[g];
+    if (N <= 0 || N > G.sig.L)
+        return set_error(SDRG_ERR_ARG, "sdrg_acq_set_codes: replica length %d outside 1..L=%d",
+                         N, G.sig.L);
+    Device *dev;
+    int e;
+    if ((e = ensure_device(&dev))) return e;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!st && (e = thread_stream(&st))) return e;
+    return code_fft_device(code_I_dev, code_Q_dev, len_code, G.sig.n_prn, T, coff, G.sig.fs, N,
+                           G.sig.L, 0, G.code, st);
 }
 
 int sdrg_acq_run(sdrg_acq_plan_t *plan, const uint8_t *const *if_dev, const int *len_if,

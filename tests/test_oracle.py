@@ -209,3 +209,27 @@ def test_l1ca_codes_vs_reference():
     c = R.gen_code("L1CA", 7)
     assert np.array_equal(R.res_code(c, None, 1e-3, -0.7 / 24e6, 24e6, 24000, 0),
                           codes.res_code(c, 1e-3, -0.7 / 24e6, 24e6, 24000, 0))
+
+
+@pytest.mark.skipif(not HAVE_REF, reason="reference build (oracle/_ref) not present")
+def test_replica_restatement_vs_reference(orc):
+    """Resampled code banks (the tracking channel's -k/fs/10 offsets,
+    src/sdr_ch.c:265-272) bit-exact and code DFTs within 1e-6 of the largest
+    value: the restatement matches the reference build it stands in for."""
+    R = oracle.Reference()
+    rng = np.random.default_rng(12)
+    for L, fs, T in ((1023, 24e6, 1e-3), (2046, 12e6, 1e-3), (10230, 20.46e6 * 1.25, 1e-3)):
+        c = rng.choice(np.array([-1, 1], np.int8), L)
+        q = rng.choice(np.array([-1, 1], np.int8), L)
+        N = int(fs * T)
+        for k in range(10):
+            coff = -k / fs / 10
+            assert np.array_equal(orc.res_code(c, None, T, coff, fs, N, 3),
+                                  R.res_code(c, None, T, coff, fs, N, 3)), (L, k)
+            assert np.array_equal(orc.res_code(c, q, T, coff, fs, N, 0),
+                                  R.res_code(c, q, T, coff, fs, N, 0)), (L, k)
+    c = rng.choice(np.array([-1, 1], np.int8), 1023)
+    for N, Nz in ((6000, 6000), (4000, 0)):
+        a = orc.gen_code_fft(c, None, 1e-3, 2e-4, N * 1000.0, N, Nz)
+        b = R.gen_code_fft(c, None, 1e-3, 2e-4, N * 1000.0, N, Nz)
+        assert np.abs(a - b).max() <= 1e-6 * np.abs(b).max()
