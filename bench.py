@@ -752,10 +752,163 @@ def run_refine(args):
     return 0
 
 
+INGEST_METRIC = ("IF ingest samples/s (Pocket SDR FE 8CH RAW32 at 24 MHz -> 8 RF + 2 array "
+                 "cpx8 buffers, fs/4 mixing, LPF, beam-forming)")
+
+
+def ingest_config(N):
+    """The receiver setup of the ingest workload: RF channels 1-4 3-bit real
+    (fs/4 real-to-complex) with the receiver's automatic LPF (cutoff
+    0.9 * fs/4, src/sdr_rcv.c:538-545), 5-8 2-bit complex, and two array
+    channels over channels 1-4 (Q8 weights of amplitude 64 = 256 / 4
+    antennas, steering phases of a seeded beam)."""
+    fs = 24e6
+    rng = np.random.default_rng(11)
+    ph = rng.uniform(0, 2 * np.pi, (2, 4))
+    w = np.zeros((2, 8, 2), np.int16)
+    w[:, :4, 0] = np.floor(64 * np.cos(ph) + 0.5)
+    w[:, :4, 1] = np.floor(64 * np.sin(ph) + 0.5)
+    return dict(fmt=6, N=N, fs=fs, IQ=[1, 1, 1, 1, 2, 2, 2, 2], bits=[3, 3, 3, 3, 2, 2, 2, 2],
+                off=(0.0, 0.0), scale=(1.0, 1.0), lpf_fc=[0.9 * 0.5 * fs * 0.5] * 4 + [0.0] * 4,
+                w=w, arch_on=[1, 1])
+
+
+def cpu_ingest_rate(cfg_block, raw, n_blocks):
+    """Reference CPU rate (samples/s): the reference's own write_buff (with its
+    LPFs and array combine) over 1 ms blocks, one independent receiver per
+    host thread, all host threads."""
+    import concurrent.futures as cf
+    from oracle import oracle
+    chk = oracle.Ingest()
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    N = cfg_block["N"]
+    blocks = [raw[j * N * 4:(j + 1) * N * 4] for j in range(len(raw) // (N * 4))]
+
+    def one(_):
+        rcv = chk.receiver(**cfg_block)
+        t0 = time.perf_counter()
+        for j in range(n_blocks):
+            rcv.write(blocks[j % len(blocks)], j)
+        return time.perf_counter() - t0
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=cores) as ex:
+        per = list(ex.map(one, range(cores)))
+    wall = time.perf_counter() - t0
+    rate = cores * n_blocks * N / wall
+    return rate, cores, chk.kind, (f"{n_blocks} blocks of {N} samples per thread, {cores} "
+                                   f"independent receivers in parallel ({wall:.1f}s; mean "
+                                   f"{statistics.mean(per) / n_blocks * 1e6:.0f} us per block)")
+
+
+def run_ingest(args):
+    """IF ingest workload: a step is 100 ms of 24 MHz RAW32 front-end data
+    (100 receiver blocks of 1 ms, one call: the LPF history and fs/4 phase
+    carry over exactly as block by block) into 8 RF + 2 array IF buffers."""
+    import torch
+    from pocketsdr_b200 import ingest
+    rank, world, local = dist_info()
+    torch.cuda.set_device(local)
+    blk = 24000                     # the receiver's block (1 ms)
+    K = 100                         # blocks per step
+    cfg = ingest_config(blk * K)
+    rng = np.random.default_rng(3 + rank)
+    n_steps = args.warmup + args.steps
+    raw = rng.integers(0, 256, blk * K * 4 * 2, dtype=np.uint8)   # two steps' worth, reused
+    st = torch.cuda.Stream()
+    torch.cuda.set_stream(st)
+    ing = ingest.Ingest(cfg["fmt"], cfg["N"], cfg["fs"], IQ=cfg["IQ"], bits=cfg["bits"],
+                        lut_off=cfg["off"], lut_scale=cfg["scale"], lpf_fc=cfg["lpf_fc"],
+                        w=cfg["w"], arch_on=cfg["arch_on"])
+    raw_d = torch.from_numpy(raw).cuda()
+    nbuf = ing.n_rf + ing.narch
+    slots = 4                                   # buffer of 4 steps (400 ms) per channel
+    bufs = [torch.zeros(cfg["N"] * slots, dtype=torch.uint8, device="cuda") for _ in range(nbuf)]
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    step_bytes = cfg["N"] * 4
+
+    def step(k, raw_src):
+        ing.run(raw_src[(k % 2) * step_bytes:(k % 2 + 1) * step_bytes], k * K, bufs,
+                cfg["N"] * (k % slots), st.cuda_stream)
+
+    for k in range(args.warmup):
+        step(k, raw_d)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    clk = ClockSampler(local)
+    clk.start()
+    reps = 50                                   # calls per timed step sample (clock sampler)
+    for k in range(args.steps):
+        flush.fill_(k & 0xFF)
+        ev[k][0].record(st)
+        for r in range(reps):
+            step(args.warmup + k * reps + r, raw_d)
+        ev[k][1].record(st)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = sum(a.elapsed_time(b) for a, b in ev) / (reps * args.steps)   # one call
+    value = cfg["N"] / (ms / 1e3)
+    # algorithmic bytes per sample: 4 raw + 8 RF + 2 array bytes
+    bps = 4 + ing.n_rf + ing.narch
+    achieved = bps * cfg["N"] / (ms / 1e3) / 1e9
+
+    # end to end: raw bytes from pinned host memory, ingest, every buffer back
+    raw_h = torch.from_numpy(raw[:step_bytes]).pin_memory()
+    out_h = [torch.empty(cfg["N"], dtype=torch.uint8).pin_memory() for _ in range(nbuf)]
+    raw_e = torch.empty(step_bytes * 2, dtype=torch.uint8, device="cuda")
+
+    def e2e_step(k):
+        raw_e[(k % 2) * step_bytes:(k % 2 + 1) * step_bytes].copy_(raw_h, non_blocking=True)
+        step(k, raw_e)
+        base = cfg["N"] * (k % slots)
+        for b, o in zip(bufs, out_h):
+            o.copy_(b[base:base + cfg["N"]], non_blocking=True)
+
+    e2e_step(0)
+    torch.cuda.synchronize()
+    e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.fill_((k + 1) & 0xFF)
+        e2e_ev[k][0].record(st)
+        e2e_step(args.warmup + k)
+        e2e_ev[k][1].record(st)
+    torch.cuda.synchronize()
+    e2e_ms = sum(a.elapsed_time(b) for a, b in e2e_ev) / args.steps
+    line = {"metric": INGEST_METRIC, "value": value, "unit": "samples/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded random raw bytes: every 2/3-bit code equally likely)",
+            "config": {"workload": "ingest_raw32_24mhz", "samples_per_step": cfg["N"],
+                       "rf_channels": ing.n_rf, "array_channels": ing.narch, "lpf_channels": 4,
+                       "timing": f"each timed step = {reps} back-to-back calls, averaged",
+                       "l2": "flushed between timed steps (512 MB write outside the events); "
+                             "a call's 96 MB raw + 240 MB out exceed L2"},
+            "e2e": {"value": cfg["N"] / (e2e_ms / 1e3), "unit": "samples/s",
+                    "h2d_bytes_per_step": step_bytes, "d2h_bytes_per_step": nbuf * cfg["N"]},
+            "gpu_launches": reps * args.steps,
+            "roofline": {"kernel": "ingest_kernel (unpack + fs/4 mix + LPF + array combine)",
+                         "bound": "hbm", "achieved": achieved, "peak": _measured_hbm(),
+                         "unit": "GB/s", "frac": achieved / _measured_hbm(),
+                         "bytes_per_sample": bps, "traffic": None},
+            "clocks": clocks}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = dict(cfg, N=blk)
+        rate, cores, kind, desc = cpu_ingest_rate(cb, raw, 1000)
+        line["cpu_baseline"] = {"value": rate, "unit": "samples/s", "cores": cores, "kind": kind,
+                                "sample": desc}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ing.close()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "ingest_raw32_24mhz":
+        return run_ingest(args)
     if args.workload == "track_24mhz":
         return run_track(args)
     if args.workload == "refine_12mhz":

@@ -44,6 +44,17 @@ typedef struct {                             /* IF data buffer */
 } sdr_buff_t;
 #define SDR_N_CODES  10                      /* src/pocket_sdr.h:60 */
 #define SDR_MAX_CORR 107                     /* src/pocket_sdr.h:58 */
+#define SDR_MAX_RFCH 8                       /* src/pocket_sdr.h:47 */
+#define SDR_MAX_ARCH 8                       /* src/pocket_sdr.h:48 */
+#define SDR_FMT_INT8   1                     /* IF data formats, src/pocket_sdr.h:85-92 */
+#define SDR_FMT_INT8X2 2
+#define SDR_FMT_RAW8   3
+#define SDR_FMT_RAW16  4
+#define SDR_FMT_RAW16I 5
+#define SDR_FMT_RAW32  6
+#define SDR_FMT_CS8    7
+#define SDR_FMT_CS16   8
+typedef struct sdr_lpf_tag sdr_lpf_t;        /* LPF state (opaque) */
 #endif
 
 /* =========================================================================
@@ -128,6 +139,15 @@ void sdr_res_code(const int8_t *code_I, const int8_t *code_Q, int len_code,
  * mixed-radix FFT on the GPU: N+Nz must be supported (sdrg_fft_supported). */
 void sdr_gen_code_fft(const int8_t *code_I, const int8_t *code_Q, int len_code,
     double T, double coff, double fs, int N, int Nz, sdr_cpx_t *code_fft);
+
+/* Replace src/sdr_func.c:311-405 (sdr_lpf_new / sdr_lpf_free / sdr_lpf_apply,
+ * src/pocket_sdr.h:449-451): the 9-tap symmetric integer FIR (Hamming-windowed
+ * sinc, Q13 taps) applied in place to packed samples, each output clipped to
+ * +-7, with the last 8 inputs carried to the next call. sdr_lpf_new returns
+ * NULL for a cutoff outside (0, fs/2), as the reference. Bit-identical. */
+sdr_lpf_t *sdr_lpf_new(double fc, double fs);
+void sdr_lpf_free(sdr_lpf_t *lpf);
+void sdr_lpf_apply(sdr_lpf_t *lpf, sdr_cpx8_t *data, int N);
 
 /* =========================================================================
  * Part 2: additive entry points (no reference counterpart)
@@ -308,6 +328,51 @@ int sdrg_gen_code_fft(const int8_t *code_I_dev, const int8_t *code_Q_dev, int le
  * sdrg_acq_run on the same stream sees the new codes. */
 int sdrg_acq_set_codes(sdrg_acq_plan_t *plan, int g, const int8_t *code_I_dev,
     const int8_t *code_Q_dev, int len_code, double T, double coff, int N, void *stream);
+
+/* ---- IF ingest ----------------------------------------------------------------
+ * One block of raw front-end data into the IF buffers on the device: what the
+ * receiver's write_buff (src/sdr_rcv.c:840-936) does per block - raw samples
+ * through the format's tables (gen_LUT8 / gen_LUTC / gen_LUTC_rtoc,
+ * src/sdr_rcv.c:773-829; real-sampled channels of INT8 and RAW8/16/32 get the
+ * fs/4 real-to-complex mix), the LPF of the filtered channels
+ * (src/sdr_func.c:361-405: every RF channel of RAW8/16/32, channel 0
+ * otherwise) and, for the multi-channel RAW formats, the array channels
+ * (sdr_arch_combine, src/sdr_array.c:553-578). Bit-identical bytes. */
+typedef struct {
+    int fmt;                     /* SDR_FMT_INT8 .. SDR_FMT_CS16 */
+    int N;                       /* samples per RF channel per block */
+    double fs;                   /* sampling rate (Hz), for the LPF taps */
+    int IQ[SDR_MAX_RFCH];        /* per RF channel: 1 real (I), 2 complex (IQ) */
+    int bits[SDR_MAX_RFCH];      /* per RF channel: bits per component */
+    double lut_off[2];           /* INT8/INT8X2/CS8/CS16: raw -> int8 table */
+    double lut_scale[2];         /*   round((raw - off) / scale), clipped to +-7;
+                                    [1] is CS16's Q table (src/sdr_rcv.c:801-813) */
+    double lpf_fc[SDR_MAX_RFCH]; /* LPF cutoff per RF channel (Hz), <= 0: none */
+    int narch;                   /* array channels (RAW8/16/16I/32 only) */
+    int arch_on[SDR_MAX_ARCH];   /* 0: not written (sdr_arch_t.scale <= 0) */
+    int16_t w[SDR_MAX_ARCH][SDR_MAX_RFCH][2]; /* Q8 weights (re, im), sdr_arch_t.w */
+} sdrg_ingest_cfg_t;
+
+typedef struct sdrg_ingest sdrg_ingest_t;
+
+/* Builds the tables and LPF taps on the device; NULL on error. */
+sdrg_ingest_t *sdrg_ingest_new(const sdrg_ingest_cfg_t *cfg);
+void sdrg_ingest_free(sdrg_ingest_t *ing);
+
+/* raw_dev: one block (N samples, the format's bytes per sample), DEVICE.
+ * buf_dev[b] (HOST array of DEVICE pointers): RF channel buffers b < n_rf
+ * (2, 4, 8 or 8 for RAW8/16/16I/32, else 1) then the narch array channel
+ * buffers; the block lands at [base, base + N) of each. ix: the block
+ * counter (the fs/4 phase of its first sample is (ix * N) & 3, as the
+ * receiver's, src/sdr_rcv.c:846). Asynchronous on `stream` (a cudaStream_t,
+ * NULL = the legacy default stream); the LPF history passes from one call to
+ * the next, so calls on one ingest object must be ordered (one stream). */
+int sdrg_ingest_run(sdrg_ingest_t *ing, const uint8_t *raw_dev, int64_t ix,
+    uint8_t *const *buf_dev, int base, void *stream);
+
+/* The LPF taps sdr_lpf_new computes for (fc, fs) into h[9]; returns 1, or 0
+ * (h untouched) when the cutoff is outside (0, fs/2). */
+int sdrg_lpf_taps(double fc, double fs, int *h);
 
 /* Host convenience: copies IF buffers to the device, runs, and copies the
  * n_prn-total results back (synchronous). if_host[b] are HOST pointers. */

@@ -396,6 +396,117 @@ def reference_available() -> bool:
     return os.path.exists(REF_SO)
 
 
+RCV_SO = os.path.join(HERE, "_ref", "librcv_ref.so")
+
+
+class Ingest:
+    """IF-ingest checker: raw front-end blocks -> packed cpx8 buffers with the
+    per-channel LPF and the array combine. kind "reference": the reference's
+    own src/sdr_rcv.c write_buff through rcv_shim.c (_ref/librcv_ref.so);
+    kind "port": the restatement in ingest_oracle.c."""
+
+    def __init__(self, kind: str | None = None):
+        if kind is None:
+            kind = "reference" if os.path.exists(RCV_SO) else "port"
+        self.kind = kind
+        if kind == "reference":
+            L = C.CDLL(RCV_SO)
+            names = dict(lut8="orr_gen_lut8", lutc="orr_gen_lutc", taps="orr_lpf_taps",
+                         new="orr_rcv_new", write="orr_write_buff", free="orr_rcv_free",
+                         lpf_new="orr_lpf_new", lpf_apply="orr_lpf_apply", lpf_free="orr_lpf_free")
+        else:
+            L = C.CDLL(ORC_SO)
+            names = dict(lut8="orc_gen_lut8", lutc="orc_gen_lutc", taps="orc_lpf_taps",
+                         new="orc_ingest_new", write="orc_ingest_write", free="orc_ingest_free",
+                         lpf_new="orc_lpf_new", lpf_apply="orc_lpf_apply", lpf_free="orc_lpf_free")
+        f = {k: getattr(L, v) for k, v in names.items()}
+        f["lut8"].argtypes = [_i, _d, _d, _p]
+        f["lutc"].argtypes = [_i, _i, _i, _i, _i, _p]
+        f["taps"].argtypes = [_d, _d, _p]
+        f["taps"].restype = _i
+        f["new"].argtypes = [_i, _i, _p, _p, _p, _p, _p, _d, _i, _p, _p]
+        f["new"].restype = _p
+        f["write"].argtypes = [_p, _p, C.c_int64, _p]
+        f["free"].argtypes = [_p]
+        f["lpf_new"].argtypes = [_d, _d]
+        f["lpf_new"].restype = _p
+        f["lpf_apply"].argtypes = [_p, _p, _i]
+        f["lpf_free"].argtypes = [_p]
+        self.f, self.lib = f, L
+
+    def gen_lut8(self, fmt, off, scale):
+        out = np.zeros(65536 if fmt == 8 else 256, np.int8)
+        self.f["lut8"](fmt, off, scale, _ptr(out))
+        return out
+
+    def gen_lutc(self, fmt, rfch, IQ, bits, rtoc):
+        out = np.zeros(1024 if rtoc else 256, np.uint8)
+        self.f["lutc"](fmt, rfch, IQ, bits, int(rtoc), _ptr(out))
+        return out
+
+    def lpf_taps(self, fc, fs):
+        h = np.zeros(9, np.int32)
+        return h if self.f["taps"](fc, fs, _ptr(h)) else None
+
+    def receiver(self, fmt, N, IQ, bits, off=(0.0, 0.0), scale=(1.0, 1.0), lpf_fc=None, fs=1.0,
+                 w=None, arch_on=None):
+        return _IngestState(self, fmt, N, IQ, bits, off, scale, lpf_fc, fs, w, arch_on)
+
+    def lpf(self, fc, fs):
+        return _LpfState(self, fc, fs)
+
+
+class _IngestState:
+    def __init__(self, chk, fmt, N, IQ, bits, off, scale, lpf_fc, fs, w, arch_on):
+        self.chk, self.N = chk, N
+        self.nrf = {3: 2, 4: 4, 5: 8, 6: 8}.get(fmt, 1)
+        iq = np.zeros(8, np.int32); iq[:len(IQ)] = IQ
+        bt = np.zeros(8, np.int32); bt[:len(bits)] = bits
+        fc = np.zeros(8, np.float64)
+        if lpf_fc is not None:
+            fc[:len(lpf_fc)] = lpf_fc
+        self.narch = 0 if w is None else len(w)
+        wa = np.zeros((max(self.narch, 1), self.nrf, 2), np.int16)
+        if self.narch:
+            wa[:] = np.asarray(w, np.int16).reshape(self.narch, self.nrf, 2)
+        on = np.ones(8, np.int32)
+        if arch_on is not None:
+            on[:len(arch_on)] = arch_on
+        o = np.asarray(off, np.float64)
+        s = np.asarray(scale, np.float64)
+        self._keep = (iq, bt, fc, wa, on, o, s)
+        self.h = chk.f["new"](fmt, N, _ptr(iq), _ptr(bt), _ptr(o), _ptr(s), _ptr(fc), fs,
+                              self.narch, _ptr(wa), _ptr(on))
+
+    def write(self, raw, ix):
+        """One block: uint8 [(n_rf + narch), N]."""
+        raw = np.ascontiguousarray(raw, np.uint8)
+        out = np.zeros((self.nrf + self.narch, self.N), np.uint8)
+        self.chk.f["write"](self.h, _ptr(raw), int(ix), _ptr(out))
+        return out
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.chk.f["free"](self.h)
+            self.h = None
+
+
+class _LpfState:
+    def __init__(self, chk, fc, fs):
+        self.chk = chk
+        self.h = chk.f["lpf_new"](fc, fs)
+
+    def apply(self, data):
+        d = np.array(data, np.uint8)
+        self.chk.f["lpf_apply"](self.h, _ptr(d), len(d))
+        return d
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.chk.f["lpf_free"](self.h)
+            self.h = None
+
+
 def best():
     """The reference build when present, else the restatement."""
     return Reference() if reference_available() else Restatement()

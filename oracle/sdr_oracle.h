@@ -109,6 +109,21 @@ void orc_refine_sums(const int8_t *chips, int Lc, double rate_nom, double rate,
 void orc_refine_step(const double *sums, int K, int Nb, double fs, double rate_nom,
                      double fc, int model, double *theta, double *rate, double *info);
 
+/* IF ingest (ingest_oracle.c): raw front-end blocks -> packed cpx8 buffers,
+ * per-channel LPF and array combine, as src/sdr_rcv.c:773-936,
+ * src/sdr_func.c:311-405 and src/sdr_array.c:487-578. */
+void orc_gen_lut8(int fmt, double off, double scale, int8_t *out);
+void orc_gen_lutc(int fmt, int rfch, int IQ, int bits, int rtoc, uint8_t *out);
+int orc_lpf_taps(double fc, double fs, int *h);
+void *orc_ingest_new(int fmt, int N, const int *IQ, const int *bits, const double *off,
+                     const double *scale, const double *lpf_fc, double fs, int narch,
+                     const int16_t *w, const int *arch_on);
+void orc_ingest_write(void *g, const uint8_t *raw, int64_t ix, uint8_t *out);
+void orc_ingest_free(void *g);
+void *orc_lpf_new(double fc, double fs);
+void orc_lpf_apply(void *f, uint8_t *data, int N);
+void orc_lpf_free(void *f);
+
 #ifdef __cplusplus
 }
 #endif

@@ -36,6 +36,13 @@ class AcqResult(C.Structure):
                 ("pave", _d), ("fd", _d)]
 
 
+class IngestCfg(C.Structure):
+    """sdrg_ingest_cfg_t."""
+    _fields_ = [("fmt", _i), ("N", _i), ("fs", _d), ("IQ", _i * 8), ("bits", _i * 8),
+                ("lut_off", _d * 2), ("lut_scale", _d * 2), ("lpf_fc", _d * 8),
+                ("narch", _i), ("arch_on", _i * 8), ("w", C.c_int16 * (8 * 8 * 2))]
+
+
 class RefineSig(C.Structure):
     """sdrg_refine_sig_t."""
     _fields_ = [("chips", _p), ("Lc", _i), ("rate", _d), ("fi", _d), ("fc", _d)]
@@ -57,6 +64,9 @@ SIGNATURES = {
     "sdr_dop_bins": ([_d, _f, _f, C.POINTER(_i)], C.POINTER(_f)),
     "sdr_res_code": ([_p, _p, _i, _d, _d, _d, _i, _i, _p], None),
     "sdr_gen_code_fft": ([_p, _p, _i, _d, _d, _d, _i, _i, _p], None),
+    "sdr_lpf_new": ([_d, _d], _p),
+    "sdr_lpf_free": ([_p], None),
+    "sdr_lpf_apply": ([_p, _p, _i], None),
     "sdr_gpu_last_error": ([C.c_char_p, _i], _i),
     "sdr_gpu_clear_error": ([], None),
     "sdrg_init": ([_i], _i),
@@ -76,6 +86,10 @@ SIGNATURES = {
     "sdrg_res_code": ([_p, _p, _i, _i, _d, _d, _d, _i, _i, _i, _p, _p], _i),
     "sdrg_gen_code_fft": ([_p, _p, _i, _i, _d, _d, _d, _i, _i, _p, _p], _i),
     "sdrg_acq_set_codes": ([_p, _i, _p, _p, _i, _d, _d, _i, _p], _i),
+    "sdrg_ingest_new": ([C.POINTER(IngestCfg)], _p),
+    "sdrg_ingest_free": ([_p], None),
+    "sdrg_ingest_run": ([_p, _p, C.c_int64, _p, _i, _p], _i),
+    "sdrg_lpf_taps": ([_d, _d, _p], _i),
     "sdrg_refine_plan_new": ([C.POINTER(RefineSig), _i, _d, _i, _i, _i], _p),
     "sdrg_refine_plan_free": ([_p], None),
     "sdrg_refine_plan_info": ([_p, _p], _i),
