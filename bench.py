@@ -903,10 +903,76 @@ def run_ingest(args):
     return 0
 
 
+SRCH_METRIC = ("channel searches/s: every idle channel of the multi-GNSS setup (163 channels, "
+               "sdr_t_acq 20 ms) through one batched search call")
+
+
+def run_search_batch(args):
+    """Batched search scheduling: a step is one sdrg_search_batch call that
+    searches every channel of the acq_multi_24mhz signal set (GPS L1 C/A 32,
+    Galileo E1-B 36, BeiDou B1I 63, GPS L5-I 32; sdr_t_acq = 20 ms, so 20 /
+    5 / 20 / 20 code periods) from its chips: grouping, plan and code DFTs on
+    the device, search, decisions back on the host. Timed with CUDA events on
+    the call's stream around the whole (synchronous) call, so host work
+    inside it counts."""
+    import torch
+    from pocketsdr_b200 import codes, schedule
+    rank, world, local = dist_info()
+    torch.cuda.set_device(local)
+    wl = make_workload("acq_multi_24mhz", 2 + rank)
+    st = torch.cuda.Stream()
+    torch.cuda.set_stream(st)
+    bufs_d = [torch.from_numpy(b).cuda() for b in wl.bufs]
+    setups, reqs = [], []
+    for i, g in enumerate(wl.groups):
+        chips = np.stack([codes.gen_code(g.sig, p) for p in g.prns])
+        setups.append(schedule.Setup(chips, g.T, g.fs, g.fi, max_dop=5000.0, buf=g.buf, N=g.N))
+        reqs += [schedule.Request(i, k) for k in range(len(g.prns))]
+    t_acq, thres = 20e-3, 38.0
+    for _ in range(args.warmup):
+        schedule.search(setups, reqs, bufs_d, 0, t_acq, thres)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    clk = ClockSampler(local)
+    clk.start()
+    res = None
+    for k in range(args.steps):
+        ev[k][0].record(st)
+        res = schedule.search(setups, reqs, bufs_d, 0, t_acq, thres)
+        ev[k][1].record(st)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
+    n = len(reqs)
+    line = {"metric": SRCH_METRIC, "value": n / (ms / 1e3), "unit": "searches/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": "search_batch_24mhz", "channels": n,
+                                            "t_acq_s": t_acq, "thres_cn0": thres,
+                                            "includes": "grouping, plan build, device code DFTs, "
+                                                        "search, decisions to host"},
+            "e2e": {"value": n / (ms / 1e3), "unit": "searches/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": n * 40,
+                    "note": "the call is already end to end from the caller's view (device IF "
+                            "buffers, host results)"},
+            "found": int(res["found"].sum()), "clocks": clocks}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, cores, kind, desc = cpu_reference_rate(wl)
+        cells_per_search = wl.cells / n
+        line["cpu_baseline"] = {"value": rate / cells_per_search, "unit": "searches/s",
+                                "cores": cores, "kind": kind, "sample": desc}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "search_batch_24mhz":
+        return run_search_batch(args)
     if args.workload == "ingest_raw32_24mhz":
         return run_ingest(args)
     if args.workload == "track_24mhz":

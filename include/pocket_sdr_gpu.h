@@ -149,6 +149,13 @@ sdr_lpf_t *sdr_lpf_new(double fc, double fs);
 void sdr_lpf_free(sdr_lpf_t *lpf);
 void sdr_lpf_apply(sdr_lpf_t *lpf, sdr_cpx8_t *data, int N);
 
+/* Replaces src/sdr_func.c:1141-1182 (sdr_psd_cpx, src/pocket_sdr.h:430-431).
+ * Welch PSD without overlap (Hann window, len_buff / N segments), dB/Hz:
+ * N/2 bins for IQ = 1, N bins from -fs/2 for IQ = 2. FP32 on the GPU; N must
+ * be supported (sdrg_fft_supported). */
+void sdr_psd_cpx(const sdr_cpx_t *buff, int len_buff, int N, double fs, int IQ,
+    float *psd);
+
 /* =========================================================================
  * Part 2: additive entry points (no reference counterpart)
  * ========================================================================= */
@@ -328,6 +335,73 @@ int sdrg_gen_code_fft(const int8_t *code_I_dev, const int8_t *code_Q_dev, int le
  * sdrg_acq_run on the same stream sees the new codes. */
 int sdrg_acq_set_codes(sdrg_acq_plan_t *plan, int g, const int8_t *code_I_dev,
     const int8_t *code_Q_dev, int len_code, double T, double coff, int N, void *stream);
+
+/* ---- PSD on the device ----------------------------------------------------
+ * sdr_psd_cpx on DEVICE data (buff_dev: len_buff complex floats; psd_dev:
+ * N/2 or N floats), and straight from a packed IF buffer: n samples of the
+ * circular cpx8 buffer if_dev (len_if samples) from sample ix - the window the
+ * receiver's sdr_rcv_rfch_psd (src/sdr_rcv.c:395-412) unpacks to floats
+ * first. Asynchronous on `stream` (NULL = the legacy default stream);
+ * scratch is stream-ordered (cudaMallocAsync). */
+int sdrg_psd(const sdr_cpx_t *buff_dev, int len_buff, int N, double fs, int IQ,
+    float *psd_dev, void *stream);
+int sdrg_psd_if(const uint8_t *if_dev, int len_if, int ix, int n, int N, double fs,
+    int IQ, float *psd_dev, void *stream);
+
+/* ---- batched signal search ---------------------------------------------------
+ * The receiver searches one channel at a time: update_srch_ch
+ * (src/sdr_rcv.c:1222-1257) gives the search to the next IDLE channel, whose
+ * search_sig (src/sdr_ch.c:398-450) accumulates sdr_search_code over one code
+ * period per update until n_sum * T >= sdr_t_acq and then decides with
+ * sdr_corr_max / sdr_fine_dop. sdrg_search_batch runs that whole search for
+ * every channel the caller submits (the caller keeps the receiver's choice of
+ * which channels are ready: re-acquisition, assisted or short-code ones) in
+ * one batched acquisition on the device: unaided channels of one code setup
+ * share a signal group with sdr_dop_bins(T, 0, max_dop) bins; a channel with an
+ * external Doppler aid gets its own fd_ext_n (default 3) bins of 0.5 / T around
+ * fd_ext. Sum s uses samples [ix + s N, ix + s N + 2 N) of its IF buffer, the
+ * windows of consecutive code periods from ix. */
+typedef struct {
+    const int8_t *code_dev; /* [n_prn][len_code] code chips, DEVICE */
+    int len_code, n_prn;
+    double T;              /* code period (s) */
+    double fs, fi;         /* sampling rate, IF (Hz) */
+    int N;                 /* samples per code period (FFTs of 2 N) */
+    double max_dop;        /* Doppler range (Hz), the receiver's sdr_max_dop */
+    int buf;               /* IF buffer index */
+} sdrg_srch_setup_t;
+
+typedef struct {
+    int setup;             /* setup index */
+    int prn;               /* code row within the setup */
+    float fd_ext;          /* external Doppler aid (Hz), 0: none (sdr_acq_t) */
+    int fd_ext_n;          /* aided bins, 0: 3 */
+} sdrg_srch_req_t;
+
+typedef struct {
+    int found;             /* C/N0 >= thres_cn0: start tracking */
+    int bin, offset;       /* peak Doppler bin (of the request's bins), offset */
+    float cn0;             /* C/N0 (dB-Hz), as sdr_corr_max */
+    double fd;             /* fine Doppler (Hz), as sdr_fine_dop */
+    double coff;           /* code offset (s) = offset / fs, as start_track gets */
+    int n_sum;             /* code periods accumulated */
+} sdrg_srch_res_t;
+
+/* Runs every request's search (res[i] for req[i]); if_dev / len_if: DEVICE
+ * IF buffers; t_acq: the receiver's sdr_t_acq (s); thres_cn0: its
+ * sdr_thres_cn0_l. Synchronous (returns with the results on the host);
+ * work is issued on `stream` (NULL = the calling thread's stream). */
+int sdrg_search_batch(const sdrg_srch_setup_t *setups, int n_setup,
+    const sdrg_srch_req_t *req, int n_req, const uint8_t *const *if_dev,
+    const int *len_if, int ix, double t_acq, double thres_cn0, sdrg_srch_res_t *res,
+    void *stream);
+
+/* The grouping sdrg_search_batch uses (host only, no device work): returns
+ * the number of signal groups (or a negative status) and, if non-NULL, each
+ * request's group and each group's sums and Doppler bins. */
+int sdrg_srch_groups(const sdrg_srch_setup_t *setups, int n_setup,
+    const sdrg_srch_req_t *req, int n_req, double t_acq, int *group_of_req,
+    int *n_sum, int *len_fds);
 
 /* ---- IF ingest ----------------------------------------------------------------
  * One block of raw front-end data into the IF buffers on the device: what the

@@ -77,6 +77,7 @@ class Restatement:
         L.orc_fft.argtypes = [_p, _i, _i, _p]
         L.orc_corr_fft.argtypes = [_p, _p, _i, _p]
         L.orc_corr_fft_cpx.argtypes = [_p, _i, _i, _i, _d, _d, _d, _p, _p]
+        L.orc_psd_cpx.argtypes = [_p, _i, _i, _d, _i, _p]
         L.orc_search_code.argtypes = [_p, _p, _i, _i, _i, _d, _d, _p, _i, _p]
         L.orc_corr_max.argtypes = [_p, _i, _i, _i, _d, _p]
         L.orc_corr_max.restype = _f
@@ -144,6 +145,12 @@ class Restatement:
         out = np.zeros(N, np.complex64)
         self.lib.orc_corr_fft_cpx(_ptr(buff), len(buff), ix, N, fs, fc, phi,
                                   _ptr(code_fft), _ptr(out))
+        return out
+
+    def psd_cpx(self, buff, N, fs, IQ):
+        buff = np.ascontiguousarray(buff, np.complex64)
+        out = np.zeros(N // 2 if IQ == 1 else N, np.float32)
+        self.lib.orc_psd_cpx(_ptr(buff), len(buff), N, fs, IQ, _ptr(out))
         return out
 
     def search_code(self, code_fft, buff, ix, N, fs, fi, fds, P):
@@ -284,6 +291,7 @@ class Reference:
         L.sdr_cpx_fft.argtypes = [_p, _i, _i, _p]
         L.sdr_cpx_fft.restype = _i
         L.sdr_free.argtypes = [_p]
+        L.sdr_psd_cpx.argtypes = [_p, _i, _i, _d, _i, _p]
         L.sdr_func_init(b"")
 
     def _buff(self, buff):
@@ -335,6 +343,12 @@ class Reference:
         out = np.zeros(N, np.complex64)
         self.lib.sdr_corr_fft_cpx(_ptr(buff), len(buff), ix, N, fs, fc, phi,
                                   _ptr(code_fft), _ptr(out))
+        return out
+
+    def psd_cpx(self, buff, N, fs, IQ):
+        buff = np.ascontiguousarray(buff, np.complex64)
+        out = np.zeros(N // 2 if IQ == 1 else N, np.float32)
+        self.lib.sdr_psd_cpx(_ptr(buff), len(buff), N, fs, IQ, _ptr(out))
         return out
 
     def search_code(self, code_fft, buff, ix, N, fs, fi, fds, P, T=1e-3):

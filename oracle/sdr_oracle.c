@@ -389,3 +389,39 @@ void orc_gen_code_fft(const int8_t *code_I, const int8_t *code_Q,
     }
     free(a); free(b);
 }
+
+/* src/sdr_func.c:1116-1182 (hann_window, sdr_psd_cpx): Welch PSD without
+ * overlap, Hann window (float taps, float sum of squares), |X|^2 summed in
+ * float over the M = len / N segments in order, matplotlib.psd scale, dB;
+ * real data keeps N/2 bins, complex data is rotated to start at -fs/2. The
+ * transform is the oracle's double FFT of the float-windowed segment. */
+void orc_psd_cpx(const float *buff, int len_buff, int N, double fs, int IQ, float *psd)
+{
+    float *w = (float *)malloc(sizeof(float) * N), *p = (float *)calloc(N, sizeof(float));
+    double *a = (double *)malloc(sizeof(double) * 2 * N), *b = (double *)malloc(sizeof(double) * 2 * N);
+    float wss = 0.0f;
+    for (int i = 0; i < N; i++) {
+        w[i] = (float)(0.5 + 0.5 * cos(2.0 * 3.1415926535897932 * (i - 0.5 * (N - 1)) / (N - 1)));
+        wss += w[i] * w[i];
+    }
+    int M = len_buff / N;
+    for (int i = 0; i < M; i++) {
+        for (int j = 0; j < N; j++) {
+            a[2 * j] = (float)(buff[2 * ((size_t)N * i + j)] * w[j]);
+            a[2 * j + 1] = (float)(buff[2 * ((size_t)N * i + j) + 1] * w[j]);
+        }
+        orc_fft(a, N, 0, b);
+        for (int j = 0; j < N; j++) {
+            float re = (float)b[2 * j], im = (float)b[2 * j + 1];
+            p[j] += re * re + im * im;
+        }
+    }
+    float scale = (float)(1.0 / M / wss / fs * (IQ == 1 ? 2.0 : 1.0));
+    if (IQ == 1) {
+        for (int i = 0; i < N / 2; i++) psd[i] = 10.0f * log10f(p[i] * scale);
+    } else {
+        for (int i = 0; i < N / 2; i++) psd[i] = 10.0f * log10f(p[N / 2 + i] * scale);
+        for (int i = N / 2; i < N; i++) psd[i] = 10.0f * log10f(p[i - N / 2] * scale);
+    }
+    free(w); free(p); free(a); free(b);
+}

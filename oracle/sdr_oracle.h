@@ -109,6 +109,9 @@ void orc_refine_sums(const int8_t *chips, int Lc, double rate_nom, double rate,
 void orc_refine_step(const double *sums, int K, int Nb, double fs, double rate_nom,
                      double fc, int model, double *theta, double *rate, double *info);
 
+/* Welch PSD of float IQ data (src/sdr_func.c:1141-1182). */
+void orc_psd_cpx(const float *buff, int len_buff, int N, double fs, int IQ, float *psd);
+
 /* IF ingest (ingest_oracle.c): raw front-end blocks -> packed cpx8 buffers,
  * per-channel LPF and array combine, as src/sdr_rcv.c:773-936,
  * src/sdr_func.c:311-405 and src/sdr_array.c:487-578. */

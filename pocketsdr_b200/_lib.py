@@ -43,6 +43,23 @@ class IngestCfg(C.Structure):
                 ("narch", _i), ("arch_on", _i * 8), ("w", C.c_int16 * (8 * 8 * 2))]
 
 
+class SrchSetup(C.Structure):
+    """sdrg_srch_setup_t."""
+    _fields_ = [("code_dev", _p), ("len_code", _i), ("n_prn", _i), ("T", _d), ("fs", _d),
+                ("fi", _d), ("N", _i), ("max_dop", _d), ("buf", _i)]
+
+
+class SrchReq(C.Structure):
+    """sdrg_srch_req_t."""
+    _fields_ = [("setup", _i), ("prn", _i), ("fd_ext", _f), ("fd_ext_n", _i)]
+
+
+class SrchRes(C.Structure):
+    """sdrg_srch_res_t."""
+    _fields_ = [("found", _i), ("bin", _i), ("offset", _i), ("cn0", _f), ("fd", _d),
+                ("coff", _d), ("n_sum", _i)]
+
+
 class RefineSig(C.Structure):
     """sdrg_refine_sig_t."""
     _fields_ = [("chips", _p), ("Lc", _i), ("rate", _d), ("fi", _d), ("fc", _d)]
@@ -67,6 +84,7 @@ SIGNATURES = {
     "sdr_lpf_new": ([_d, _d], _p),
     "sdr_lpf_free": ([_p], None),
     "sdr_lpf_apply": ([_p, _p, _i], None),
+    "sdr_psd_cpx": ([_p, _i, _i, _d, _i, _p], None),
     "sdr_gpu_last_error": ([C.c_char_p, _i], _i),
     "sdr_gpu_clear_error": ([], None),
     "sdrg_init": ([_i], _i),
@@ -86,6 +104,11 @@ SIGNATURES = {
     "sdrg_res_code": ([_p, _p, _i, _i, _d, _d, _d, _i, _i, _i, _p, _p], _i),
     "sdrg_gen_code_fft": ([_p, _p, _i, _i, _d, _d, _d, _i, _i, _p, _p], _i),
     "sdrg_acq_set_codes": ([_p, _i, _p, _p, _i, _d, _d, _i, _p], _i),
+    "sdrg_search_batch": ([C.POINTER(SrchSetup), _i, C.POINTER(SrchReq), _i, _p, _p, _i, _d, _d,
+                           C.POINTER(SrchRes), _p], _i),
+    "sdrg_srch_groups": ([C.POINTER(SrchSetup), _i, C.POINTER(SrchReq), _i, _d, _p, _p, _p], _i),
+    "sdrg_psd": ([_p, _i, _i, _d, _i, _p, _p], _i),
+    "sdrg_psd_if": ([_p, _i, _i, _i, _i, _d, _i, _p, _p], _i),
     "sdrg_ingest_new": ([C.POINTER(IngestCfg)], _p),
     "sdrg_ingest_free": ([_p], None),
     "sdrg_ingest_run": ([_p, _p, C.c_int64, _p, _i, _p], _i),

@@ -137,16 +137,7 @@ __global__ void __launch_bounds__(256) code_combine_kernel(const float2 *F, cons
         float2 g[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) g[r] = F[(p * R + r) * (size_t)M + q];
-        if constexpr (R > 1) {
-            const float2 tc = cconj(__ldg(split + q));
-            float2 w = tc;
-#pragma unroll
-            for (int r = 1; r < R; ++r) {
-                g[r] = cmul(g[r], w);
-                if (r + 1 < R) w = cmul(w, tc);
-            }
-            Dft<R, -1>::run(g);
-        }
+        split_combine_fwd<R>(g, R > 1 ? __ldg(split + q) : make_float2(1.0f, 0.0f));
         const int k = natural ? __ldg(kperm + q) : q;
 #pragma unroll
         for (int j = 0; j < R; ++j) out[(p * R + j) * (size_t)M + k] = cconj(g[j]);

@@ -504,6 +504,25 @@ __device__ __forceinline__ void fft_inverse_static(float2 *sm, const float2 *tw,
     s_pass0_store<P::R0, P::S0, P::NT>(sm, tw + P::O0, store);
 }
 
+// Split combine of a length-L = R*M forward transform computed as R
+// decimated sub-transforms F_r = FFT_M(x[R m + r]): given g[r] = F_r[k] at
+// k = k(q) and t = exp(+2 pi i k / L), leaves g[j] = X[k + j M]
+// = sum_r e^{-2 pi i r (k + j M) / L} F_r[k].
+template <int R>
+__device__ __forceinline__ void split_combine_fwd(float2 *g, float2 t)
+{
+    if constexpr (R > 1) {
+        const float2 tc = cconj(t);
+        float2 w = tc;
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+            g[r] = cmul(g[r], w);
+            if (r + 1 < R) w = cmul(w, tc);
+        }
+        Dft<R, -1>::run(g);
+    }
+}
+
 // Copies the per-pass twiddle tables from global to shared memory.
 __device__ __forceinline__ void load_twiddles(float2 *tw_sm, const float2 *tw_g,
                                               int n)

@@ -11,6 +11,7 @@ Same names, arguments and return values as the reference module
   corr_std(buff, ix, N, fs, fc, phi, code, pos) -> corr     (:156-171)
   corr_fft(buff, ix, N, fs, fc, phi, code_fft) -> corr      (:174-187)
   mix_carr(buff, ix, N, fs, fc, phi) -> int8 [N, 2]
+  psd(data, N, fs, IQ) -> float32 [N/2 or N] (dB/Hz)          (:215-223)
 
 `buff` is the complex64 IF array of the reference's Python layer. Like the
 reference's C-library path (LIBSDR_ENA), samples are cast to int8 and packed
@@ -69,6 +70,15 @@ def search_code(code_fft, T, buff, ix, fs, fi, fds):
         C_ = corr_fft(buff, ix, len(code_fft), fs, fi + fds[i], 0.0, code_fft)[:N]
         P[i] = np.abs(C_) ** 2
     return P
+
+
+def psd(data, N, fs, IQ):
+    """Welch PSD of IF data (sdr_psd_cpx): N/2 bins for IQ = 1, N for IQ = 2."""
+    data = np.ascontiguousarray(data, np.complex64)
+    out = np.zeros(N if IQ == 2 else N // 2, np.float32)
+    lib.sdr_psd_cpx(ptr(data), len(data), int(N), float(fs), int(IQ), ptr(out))
+    check("sdr_psd_cpx")
+    return out
 
 
 def corr_max(P, T):

@@ -233,3 +233,19 @@ def test_replica_restatement_vs_reference(orc):
         a = orc.gen_code_fft(c, None, 1e-3, 2e-4, N * 1000.0, N, Nz)
         b = R.gen_code_fft(c, None, 1e-3, 2e-4, N * 1000.0, N, Nz)
         assert np.abs(a - b).max() <= 1e-6 * np.abs(b).max()
+
+
+@pytest.mark.skipif(not HAVE_REF, reason="reference build (oracle/_ref) not present")
+def test_psd_restatement_vs_reference(orc):
+    """Welch PSD (src/sdr_func.c:1141-1182): the restatement within 1e-4 dB of
+    the reference build, real and complex data, several FFT sizes, and the
+    same NaN output when the data hold no full segment."""
+    R = oracle.Reference()
+    rng = np.random.default_rng(2)
+    for N, IQ, n in ((4096, 2, 4096 * 30 + 17), (4096, 1, 4096 * 9), (6000, 2, 42000),
+                     (1024, 1, 100)):
+        x = (rng.integers(-7, 8, n) + 1j * rng.integers(-7, 8, n) * (IQ == 2)).astype(np.complex64)
+        a, b = R.psd_cpx(x, N, 24e6, IQ), orc.psd_cpx(x, N, 24e6, IQ)
+        assert np.array_equal(np.isnan(a), np.isnan(b))
+        ok = ~np.isnan(a)
+        assert np.all(np.abs(a[ok] - b[ok]) <= 1e-4), (N, IQ)
