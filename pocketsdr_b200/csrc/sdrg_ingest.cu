@@ -11,12 +11,15 @@
 // ahead of every search and correlator; here one kernel does all of it, so
 // raw bytes uploaded once become search-ready buffers without a host pass.
 //
-// Kernel: one CTA per tile of 1024 samples. It unpacks the tile and the 8
-// samples before it (the filter's reach; the previous block's last 8
-// unfiltered samples for the first tile) of every RF channel into shared
-// memory, then each thread filters, packs and combines its samples. The
-// filter is the reference's integer FIR, so every output byte is exact.
-// Reads 1-4 raw bytes and writes one byte per channel per sample: HBM bound.
+// Kernel (one instantiation per format): one CTA per tile of 1024 samples,
+// 4 consecutive samples per thread. It unpacks the tile and the 8 samples
+// before it (the filter's reach; the previous block's last 8 unfiltered
+// samples for the first tile) of every RF channel into shared memory as
+// packed bytes (tables staged in shared memory, raw bytes read with one
+// vector load per 4 samples), then each thread filters (the reference's
+// integer FIR on nibbles extracted with bfe), packs and stores 4 samples per
+// channel as one 32-bit word and forms the array channels. Every output byte
+// is exact. Reads 1-4 raw bytes and writes one byte per channel per sample.
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -44,113 +47,203 @@ __host__ __device__ __forceinline__ uint8_t pack8(int I, int Q)
 
 struct IngestArgs {
     const uint8_t *raw;
-    int fmt, N, nrfch, ph0;
+    int N, ph0;
     int rtoc_mask, lpf_mask;
+    int vec;                  // raw 16-byte aligned and outputs 4-byte aligned
     const int8_t *lut8;       // [2][65536] (INT8 formats; CS16 uses both)
     const uint8_t *lutc;      // [8][1024] (RAW formats)
-    const char2 *hist_in;     // [8][8] unfiltered samples before the block
-    char2 *hist_out;          // [8][8]
+    const uint8_t *hist_in;   // [8][8] packed samples before the block (unfiltered)
+    uint8_t *hist_out;        // [8][8]
     uint8_t *out[kMaxRf];
     int narch;
     uint8_t *aout[kMaxArch];
+    int amask[kMaxArch];      // RF channels with a non-zero weight per array channel
     int h[kMaxRf][9];
     short2 w[kMaxArch][kMaxRf];
 };
 
-// sample n of RF channel k, as write_buff stores it (before the LPF)
-__device__ __forceinline__ char2 unpack(const IngestArgs &a, int k, int n)
+__host__ __device__ constexpr int bps_of(int f)
 {
-    uint8_t b;
-    switch (a.fmt) {
-    case F_CPX8:
-        b = a.raw[n];
-        break;
-    case F_INT8: {
-        const int I = __ldg(a.lut8 + a.raw[n]);
-        if (!(a.rtoc_mask & 1)) { b = pack8(I, 0); break; }
-        const int ph = (a.ph0 + n) & 3;
-        b = ph == 0 ? pack8(I, 0) : ph == 1 ? pack8(0, -I) : ph == 2 ? pack8(-I, 0) : pack8(0, I);
-        break;
-    }
-    case F_INT8X2:
-        b = pack8(__ldg(a.lut8 + a.raw[2 * n]), -__ldg(a.lut8 + a.raw[2 * n + 1]));
-        break;
-    case F_CS8:
-        b = pack8(__ldg(a.lut8 + a.raw[2 * n]), __ldg(a.lut8 + a.raw[2 * n + 1]));
-        break;
-    case F_CS16: {
-        const uint16_t u = (uint16_t)(a.raw[4 * n] | (a.raw[4 * n + 1] << 8));
-        const uint16_t v = (uint16_t)(a.raw[4 * n + 2] | (a.raw[4 * n + 3] << 8));
-        b = pack8(__ldg(a.lut8 + u), __ldg(a.lut8 + 65536 + v));
-        break;
-    }
-    case F_RAW16I:
-        b = __ldg(a.lutc + k * 1024 + a.raw[2 * n + k / 4]);
-        break;
-    default: {   // RAW8 / RAW16 / RAW32: RF channels 2j and 2j+1 share byte j
-        const int bpr = a.nrfch / 2;
-        const uint8_t byte = a.raw[(size_t)bpr * n + k / 2];
-        const int ph = ((a.rtoc_mask >> k) & 1) ? ((a.ph0 + n) & 3) : 0;
-        b = __ldg(a.lutc + k * 1024 + (ph << 8) + byte);
-    }
-    }
-    return make_char2((signed char)((int8_t)(uint8_t)(b << 4) >> 4), (signed char)((int8_t)b >> 4));
+    return (f == F_CPX8 || f == F_INT8 || f == F_RAW8) ? 1
+         : (f == F_INT8X2 || f == F_CS8 || f == F_RAW16 || f == F_RAW16I) ? 2 : 4;
+}
+__host__ __device__ constexpr int nrf_of(int f)
+{
+    return f == F_RAW8 ? 2 : f == F_RAW16 ? 4 : (f == F_RAW16I || f == F_RAW32) ? 8 : 1;
 }
 
+// sign-extended 4-bit field at bit `pos` (the I or Q nibble of a packed sample)
+__device__ __forceinline__ int nib(uint32_t w, int pos)
+{
+    int r;
+    asm("bfe.s32 %0, %1, %2, 4;" : "=r"(r) : "r"(w), "r"(pos));
+    return r;
+}
+
+// Packed byte (as write_buff stores it, before the LPF) of RF channel k for
+// one sample whose raw bytes are `b` (little-endian, bps_of(FMT) bytes), at
+// fs/4 phase ph.
+template <int FMT>
+__device__ __forceinline__ uint32_t unpack1(uint32_t b, int k, int ph, const IngestArgs &a,
+                                            const uint8_t *lutc, const int8_t *lut8)
+{
+    if constexpr (FMT == F_CPX8) {
+        return b & 0xFF;
+    } else if constexpr (FMT == F_INT8) {
+        const int I = lut8[b & 0xFF];
+        if (!(a.rtoc_mask & 1)) return pack8(I, 0);
+        return ph == 0 ? pack8(I, 0) : ph == 1 ? pack8(0, -I) : ph == 2 ? pack8(-I, 0) : pack8(0, I);
+    } else if constexpr (FMT == F_INT8X2) {
+        return pack8(lut8[b & 0xFF], -lut8[(b >> 8) & 0xFF]);
+    } else if constexpr (FMT == F_CS8) {
+        return pack8(lut8[b & 0xFF], lut8[(b >> 8) & 0xFF]);
+    } else if constexpr (FMT == F_CS16) {
+        return pack8(__ldg(a.lut8 + (b & 0xFFFF)), __ldg(a.lut8 + 65536 + (b >> 16)));
+    } else if constexpr (FMT == F_RAW16I) {
+        return lutc[k * 1024 + ((b >> (8 * (k / 4))) & 0xFF)];
+    } else {   // RAW8 / RAW16 / RAW32: RF channels 2j and 2j+1 share byte j
+        const int p = ((a.rtoc_mask >> k) & 1) ? ph : 0;
+        return lutc[k * 1024 + (p << 8) + ((b >> (8 * (k / 2))) & 0xFF)];
+    }
+}
+
+// raw bytes of sample s of a loaded quad (4 samples)
+template <int BPS>
+__device__ __forceinline__ uint32_t sample_bytes(const uint32_t *rw, int s)
+{
+    if constexpr (BPS == 1) return (rw[0] >> (8 * s)) & 0xFF;
+    else if constexpr (BPS == 2) return (rw[s >> 1] >> (16 * (s & 1))) & 0xFFFF;
+    else return rw[s];
+}
+
+// One CTA per tile of kTile samples (256 threads x 4 samples): unpack the
+// tile and the 8 samples before it into shared memory (packed bytes, one
+// 32-bit word per 4 samples and channel), then filter, pack, store and
+// combine 4 samples per thread.
+template <int FMT>
 __global__ void __launch_bounds__(kIngThreads) ingest_kernel(IngestArgs a)
 {
-    __shared__ char2 xs[kMaxRf][kTile + 8];
-    const int t0 = blockIdx.x * kTile;
-    const int nk = a.nrfch;
-    for (int idx = threadIdx.x; idx < kTile + 8; idx += kIngThreads) {
-        const int n = t0 - 8 + idx;
-        if (n >= a.N) continue;
-        for (int k = 0; k < nk; ++k)
-            xs[k][idx] = n < 0 ? a.hist_in[k * 8 + 8 + n] : unpack(a, k, n);
+    constexpr int NRF = nrf_of(FMT), BPS = bps_of(FMT), QW = (kTile + 8) / 4;
+    __shared__ uint32_t xs[NRF][QW];
+    __shared__ uint8_t lutc[(FMT >= F_RAW8 && FMT <= F_RAW32) ? NRF * 1024 : 4];
+    __shared__ int8_t lut8[(FMT == F_INT8 || FMT == F_INT8X2 || FMT == F_CS8) ? 256 : 4];
+    if constexpr (FMT >= F_RAW8 && FMT <= F_RAW32) {
+        for (int i = threadIdx.x; i < NRF * 256; i += kIngThreads)
+            ((uint32_t *)lutc)[i] = __ldg((const uint32_t *)a.lutc + i);
+    }
+    if constexpr (FMT == F_INT8 || FMT == F_INT8X2 || FMT == F_CS8) {
+        if (threadIdx.x < 64) ((uint32_t *)lut8)[threadIdx.x] = __ldg((const uint32_t *)a.lut8 + threadIdx.x);
     }
     __syncthreads();
-    for (int idx = threadIdx.x; idx < kTile; idx += kIngThreads) {
-        const int n = t0 + idx;
-        if (n >= a.N) continue;
-        int yi[kMaxRf], yq[kMaxRf];
+    const int t0 = blockIdx.x * kTile;
+    for (int qd = threadIdx.x; qd < QW; qd += kIngThreads) {
+        const int n0 = t0 - 8 + 4 * qd;             // first sample of the quad
+        uint32_t wq[NRF];
 #pragma unroll
-        for (int k = 0; k < kMaxRf; ++k) {
-            if (k >= nk) break;
-            const char2 *x = xs[k] + idx;      // x[0..8] = samples n-8 .. n
-            int I = x[8].x, Q = x[8].y;
+        for (int k = 0; k < NRF; ++k) wq[k] = 0u;
+        if (n0 < 0) {                               // before the block: history
+#pragma unroll
+            for (int k = 0; k < NRF; ++k)
+                wq[k] = *(const uint32_t *)(a.hist_in + k * 8 + 8 + n0);
+        } else if (n0 < a.N) {
+            uint32_t rw[BPS];
+            const bool full = n0 + 4 <= a.N;
+            if (full && a.vec) {
+                const uint8_t *src = a.raw + (size_t)n0 * BPS;
+                if constexpr (BPS == 1) rw[0] = __ldg((const uint32_t *)src);
+                else if constexpr (BPS == 2) { const uint2 v = __ldg((const uint2 *)src); rw[0] = v.x; rw[1] = v.y; }
+                else { const uint4 v = __ldg((const uint4 *)src); rw[0] = v.x; rw[1] = v.y; rw[2] = v.z; rw[3] = v.w; }
+            } else {
+#pragma unroll
+                for (int i = 0; i < BPS; ++i) rw[i] = 0u;
+                const int ns = full ? 4 : a.N - n0;
+                for (int i = 0; i < ns * BPS; ++i)
+                    rw[i >> 2] |= (uint32_t)a.raw[(size_t)n0 * BPS + i] << (8 * (i & 3));
+            }
+            const int ns = full ? 4 : a.N - n0;
+#pragma unroll
+            for (int sm = 0; sm < 4; ++sm) {
+                if (sm < ns) {
+                    const uint32_t b = sample_bytes<BPS>(rw, sm);
+                    const int ph = (a.ph0 + n0 + sm) & 3;
+#pragma unroll
+                    for (int k = 0; k < NRF; ++k)
+                        wq[k] |= unpack1<FMT>(b, k, ph, a, lutc, lut8) << (8 * sm);
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < NRF; ++k) xs[k][qd] = wq[k];
+    }
+    __syncthreads();
+
+    const int n0 = t0 + 4 * threadIdx.x;           // this thread's 4 outputs
+    if (n0 < a.N) {
+        const int ns = n0 + 4 <= a.N ? 4 : a.N - n0;
+        uint32_t yw[NRF];
+#pragma unroll
+        for (int k = 0; k < NRF; ++k) {
+            const uint32_t w2 = xs[k][threadIdx.x + 2];   // samples n0 .. n0+3
+            uint32_t y = w2;
             if ((a.lpf_mask >> k) & 1) {
-                const int *h = a.h[k];
-                int ai = h[4] * x[4].x, aq = h[4] * x[4].y;
+                const uint32_t w0 = xs[k][threadIdx.x], w1 = xs[k][threadIdx.x + 1];
+                int xi[12], xq[12];
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
-                    ai += h[j] * (x[j].x + x[8 - j].x);
-                    aq += h[j] * (x[j].y + x[8 - j].y);
+                    xi[j] = nib(w0, 8 * j); xq[j] = nib(w0, 8 * j + 4);
+                    xi[4 + j] = nib(w1, 8 * j); xq[4 + j] = nib(w1, 8 * j + 4);
+                    xi[8 + j] = nib(w2, 8 * j); xq[8 + j] = nib(w2, 8 * j + 4);
                 }
-                I = min(7, max(-7, (ai + (1 << 12)) >> 13));
-                Q = min(7, max(-7, (aq + (1 << 12)) >> 13));
+                const int *h = a.h[k];
+                y = 0u;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {       // output n0 + j: inputs n0+j-8 .. n0+j
+                    int ai = h[4] * xi[j + 4], aq = h[4] * xq[j + 4];
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) {
+                        ai += h[m] * (xi[j + m] + xi[j + 8 - m]);
+                        aq += h[m] * (xq[j + m] + xq[j + 8 - m]);
+                    }
+                    const int I = min(7, max(-7, (ai + (1 << 12)) >> 13));
+                    const int Q = min(7, max(-7, (aq + (1 << 12)) >> 13));
+                    y |= (uint32_t)pack8(I, Q) << (8 * j);
+                }
             }
-            yi[k] = I;
-            yq[k] = Q;
-            a.out[k][n] = pack8(I, Q);
+            yw[k] = y;
+            uint8_t *dst = a.out[k] + n0;
+            if (ns == 4 && a.vec) *(uint32_t *)dst = y;
+            else for (int j = 0; j < ns; ++j) dst[j] = (uint8_t)(y >> (8 * j));
         }
         for (int m = 0; m < a.narch; ++m) {
-            int I = 0, Q = 0;
-            for (int k = 0; k < nk; ++k) {
-                const short2 w = a.w[m][k];
-                I += yi[k] * w.x - yq[k] * w.y;
-                Q += yi[k] * w.y + yq[k] * w.x;
+            int I[4] = {0, 0, 0, 0}, Q[4] = {0, 0, 0, 0};
+#pragma unroll
+            for (int k = 0; k < NRF; ++k) {
+                if (!((a.amask[m] >> k) & 1)) continue;
+                const int wr = a.w[m][k].x, wi = a.w[m][k].y;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int xi = nib(yw[k], 8 * j), xq = nib(yw[k], 8 * j + 4);
+                    I[j] += xi * wr - xq * wi;
+                    Q[j] += xi * wi + xq * wr;
+                }
             }
-            I += I >= 0 ? 128 : -128;
-            Q += Q >= 0 ? 128 : -128;
-            I /= 256;
-            Q /= 256;
-            a.aout[m][n] = pack8(min(7, max(-8, I)), min(7, max(-8, Q)));
+            uint32_t o = 0u;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int ii = (I[j] + (I[j] >= 0 ? 128 : -128)) / 256;
+                const int qq = (Q[j] + (Q[j] >= 0 ? 128 : -128)) / 256;
+                o |= (uint32_t)pack8(min(7, max(-8, ii)), min(7, max(-8, qq))) << (8 * j);
+            }
+            uint8_t *dst = a.aout[m] + n0;
+            if (ns == 4 && a.vec) *(uint32_t *)dst = o;
+            else for (int j = 0; j < ns; ++j) dst[j] = (uint8_t)(o >> (8 * j));
         }
     }
     // the tile holding sample N-1 keeps the block's last 8 unfiltered samples
-    if (t0 <= a.N - 1 && a.N - 1 < t0 + kTile && threadIdx.x < 8 * nk) {
+    if (t0 <= a.N - 1 && a.N - 1 < t0 + kTile && threadIdx.x < 8 * NRF) {
         const int k = threadIdx.x / 8, j = threadIdx.x % 8;
-        a.hist_out[k * 8 + j] = xs[k][a.N - t0 + j];
+        const int p = a.N - t0 + j;                 // buffer position of sample N-8+j
+        a.hist_out[k * 8 + j] = (uint8_t)(xs[k][p >> 2] >> (8 * (p & 3)));
     }
 }
 
@@ -219,11 +312,22 @@ static int host_lpf_taps(double fc, double fs, int *h)
     return 1;
 }
 
-static int launch_ingest(IngestArgs &a, cudaStream_t st)
+static int launch_ingest(IngestArgs &a, int fmt, cudaStream_t st)
 {
     if (a.N <= 0) return SDRG_OK;
     const int grid = (a.N + kTile - 1) / kTile;
-    ingest_kernel<<<grid, kIngThreads, 0, st>>>(a);
+    switch (fmt) {
+    case F_CPX8: ingest_kernel<F_CPX8><<<grid, kIngThreads, 0, st>>>(a); break;
+    case F_INT8: ingest_kernel<F_INT8><<<grid, kIngThreads, 0, st>>>(a); break;
+    case F_INT8X2: ingest_kernel<F_INT8X2><<<grid, kIngThreads, 0, st>>>(a); break;
+    case F_RAW8: ingest_kernel<F_RAW8><<<grid, kIngThreads, 0, st>>>(a); break;
+    case F_RAW16: ingest_kernel<F_RAW16><<<grid, kIngThreads, 0, st>>>(a); break;
+    case F_RAW16I: ingest_kernel<F_RAW16I><<<grid, kIngThreads, 0, st>>>(a); break;
+    case F_RAW32: ingest_kernel<F_RAW32><<<grid, kIngThreads, 0, st>>>(a); break;
+    case F_CS8: ingest_kernel<F_CS8><<<grid, kIngThreads, 0, st>>>(a); break;
+    case F_CS16: ingest_kernel<F_CS16><<<grid, kIngThreads, 0, st>>>(a); break;
+    default: return set_error(SDRG_ERR_ARG, "ingest: bad format %d", fmt);
+    }
     SDRG_CUDA(cudaGetLastError());
     return SDRG_OK;
 }
@@ -239,14 +343,14 @@ struct sdrg_ingest {
     int h[kMaxRf][9] = {};
     int8_t *lut8_dev = nullptr;     // [2][65536]
     uint8_t *lutc_dev = nullptr;    // [8][1024]
-    char2 *hist_dev = nullptr;      // [2][8][8] double-buffered history
+    uint8_t *hist_dev = nullptr;    // [2][8][8] double-buffered history (packed samples)
     int parity = 0;
 };
 
 // sdr_lpf_t of the drop-in calls (opaque to callers, as in the reference)
 struct sdr_lpf_tag {
     int h[9];
-    char2 hist[8];     // last 8 unfiltered samples of the previous call
+    uint8_t hist[8];   // last 8 unfiltered (packed) samples of the previous call
 };
 
 extern "C" {
@@ -302,12 +406,12 @@ sdrg_ingest_t *sdrg_ingest_new(const sdrg_ingest_cfg_t *cfg)
         if (host_lpf_taps(cfg->lpf_fc[k], cfg->fs, g->h[k])) g->lpf_mask |= 1 << k;
     bool ok = cudaMalloc(&g->lut8_dev, lut8.size()) == cudaSuccess &&
               cudaMalloc(&g->lutc_dev, lutc.size()) == cudaSuccess &&
-              cudaMalloc(&g->hist_dev, 2 * kMaxRf * 8 * sizeof(char2)) == cudaSuccess &&
+              cudaMalloc(&g->hist_dev, 2 * kMaxRf * 8) == cudaSuccess &&
               cudaMemcpyAsync(g->lut8_dev, lut8.data(), lut8.size(), cudaMemcpyHostToDevice, st) ==
                   cudaSuccess &&
               cudaMemcpyAsync(g->lutc_dev, lutc.data(), lutc.size(), cudaMemcpyHostToDevice, st) ==
                   cudaSuccess &&
-              cudaMemsetAsync(g->hist_dev, 0, 2 * kMaxRf * 8 * sizeof(char2), st) == cudaSuccess &&
+              cudaMemsetAsync(g->hist_dev, 0, 2 * kMaxRf * 8, st) == cudaSuccess &&
               cudaStreamSynchronize(st) == cudaSuccess;
     if (!ok) {
         cuda_error(cudaGetLastError(), "sdrg_ingest_new");
@@ -336,9 +440,7 @@ int sdrg_ingest_run(sdrg_ingest_t *g, const uint8_t *raw_dev, int64_t ix, uint8_
     if ((e = ensure_device(&dev))) return e;
     IngestArgs a = {};
     a.raw = raw_dev;
-    a.fmt = g->cfg.fmt;
     a.N = g->cfg.N;
-    a.nrfch = g->nrfch;
     a.ph0 = (int)((ix * (int64_t)g->cfg.N) & 3);    // src/sdr_rcv.c:846
     a.rtoc_mask = g->rtoc_mask;
     a.lpf_mask = g->lpf_mask;
@@ -346,9 +448,13 @@ int sdrg_ingest_run(sdrg_ingest_t *g, const uint8_t *raw_dev, int64_t ix, uint8_
     a.lutc = g->lutc_dev;
     a.hist_in = g->hist_dev + g->parity * kMaxRf * 8;
     a.hist_out = g->hist_dev + (g->parity ^ 1) * kMaxRf * 8;
+    // vector loads / stores when the raw block is 16-byte and every output
+    // 4-byte aligned (else the same kernel moves bytes)
+    bool vec = ((uintptr_t)raw_dev & 15) == 0;
     for (int k = 0; k < g->nrfch; ++k) {
         if (!buf_dev[k]) return set_error(SDRG_ERR_ARG, "sdrg_ingest_run: no buffer %d", k);
         a.out[k] = buf_dev[k] + base;
+        vec = vec && ((uintptr_t)a.out[k] & 3) == 0;
         memcpy(a.h[k], g->h[k], sizeof(a.h[k]));
     }
     a.narch = 0;
@@ -357,11 +463,17 @@ int sdrg_ingest_run(sdrg_ingest_t *g, const uint8_t *raw_dev, int64_t ix, uint8_
         uint8_t *o = buf_dev[g->nrfch + m];
         if (!o) return set_error(SDRG_ERR_ARG, "sdrg_ingest_run: no buffer %d", g->nrfch + m);
         a.aout[a.narch] = o + base;
-        for (int k = 0; k < g->nrfch; ++k)
+        vec = vec && ((uintptr_t)a.aout[a.narch] & 3) == 0;
+        a.amask[a.narch] = 0;
+        for (int k = 0; k < g->nrfch; ++k) {
             a.w[a.narch][k] = make_short2(g->cfg.w[m][k][0], g->cfg.w[m][k][1]);
+            // zero weights add nothing to the sums: skip those channels
+            if (g->cfg.w[m][k][0] || g->cfg.w[m][k][1]) a.amask[a.narch] |= 1 << k;
+        }
         a.narch++;
     }
-    if ((e = launch_ingest(a, (cudaStream_t)stream))) return e;
+    a.vec = vec;
+    if ((e = launch_ingest(a, g->cfg.fmt, (cudaStream_t)stream))) return e;
     g->parity ^= 1;
     return SDRG_OK;
 }
@@ -392,18 +504,17 @@ void sdr_lpf_apply(sdr_lpf_t *lpf, sdr_cpx8_t *data, int N)
     c.host[0].pinned = true;
     const size_t nb = ((size_t)N + 255) / 256 * 256;
     if ((e = ensure_device(&dev)) || (e = thread_stream(&st)) || (e = c.host[0].reserve(2 * nb)) ||
-        (e = c.dev[0].reserve(2 * nb + 2 * kMaxRf * 8 * sizeof(char2))))
+        (e = c.dev[0].reserve(2 * nb + 2 * kMaxRf * 8)))
         return;   // error recorded; data left unfiltered
     uint8_t *h_in = (uint8_t *)c.host[0].ptr, *h_out = h_in + nb;
     uint8_t *d_in = (uint8_t *)c.dev[0].ptr, *d_out = d_in + nb;
-    char2 *d_hist = (char2 *)(d_in + 2 * nb);
+    uint8_t *d_hist = d_in + 2 * nb;
     memcpy(h_in, data, (size_t)N);
     IngestArgs a = {};
     a.raw = d_in;
-    a.fmt = F_CPX8;
     a.N = N;
-    a.nrfch = 1;
     a.lpf_mask = 1;
+    a.vec = 1;           // scratch slots are 256-byte aligned
     a.hist_in = d_hist;
     a.hist_out = d_hist + kMaxRf * 8;
     a.out[0] = d_out;
@@ -411,23 +522,17 @@ void sdr_lpf_apply(sdr_lpf_t *lpf, sdr_cpx8_t *data, int N)
     if (cudaMemcpyAsync(d_in, h_in, (size_t)N, cudaMemcpyHostToDevice, st) != cudaSuccess ||
         cudaMemcpyAsync(d_hist, lpf->hist, sizeof(lpf->hist), cudaMemcpyHostToDevice, st) !=
             cudaSuccess ||
-        launch_ingest(a, st) ||
+        launch_ingest(a, F_CPX8, st) ||
         cudaMemcpyAsync(h_out, d_out, (size_t)N, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess) {
         cuda_error(cudaGetLastError(), "sdr_lpf_apply");
         return;
     }
     // next history: the last 8 of (history, this call's unfiltered input)
-    char2 nh[8];
+    uint8_t nh[8];
     for (int j = 0; j < 8; ++j) {
         const int n = N - 8 + j;
-        if (n < 0) {
-            nh[j] = lpf->hist[8 + n];
-        } else {
-            const uint8_t b = h_in[n];
-            nh[j] = make_char2((signed char)((int8_t)(uint8_t)(b << 4) >> 4),
-                               (signed char)((int8_t)b >> 4));
-        }
+        nh[j] = n < 0 ? lpf->hist[8 + n] : h_in[n];
     }
     memcpy(lpf->hist, nh, sizeof(nh));
     memcpy(data, h_out, (size_t)N);
