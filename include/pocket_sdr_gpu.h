@@ -448,6 +448,38 @@ int sdrg_ingest_run(sdrg_ingest_t *ing, const uint8_t *raw_dev, int64_t ix,
  * (h untouched) when the cutoff is outside (0, fs/2). */
 int sdrg_lpf_taps(double fc, double fs, int *h);
 
+/* ---- QZSS L6 CSK tracking ---------------------------------------------------
+ * What a tracking L6D / L6E channel does per code period (src/sdr_ch.c:705-720):
+ * sdr_mix_carr of its window, sdr_corr_fft with the code bank of its
+ * fractional code phase, and the CSK decode (src/sdr_ch.c:636-664) giving the
+ * code-shift symbol and the correlator outputs around it - for every L6
+ * channel of an epoch in one call. The decode is bit-identical to the
+ * reference's CSK on the same correlation; the correlation itself is the FP32
+ * FFT correlator of sdr_corr_fft. */
+typedef struct {
+    int buf;                   /* IF buffer index */
+    int ix;                    /* first sample of the window (the reference's ix + i) */
+    int N;                     /* samples per code period */
+    double fs, fc, phi;        /* sdr_mix_carr arguments (phi at sample ix) */
+    const sdr_cpx_t *code_fft; /* DEVICE: conjugated code DFT of the bank (N values) */
+    int len_code;              /* code length incl. TDM zeros (sdr_ch_t.len_code) */
+    int n;                     /* correlator taps (<= SDR_MAX_CORR) */
+    const double *pos;         /* HOST: tap positions (samples) */
+} sdrg_l6_job_t;
+
+/* sym_dev[j]: symbol of job j; C_dev: [n_job][SDR_MAX_CORR] correlator
+ * outputs; corr_dev (may be NULL): [n_job][max N] the FFT correlations. All
+ * DEVICE pointers; asynchronous on `stream` (NULL = the legacy default
+ * stream); scratch is stream-ordered. */
+int sdrg_l6_csk_batch(const sdrg_l6_job_t *jobs, int n_job, const uint8_t *const *if_dev,
+    const int *len_if, uint8_t *sym_dev, sdr_cpx_t *C_dev, sdr_cpx_t *corr_dev,
+    void *stream);
+
+/* The CSK decode alone on n_job given correlations corr_dev [n_job][N] (DEVICE)
+ * with common code length and taps (pos: HOST); outputs as above. */
+int sdrg_csk_decode(const sdr_cpx_t *corr_dev, int n_job, int N, int len_code,
+    const double *pos, int npos, uint8_t *sym_dev, sdr_cpx_t *C_dev, void *stream);
+
 /* Host convenience: copies IF buffers to the device, runs, and copies the
  * n_prn-total results back (synchronous). if_host[b] are HOST pointers. */
 int sdrg_acq_run_host(sdrg_acq_plan_t *plan, const uint8_t *const *if_host,

@@ -78,6 +78,7 @@ class Restatement:
         L.orc_corr_fft.argtypes = [_p, _p, _i, _p]
         L.orc_corr_fft_cpx.argtypes = [_p, _i, _i, _i, _d, _d, _d, _p, _p]
         L.orc_psd_cpx.argtypes = [_p, _i, _i, _d, _i, _p]
+        L.orc_csk.argtypes = [_p, _i, _i, _p, _i, _p, _p]
         L.orc_search_code.argtypes = [_p, _p, _i, _i, _i, _d, _d, _p, _i, _p]
         L.orc_corr_max.argtypes = [_p, _i, _i, _i, _d, _p]
         L.orc_corr_max.restype = _f
@@ -152,6 +153,15 @@ class Restatement:
         out = np.zeros(N // 2 if IQ == 1 else N, np.float32)
         self.lib.orc_psd_cpx(_ptr(buff), len(buff), N, fs, IQ, _ptr(out))
         return out
+
+    def csk(self, corr, len_code, pos):
+        """L6 CSK decode: (symbol, taps complex64[len(pos)])."""
+        corr = np.ascontiguousarray(corr, np.complex64)
+        pos = np.ascontiguousarray(pos, np.float64)
+        sym = np.zeros(1, np.uint8)
+        C = np.zeros(len(pos), np.complex64)
+        self.lib.orc_csk(_ptr(corr), len(corr), len_code, _ptr(pos), len(pos), _ptr(sym), _ptr(C))
+        return int(sym[0]), C
 
     def search_code(self, code_fft, buff, ix, N, fs, fi, fds, P):
         code_fft = np.ascontiguousarray(code_fft, np.complex64)
@@ -519,6 +529,27 @@ class _LpfState:
         if getattr(self, "h", None):
             self.chk.f["lpf_free"](self.h)
             self.h = None
+
+
+CH_SO = os.path.join(HERE, "_ref", "libch_ref.so")
+
+
+class Channel:
+    """The reference channel's L6 CSK decoder (src/sdr_ch.c:636-664) through
+    ch_shim.c (_ref/libch_ref.so), same API as Restatement.csk."""
+    kind = "reference"
+
+    def __init__(self):
+        self.lib = C.CDLL(CH_SO)
+        self.lib.orr_csk.argtypes = [_p, _i, _i, _p, _i, _p, _p]
+
+    def csk(self, corr, len_code, pos):
+        corr = np.ascontiguousarray(corr, np.complex64)
+        pos = np.ascontiguousarray(pos, np.float64)
+        sym = np.zeros(1, np.uint8)
+        Cc = np.zeros(len(pos), np.complex64)
+        self.lib.orr_csk(_ptr(corr), len(corr), len_code, _ptr(pos), len(pos), _ptr(sym), _ptr(Cc))
+        return int(sym[0]), Cc
 
 
 def best():

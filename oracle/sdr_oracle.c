@@ -425,3 +425,40 @@ void orc_psd_cpx(const float *buff, int len_buff, int N, double fs, int IQ, floa
     }
     free(w); free(p); free(a); free(b);
 }
+
+/* src/sdr_ch.c:626-664 (interp_corr, CSK): the correlation, rotated so the
+ * zero lag sits at n = (int)(280 R) (R = N / (len_code / 2) samples per
+ * chip), linearly interpolated in double at n + i R for i = -255..255 (the
+ * reference build forms n + i R as one fused multiply-add); the
+ * first strict maximum of |c| (float) gives ix (0 when all are 0), the symbol
+ * (uint8)(255 - ix % 256) and the taps interpolated at n + ix R + pos[k]. */
+static void orc_interp(const float *C, double x, float *c)
+{
+    int i = (int)x;
+    double a1 = x - i, a0 = 1.0 - a1;
+    c[0] = (float)(a0 * C[2 * i] + a1 * C[2 * i + 2]);
+    c[1] = (float)(a0 * C[2 * i + 1] + a1 * C[2 * i + 3]);
+}
+
+void orc_csk(const float *corr, int N, int len_code, const double *pos, int npos, uint8_t *sym,
+             float *Cout)
+{
+    double R = (double)N / (len_code / 2);
+    int n = (int)(280 * R);
+    float *C = (float *)malloc(sizeof(float) * 4 * n);
+    memcpy(C, corr + 2 * (N - n), sizeof(float) * 2 * n);
+    memcpy(C + 2 * n, corr, sizeof(float) * 2 * n);
+    double P_max = 0.0;
+    int ix = 0;
+    for (int i = -255; i <= 255; i++) {
+        float c[2];
+        orc_interp(C, fma((double)i, R, (double)n), c);   /* gcc -mfma contracts n + i*R */
+        double P = sqrtf(c[0] * c[0] + c[1] * c[1]);
+        if (P <= P_max) continue;
+        P_max = P;
+        ix = i;
+    }
+    *sym = (uint8_t)(255 - ix % 256);
+    for (int k = 0; k < npos; k++) orc_interp(C, fma((double)ix, R, (double)n) + pos[k], Cout + 2 * k);
+    free(C);
+}

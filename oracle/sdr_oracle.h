@@ -112,6 +112,10 @@ void orc_refine_step(const double *sums, int K, int Nb, double fs, double rate_n
 /* Welch PSD of float IQ data (src/sdr_func.c:1141-1182). */
 void orc_psd_cpx(const float *buff, int len_buff, int N, double fs, int IQ, float *psd);
 
+/* L6 CSK decode of an N-point FFT correlation (src/sdr_ch.c:626-664). */
+void orc_csk(const float *corr, int N, int len_code, const double *pos, int npos, uint8_t *sym,
+             float *C);
+
 /* IF ingest (ingest_oracle.c): raw front-end blocks -> packed cpx8 buffers,
  * per-channel LPF and array combine, as src/sdr_rcv.c:773-936,
  * src/sdr_func.c:311-405 and src/sdr_array.c:487-578. */

@@ -60,6 +60,12 @@ class SrchRes(C.Structure):
                 ("coff", _d), ("n_sum", _i)]
 
 
+class L6Job(C.Structure):
+    """sdrg_l6_job_t."""
+    _fields_ = [("buf", _i), ("ix", _i), ("N", _i), ("fs", _d), ("fc", _d), ("phi", _d),
+                ("code_fft", _p), ("len_code", _i), ("n", _i), ("pos", C.POINTER(_d))]
+
+
 class RefineSig(C.Structure):
     """sdrg_refine_sig_t."""
     _fields_ = [("chips", _p), ("Lc", _i), ("rate", _d), ("fi", _d), ("fc", _d)]
@@ -107,6 +113,8 @@ SIGNATURES = {
     "sdrg_search_batch": ([C.POINTER(SrchSetup), _i, C.POINTER(SrchReq), _i, _p, _p, _i, _d, _d,
                            C.POINTER(SrchRes), _p], _i),
     "sdrg_srch_groups": ([C.POINTER(SrchSetup), _i, C.POINTER(SrchReq), _i, _d, _p, _p, _p], _i),
+    "sdrg_l6_csk_batch": ([C.POINTER(L6Job), _i, _p, _p, _p, _p, _p, _p], _i),
+    "sdrg_csk_decode": ([_p, _i, _i, _i, _p, _i, _p, _p, _p], _i),
     "sdrg_psd": ([_p, _i, _i, _d, _i, _p, _p], _i),
     "sdrg_psd_if": ([_p, _i, _i, _i, _i, _d, _i, _p, _p], _i),
     "sdrg_ingest_new": ([C.POINTER(IngestCfg)], _p),

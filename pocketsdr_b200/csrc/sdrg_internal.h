@@ -102,4 +102,14 @@ int code_fft_device(const int8_t *ci, const int8_t *cq, int len_code, int n_code
                     double coff, double fs, int N, int L, int natural, float2 *out,
                     cudaStream_t st);
 
+// One correlation job on device data (sdrg_search.cu): sdr_mix_carr of the
+// window [ix, ix + N) of circular buffer buf (len samples) at (fs, fc, phi)
+// followed by sdr_corr_fft with the natural-order conjugated code DFT
+// code_nat, into corr[N]. tab_dev holds the 5 words corr_job_tables fills;
+// scratch must hold corr_job_scratch(N) bytes. Asynchronous on st.
+void corr_job_tables(int len, int ix, int N, double fs, double fc, double phi, uint32_t *tab);
+size_t corr_job_scratch(int N);
+int corr_job_device(const uint8_t *buf, int len, const uint32_t *tab_dev, int N,
+                    const float2 *code_nat, float2 *corr, void *scratch, cudaStream_t st);
+
 } // namespace sdrg

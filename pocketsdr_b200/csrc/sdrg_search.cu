@@ -631,6 +631,57 @@ static int corr_fft_device(const char2 *iq_dev, const sdr_cpx_t *code_host, int 
 }
 
 // ---------------------------------------------------------------------------
+// one correlation job on device data: sdr_mix_carr(buf, ix, N, fs, fc, phi)
+// then sdr_corr_fft with a natural-order conjugated code DFT
+// ---------------------------------------------------------------------------
+void corr_job_tables(int len, int ix, int N, double fs, double fc, double phi, uint32_t *tab)
+{
+    // mixing phases as sdr_mix_carr (src/sdr_func.c:824-836): restart at the
+    // buffer wrap with phi + step * n
+    const double step = fc / fs;
+    const int n1 = (ix + N <= len) ? N : len - ix;
+    tab[0] = step_of(step);
+    tab[1] = phase_of(phi);
+    tab[2] = n1 < N ? phase_of(phi + step * n1) : 0;
+    tab[3] = (uint32_t)ix;
+    tab[4] = (uint32_t)n1;
+}
+
+size_t corr_job_scratch(int N)
+{
+    const FftPlan *pl = get_plan(N);
+    if (!pl) return 0;
+    const int wt = staged_chunk(pl, 1);
+    return (size_t)N * sizeof(float2) * (2 + (size_t)wt);
+}
+
+int corr_job_device(const uint8_t *buf, int len, const uint32_t *tab_dev, int N,
+                    const float2 *code_nat, float2 *corr, void *scratch, cudaStream_t st)
+{
+    const FftPlan *pl = get_plan(N);
+    if (!pl) return tctx().error ? tctx().error : SDRG_ERR_ARG;
+    Device *dev;
+    int e;
+    if ((e = ensure_device(&dev))) return e;
+    float2 *code_perm = (float2 *)scratch, *X = code_perm + N, *W = X + N;
+    if ((e = perm_code(pl, code_nat, 1, code_perm, st))) return e;
+    FwdArgs fa = {};
+    fa.pl = pl->k; fa.tw = pl->tw_dev; fa.ctab = dev->ctab_dev; fa.R = pl->R;
+    fa.n_bin = 1; fa.n_sum = 1; fa.cscale = kCScale;
+    fa.buf = buf; fa.buf_len = len;
+    fa.phstep = tab_dev; fa.ph0a = tab_dev + 1; fa.ph0b = tab_dev + 2;
+    fa.ix = (const int *)(tab_dev + 3); fa.nsplit = (const int *)(tab_dev + 4);
+    fa.X = X;
+    if ((e = launch_fwd<0>(pl, fa, pl->R, st))) return e;
+    ConsArgs ca = {};
+    ca.pl = pl->k; ca.tw = pl->tw_dev; ca.split = pl->split_dev; ca.X = X; ca.code = code_perm;
+    ca.n_prn = 1; ca.n_bin = 1; ca.n_sum = 1; ca.prn0 = 0;
+    ca.scale = 1.0f / N / N; ca.Nmax = N; ca.Y = corr;
+    const int wt = staged_chunk(pl, 1);
+    return launch_consumer<1>(pl, ca, 1, st, wt ? W : nullptr, wt);
+}
+
+// ---------------------------------------------------------------------------
 // batched plan
 // ---------------------------------------------------------------------------
 struct GroupState {

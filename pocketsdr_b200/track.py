@@ -72,3 +72,36 @@ def code_bank(code, T, fs, N, code_Q=None) -> np.ndarray:
     from .codes import res_code
     banks = [res_code(code, T, -k / fs / SDR_N_CODES, fs, N, 0, code_Q) for k in range(SDR_N_CODES)]
     return np.concatenate(banks)
+
+
+def l6_csk_batch(specs, if_ptrs, lens, stream: int = 0):
+    """QZSS L6 channels of one epoch (sdrg_l6_csk_batch): specs are dicts with
+    buf, ix, N, fs, fc, phi, code_fft (CUDA complex64 tensor: the bank's
+    conjugated code DFT), len_code, pos. Returns CUDA tensors (symbols uint8
+    [n], taps complex64 [n, SDR_MAX_CORR], correlations complex64 [n, max N])."""
+    import torch
+    from ._lib import L6Job
+    specs = list(specs)
+    arr = (L6Job * len(specs))()
+    keep = []
+    for j, s in zip(arr, specs):
+        pos = np.ascontiguousarray(s["pos"], np.float64)
+        keep += [pos, s["code_fft"]]
+        j.buf, j.ix, j.N = int(s["buf"]), int(s["ix"]), int(s["N"])
+        j.fs, j.fc, j.phi = float(s["fs"]), float(s["fc"]), float(s["phi"])
+        j.code_fft = C.c_void_p(s["code_fft"].data_ptr())
+        j.len_code, j.n = int(s["len_code"]), len(pos)
+        j.pos = pos.ctypes.data_as(C.POINTER(C.c_double))
+    n = len(specs)
+    nmax = max(int(s["N"]) for s in specs)
+    sym = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    taps = torch.zeros((n, SDR_MAX_CORR), dtype=torch.complex64, device="cuda")
+    corr = torch.zeros((n, nmax), dtype=torch.complex64, device="cuda")
+    ptrs = (C.c_void_p * len(if_ptrs))(*if_ptrs)
+    ls = (C.c_int * len(if_ptrs))(*lens)
+    st = stream or torch.cuda.current_stream().cuda_stream
+    if lib.sdrg_l6_csk_batch(arr, n, ptrs, ls, C.c_void_p(sym.data_ptr()),
+                             C.c_void_p(taps.data_ptr()), C.c_void_p(corr.data_ptr()),
+                             C.c_void_p(st)):
+        check("sdrg_l6_csk_batch")
+    return sym, taps, corr

@@ -249,3 +249,24 @@ def test_psd_restatement_vs_reference(orc):
         assert np.array_equal(np.isnan(a), np.isnan(b))
         ok = ~np.isnan(a)
         assert np.all(np.abs(a[ok] - b[ok]) <= 1e-4), (N, IQ)
+
+
+@pytest.mark.skipif(not os.path.exists(oracle.CH_SO), reason="reference channel build absent")
+def test_csk_restatement_vs_reference(orc):
+    """L6 CSK decode (src/sdr_ch.c:626-664): the restatement gives the
+    reference's symbol and bit-identical taps on random correlations with a
+    planted code-shift peak."""
+    R = oracle.Channel()
+    rng = np.random.default_rng(6)
+    for _ in range(300):
+        N = int(rng.choice([96000, 48000, 192000, 24000]))
+        Lc = 20460
+        corr = (rng.normal(size=N) + 1j * rng.normal(size=N)).astype(np.complex64)
+        sc = N / (Lc / 2)
+        corr[int(round(int(rng.integers(0, 256)) * sc)) % N] += np.complex64(40 + 30j)
+        pos = np.array([0.0, -0.5 * sc, 0.5 * sc, -120.0] + list(rng.uniform(-3 * sc, 3 * sc, 3)))
+        a, b = R.csk(corr, Lc, pos), orc.csk(corr, Lc, pos)
+        assert a[0] == b[0] and np.array_equal(a[1].view(np.uint32), b[1].view(np.uint32))
+    # no power anywhere: symbol of shift 0
+    z = np.zeros(24000, np.complex64)
+    assert R.csk(z, Lc, [0.0])[0] == orc.csk(z, Lc, [0.0])[0] == 255
