@@ -1038,10 +1038,13 @@ def run_l6(args):
                      len_code=Lc, pos=pos) for i, s in enumerate(sats)]
     epochs = [specs(e) for e in range(E)]
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    outs = [(torch.empty(len(sats), dtype=torch.uint8, device="cuda"),
+             torch.empty((len(sats), 107), dtype=torch.complex64, device="cuda"),
+             torch.empty((len(sats), N), dtype=torch.complex64, device="cuda")) for _ in range(E)]
 
     def step():
         for e in range(E):
-            track.l6_csk_batch(epochs[e], [d.data_ptr()], [len(buf)], st.cuda_stream)
+            track.l6_csk_batch(epochs[e], [d.data_ptr()], [len(buf)], st.cuda_stream, outs[e])
 
     for _ in range(args.warmup):
         step()

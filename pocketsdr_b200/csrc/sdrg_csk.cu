@@ -207,47 +207,93 @@ int sdrg_l6_csk_batch(const sdrg_l6_job_t *jobs, int n_job, const uint8_t *const
         scr = s > scr ? s : scr;
         Nmax = b.N > Nmax ? b.N : Nmax;
     }
-    // correlations: the caller's buffer ([n_job][Nmax]) or scratch
-    CskTables t;
-    t.ints.assign(3 * (size_t)n_job, 0);
-    t.pos.assign((size_t)n_job * SDR_MAX_CORR, 0.0);
-    std::vector<uint32_t> mix(5 * (size_t)n_job);
+    // one batch (one code permutation, one forward and one consumer launch for
+    // all jobs) when every job reads the same buffer with the same length and
+    // that length splits over one cluster; job by job otherwise
+    bool same = true;
+    for (int j = 1; j < n_job; ++j)
+        same = same && jobs[j].buf == jobs[0].buf && jobs[j].N == jobs[0].N;
+    const FftPlan *pl0 = get_plan(jobs[0].N);
+    const bool batched = same && pl0 && pl0->R <= 8;
+
+    // staging: mixing words (5 per job; transposed for the batch) | CSK ints
+    // (3 per job) | tap positions (SDR_MAX_CORR doubles per job), one upload
+    const size_t mb = 5 * (size_t)n_job * sizeof(uint32_t), ib = 3 * (size_t)n_job * sizeof(int);
+    const size_t pb = (size_t)n_job * SDR_MAX_CORR * sizeof(double);
+    const size_t o_i = (mb + 15) / 16 * 16, o_p = (o_i + ib + 15) / 16 * 16;
+    const size_t tab_bytes = (o_p + pb + 255) / 256 * 256;
+    const size_t cb = corr_dev ? 0 : ((size_t)n_job * Nmax * sizeof(float2) + 255) / 256 * 256;
+    const size_t wb = batched ? 3 * (size_t)n_job * Nmax * sizeof(float2) : scr;
+    const size_t dev_bytes = tab_bytes + cb + wb + 256;
+    ThreadCtx &c = tctx();
+    if (!c.l6_ev) {
+        SDRG_CUDA(cudaEventCreateWithFlags(&c.l6_ev, cudaEventDisableTiming));
+        SDRG_CUDA(cudaEventCreateWithFlags(&c.l6_done, cudaEventDisableTiming));
+    }
+    // the previous call's upload from the staging has landed, and this call's
+    // device work follows the previous call's (both use this thread's scratch)
+    SDRG_CUDA(cudaEventSynchronize(c.l6_ev));
+    SDRG_CUDA(cudaStreamWaitEvent(st, c.l6_done, 0));
+    c.l6_host.pinned = true;
+    if (dev_bytes > c.l6_dev.size) SDRG_CUDA(cudaStreamSynchronize(st));
+    if ((e = c.l6_host.reserve(tab_bytes)) || (e = c.l6_dev.reserve(dev_bytes))) return e;
+    char *hb = (char *)c.l6_host.ptr;
+    uint32_t *mix = (uint32_t *)hb;
+    int *ints = (int *)(hb + o_i);
+    double *posh = (double *)(hb + o_p);
+    memset(posh, 0, pb);
     for (int j = 0; j < n_job; ++j) {
         const sdrg_l6_job_t &b = jobs[j];
-        t.ints[j] = b.N;
-        t.ints[n_job + j] = b.len_code;
-        t.ints[2 * n_job + j] = b.n;
-        for (int k = 0; k < b.n; ++k) t.pos[(size_t)j * SDR_MAX_CORR + k] = b.pos[k];
-        corr_job_tables(len_if[b.buf], b.ix, b.N, b.fs, b.fc, b.phi, mix.data() + 5 * j);
+        ints[j] = b.N;
+        ints[n_job + j] = b.len_code;
+        ints[2 * n_job + j] = b.n;
+        for (int k = 0; k < b.n; ++k) posh[(size_t)j * SDR_MAX_CORR + k] = b.pos[k];
+        uint32_t w[5];
+        corr_job_tables(len_if[b.buf], b.ix, b.N, b.fs, b.fc, b.phi, w);
+        for (int k = 0; k < 5; ++k) {
+            if (batched) mix[(size_t)k * n_job + j] = w[k];
+            else mix[5 * (size_t)j + k] = w[k];
+        }
     }
-    float2 *corr = (float2 *)corr_dev;
-    char *work = nullptr;
-    const size_t cb = corr ? 0 : (size_t)n_job * Nmax * sizeof(float2);
-    const size_t mb = mix.size() * sizeof(uint32_t);
-    if (cudaMallocAsync((void **)&work, cb + mb + scr + 512, st) != cudaSuccess)
-        return cuda_error(cudaGetLastError(), "sdrg_l6_csk_batch scratch");
-    if (!corr) corr = (float2 *)work;
-    uint32_t *mix_d = (uint32_t *)(work + (cb + 255) / 256 * 256);
-    void *scratch = (char *)mix_d + (mb + 255) / 256 * 256;
+    char *db = (char *)c.l6_dev.ptr;
+    SDRG_CUDA(cudaMemcpyAsync(db, hb, o_p + pb, cudaMemcpyHostToDevice, st));
+    SDRG_CUDA(cudaEventRecord(c.l6_ev, st));
+    const uint32_t *mix_d = (const uint32_t *)db;
+    float2 *corr = corr_dev ? (float2 *)corr_dev : (float2 *)(db + tab_bytes);
+    char *work = db + tab_bytes + cb;
     e = SDRG_OK;
-    if (cudaMemcpyAsync(mix_d, mix.data(), mb, cudaMemcpyHostToDevice, st) != cudaSuccess)
-        e = cuda_error(cudaGetLastError(), "sdrg_l6_csk_batch tables");
-    // each job: mixing + FFT correlation (src/sdr_ch.c:710-713)
-    for (int j = 0; j < n_job && !e; ++j) {
-        const sdrg_l6_job_t &b = jobs[j];
-        e = corr_job_device(if_dev[b.buf], len_if[b.buf], mix_d + 5 * j, b.N,
-                            (const float2 *)b.code_fft, corr + (size_t)j * Nmax, scratch, st);
+    if (batched) {
+        float2 *codes = (float2 *)work;       // the jobs' code DFTs back to back
+        for (int j = 0; j < n_job && !e; ++j)
+            if (cudaMemcpyAsync(codes + (size_t)j * Nmax, jobs[j].code_fft,
+                                (size_t)Nmax * sizeof(float2), cudaMemcpyDeviceToDevice,
+                                st) != cudaSuccess)
+                e = cuda_error(cudaGetLastError(), "sdrg_l6_csk_batch codes");
+        if (!e)
+            e = corr_jobs_device(if_dev[jobs[0].buf], len_if[jobs[0].buf], mix_d, n_job, Nmax,
+                                 codes, corr, codes + (size_t)n_job * Nmax, st);
+    } else {
+        // each job: mixing + FFT correlation (src/sdr_ch.c:710-713)
+        for (int j = 0; j < n_job && !e; ++j) {
+            const sdrg_l6_job_t &b = jobs[j];
+            e = corr_job_device(if_dev[b.buf], len_if[b.buf], mix_d + 5 * j, b.N,
+                                (const float2 *)b.code_fft, corr + (size_t)j * Nmax, work, st);
+        }
     }
-    CskArgs a = {};
-    a.corr = corr;
-    a.stride = (size_t)Nmax;
-    a.sym = sym_dev;
-    a.C = (float2 *)C_dev;
-    void *td = nullptr;
-    if (!e) e = csk_upload(t, n_job, &td, st, a);
-    if (!e) e = launch_csk(a, n_job, st);
-    if (td) cudaFreeAsync(td, st);
-    cudaFreeAsync(work, st);
+    if (!e) {
+        CskArgs a = {};
+        a.corr = corr;
+        a.stride = (size_t)Nmax;
+        a.N = (const int *)(db + o_i);
+        a.len_code = a.N + n_job;
+        a.npos = a.N + 2 * n_job;
+        a.pos = (const double *)(db + o_p);
+        a.sym = sym_dev;
+        a.C = (float2 *)C_dev;
+        e = launch_csk(a, n_job, st);
+    }
+    cudaError_t re = cudaEventRecord(c.l6_done, st);
+    if (!e && re != cudaSuccess) e = cuda_error(re, "sdrg_l6_csk_batch");
     return e;
 }
 

@@ -53,6 +53,9 @@ struct ThreadCtx {
     // the last upload from cb_host
     Scratch cb_dev, cb_host;
     cudaEvent_t cb_ev = nullptr, cb_done = nullptr;
+    // batched L6 CSK tracking (asynchronous): the same scheme
+    Scratch l6_dev, l6_host;
+    cudaEvent_t l6_ev = nullptr, l6_done = nullptr;
     int error = 0;
     std::string msg;
 };
@@ -111,5 +114,12 @@ void corr_job_tables(int len, int ix, int N, double fs, double fc, double phi, u
 size_t corr_job_scratch(int N);
 int corr_job_device(const uint8_t *buf, int len, const uint32_t *tab_dev, int N,
                     const float2 *code_nat, float2 *corr, void *scratch, cudaStream_t st);
+
+// n such jobs of one length N on one buffer, batched (cluster splits only):
+// tab_dev = phstep[n] | ph0a[n] | ph0b[n] | ix[n] | nsplit[n] (the words of
+// corr_job_tables, transposed), code_nat and corr [n][N], scratch 2 n N
+// complex values.
+int corr_jobs_device(const uint8_t *buf, int len, const uint32_t *tab_dev, int n, int N,
+                     const float2 *code_nat, float2 *corr, void *scratch, cudaStream_t st);
 
 } // namespace sdrg

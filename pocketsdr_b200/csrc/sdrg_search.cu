@@ -66,6 +66,7 @@ struct FwdArgs {
     // mode 1: already mixed samples (sdr_cpx16_t), one block
     const char2 *iq;
     float2 *X;             // out: [n_bin][n_sum][R][M]
+    int ix_per_bin;        // 1: ix / nsplit indexed by bin (independent windows per bin)
 };
 
 struct LoadIF {
@@ -117,7 +118,8 @@ __global__ void __launch_bounds__(512, 1) fwd_kernel(FwdArgs a)
     __syncthreads();
 
     if (MODE == 0) {
-        LoadIF ld{a.buf, a.buf_len, a.ix[s], a.nsplit[s], a.R, r, a.phstep[b],
+        const int w = a.ix_per_bin ? b : s;
+        LoadIF ld{a.buf, a.buf_len, a.ix[w], a.nsplit[w], a.R, r, a.phstep[b],
                   a.ph0a[b], a.ph0b[bs], ctab, a.cscale};
         fft_forward(sm, tw, a.pl, ld);
     } else {
@@ -152,6 +154,7 @@ struct ConsArgs {
     size_t prn_stride;      // P stride between PRNs (elements)
     size_t bin_stride;      // P stride between bins (elements)
     int accumulate;         // 1: P += |y|^2 from the first sum on (IN/OUT P)
+    int code_per_bin;       // 1: bin b correlates with code b (independent jobs)
     float *P;               // mode 0
     float2 *Y;              // mode 1: [n_bin][L]
 };
@@ -214,7 +217,7 @@ __global__ void __launch_bounds__(512, 1) cons_kernel(ConsArgs a)
     }
     const int Mc = (M + R - 1) / R;
     const int q0 = c * Mc, q1 = min(M, q0 + Mc);
-    const float2 *code = a.code + (size_t)prn * R * M;
+    const float2 *code = a.code + (size_t)(a.code_per_bin ? b : prn) * R * M;
 
     for (int s = 0; s < a.n_sum; ++s) {
         // all CTAs of the cluster are done with their shared memory
@@ -679,6 +682,36 @@ int corr_job_device(const uint8_t *buf, int len, const uint32_t *tab_dev, int N,
     ca.scale = 1.0f / N / N; ca.Nmax = N; ca.Y = corr;
     const int wt = staged_chunk(pl, 1);
     return launch_consumer<1>(pl, ca, 1, st, wt ? W : nullptr, wt);
+}
+
+// n jobs of the same length N on one buffer in one launch each (splits of a
+// thread-block cluster, R <= 8): tab_dev = phstep[n] | ph0a[n] | ph0b[n] |
+// ix[n] | nsplit[n]; code_nat [n][N]; corr [n][N]; scratch 2 n N complex.
+int corr_jobs_device(const uint8_t *buf, int len, const uint32_t *tab_dev, int n, int N,
+                     const float2 *code_nat, float2 *corr, void *scratch, cudaStream_t st)
+{
+    const FftPlan *pl = get_plan(N);
+    if (!pl) return tctx().error ? tctx().error : SDRG_ERR_ARG;
+    if (pl->R > 8) return set_error(SDRG_ERR_ARG, "batched jobs need a cluster split (N=%d)", N);
+    Device *dev;
+    int e;
+    if ((e = ensure_device(&dev))) return e;
+    float2 *code_perm = (float2 *)scratch, *X = code_perm + (size_t)n * N;
+    if ((e = perm_code(pl, code_nat, n, code_perm, st))) return e;
+    FwdArgs fa = {};
+    fa.pl = pl->k; fa.tw = pl->tw_dev; fa.ctab = dev->ctab_dev; fa.R = pl->R;
+    fa.n_bin = n; fa.n_sum = 1; fa.cscale = kCScale;
+    fa.buf = buf; fa.buf_len = len;
+    fa.phstep = tab_dev; fa.ph0a = tab_dev + n; fa.ph0b = tab_dev + 2 * n;
+    fa.ix = (const int *)(tab_dev + 3 * n); fa.nsplit = (const int *)(tab_dev + 4 * n);
+    fa.ix_per_bin = 1;
+    fa.X = X;
+    if ((e = launch_fwd<0>(pl, fa, n * pl->R, st))) return e;
+    ConsArgs ca = {};
+    ca.pl = pl->k; ca.tw = pl->tw_dev; ca.split = pl->split_dev; ca.X = X; ca.code = code_perm;
+    ca.n_prn = 1; ca.n_bin = n; ca.n_sum = 1; ca.prn0 = 0; ca.code_per_bin = 1;
+    ca.scale = 1.0f / N / N; ca.Nmax = N; ca.Y = corr;
+    return launch_cons<1>(pl, ca, n, st);
 }
 
 // ---------------------------------------------------------------------------

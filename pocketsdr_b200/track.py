@@ -74,11 +74,12 @@ def code_bank(code, T, fs, N, code_Q=None) -> np.ndarray:
     return np.concatenate(banks)
 
 
-def l6_csk_batch(specs, if_ptrs, lens, stream: int = 0):
+def l6_csk_batch(specs, if_ptrs, lens, stream: int = 0, out=None):
     """QZSS L6 channels of one epoch (sdrg_l6_csk_batch): specs are dicts with
     buf, ix, N, fs, fc, phi, code_fft (CUDA complex64 tensor: the bank's
     conjugated code DFT), len_code, pos. Returns CUDA tensors (symbols uint8
-    [n], taps complex64 [n, SDR_MAX_CORR], correlations complex64 [n, max N])."""
+    [n], taps complex64 [n, SDR_MAX_CORR], correlations complex64 [n, max N]),
+    written into `out` (the same three tensors) when given; asynchronous."""
     import torch
     from ._lib import L6Job
     specs = list(specs)
@@ -94,9 +95,11 @@ def l6_csk_batch(specs, if_ptrs, lens, stream: int = 0):
         j.pos = pos.ctypes.data_as(C.POINTER(C.c_double))
     n = len(specs)
     nmax = max(int(s["N"]) for s in specs)
-    sym = torch.zeros(n, dtype=torch.uint8, device="cuda")
-    taps = torch.zeros((n, SDR_MAX_CORR), dtype=torch.complex64, device="cuda")
-    corr = torch.zeros((n, nmax), dtype=torch.complex64, device="cuda")
+    if out is None:
+        out = (torch.empty(n, dtype=torch.uint8, device="cuda"),
+               torch.empty((n, SDR_MAX_CORR), dtype=torch.complex64, device="cuda"),
+               torch.empty((n, nmax), dtype=torch.complex64, device="cuda"))
+    sym, taps, corr = out
     ptrs = (C.c_void_p * len(if_ptrs))(*if_ptrs)
     ls = (C.c_int * len(if_ptrs))(*lens)
     st = stream or torch.cuda.current_stream().cuda_stream

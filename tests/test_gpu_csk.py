@@ -102,3 +102,28 @@ def test_l6_batch_matches_reference_chain(ref, ch, gpu):
         assert np.abs(corr[j, :jb["N"]] - wcorr).max() <= TOL * scale, j
         assert int(sym[j]) == wsym, (j, int(sym[j]), wsym)
         assert np.abs(taps[j, :len(jb["pos"])] - wC).max() <= TOL * np.abs(wC).max(), j
+
+
+def test_l6_batch_mixed_lengths_job_by_job(ref, ch, gpu):
+    """Jobs of different lengths take the job-by-job path: same results."""
+    torch = pytest.importorskip("torch")
+    from pocketsdr_b200 import codes, track
+    buf, jobs = _l6_setup(ref, seed=11)
+    fs, T2 = jobs[0]["fs"], 2e-3                      # a half-period window of 48 000
+    N2 = int(fs * T2)
+    chips = codes.gen_code("L6D", 196)
+    # P, E, L only: at this length the noise tap (-120 samples) would fall
+    # before the +-280-chip window, which the library rejects
+    extra = dict(jobs[1], N=N2, ix=12345, code_fft=ref.gen_code_fft(chips, None, T2, 0.0, fs, N2, 0),
+                 pos=jobs[1]["pos"][:3])
+    alljobs = jobs[:2] + [extra]
+    specs = [dict(jb, code_fft=torch.from_numpy(jb["code_fft"]).cuda()) for jb in alljobs]
+    d = torch.from_numpy(buf).cuda()
+    sym, taps, corr = track.l6_csk_batch(specs, [d.data_ptr()], [len(buf)])
+    torch.cuda.synchronize()
+    sym, taps, corr = sym.cpu().numpy(), taps.cpu().numpy(), corr.cpu().numpy()
+    for j, jb in enumerate(alljobs):
+        wcorr, wsym, wC = _reference_chain(ref, ch, buf, jb)
+        assert np.abs(corr[j, :jb["N"]] - wcorr).max() <= TOL * np.abs(wcorr).max(), j
+        assert int(sym[j]) == wsym, j
+        assert np.abs(taps[j, :len(jb["pos"])] - wC).max() <= TOL * np.abs(wC).max(), j
