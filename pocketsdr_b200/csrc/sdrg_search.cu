@@ -726,6 +726,7 @@ struct GroupState {
     float2 *X = nullptr;                // [n_bin][n_sum][R][M]
     float *P = nullptr;                 // [n_prn][n_bin][Nmax]
     float2 *W = nullptr;                // staged splits: [w_tasks][R][M] sub-spectra
+    void *peak_parts = nullptr;         // partial peak reductions
     int w_tasks = 0;
     uint32_t *tab_dev = nullptr;        // phstep | ph0a | ph0b | (int) ix | nsplit
     uint32_t *tab_host = nullptr;       // pinned mirror
@@ -748,7 +749,7 @@ struct sdrg_acq_plan {
     cudaEvent_t ev_fork = nullptr;
     std::vector<cudaEvent_t> ev_join;
     // kernel timing (sdrg_acq_profile): event pairs recorded around launches
-    struct Rec { int kind, run; cudaEvent_t a, b; };
+    struct Rec { int kind, run; cudaEvent_t a, b; int n; };   // n: kernel launches inside
     bool prof = false;
     int run = 0;
     std::vector<cudaEvent_t> ev_pool;
@@ -760,7 +761,8 @@ namespace sdrg {
 // device reduction for (group, PRN) peaks, defined in sdrg_peak.cu
 int launch_peaks(const float *P, int n_prn, int M_rows, int Nmax, size_t row_stride,
                  size_t prn_stride, double T, const float *fds_dev,
-                 sdrg_acq_result_t *res, cudaStream_t st);
+                 sdrg_acq_result_t *res, void *scratch, cudaStream_t st);
+size_t peak_scratch_bytes(int n_prn);
 
 static int group_tables(GroupState &G, const int *len_if, const int *ix)
 {
@@ -804,11 +806,12 @@ static int prof_begin(sdrg_acq_plan *plan, cudaStream_t st, cudaEvent_t *ev)
     return SDRG_OK;
 }
 
-static int prof_end(sdrg_acq_plan *plan, cudaStream_t st, cudaEvent_t *ev, int kind)
+static int prof_end(sdrg_acq_plan *plan, cudaStream_t st, cudaEvent_t *ev, int kind,
+                    int n_launch = 1)
 {
     if (!plan->prof) return SDRG_OK;
     SDRG_CUDA(cudaEventRecord(ev[1], st));
-    plan->ev_used.push_back({kind, plan->run, ev[0], ev[1]});
+    plan->ev_used.push_back({kind, plan->run, ev[0], ev[1], n_launch});
     return SDRG_OK;
 }
 
@@ -851,7 +854,7 @@ int sdrg_acq_profile_get(sdrg_acq_plan_t *plan, double *ms, int64_t *launches)
         float t = 0.0f, t0 = 0.0f, t1 = 0.0f;
         SDRG_CUDA(cudaEventElapsedTime(&t, u.a, u.b));
         ms[u.kind] += t;
-        launches[u.kind] += 1;
+        launches[u.kind] += u.n;
         if (!ref) continue;
         SDRG_CUDA(cudaEventElapsedTime(&t0, ref, u.a));
         SDRG_CUDA(cudaEventElapsedTime(&t1, ref, u.b));
@@ -1044,6 +1047,7 @@ sdrg_acq_plan_t *sdrg_acq_plan_new(const sdrg_acq_sig_t *sigs, int n_sig)
         G.w_tasks = staged_chunk(G.pl, s.n_prn * s.len_fds);
         ok = ok && (!G.w_tasks ||
                     cudaMalloc(&G.W, (size_t)G.w_tasks * L * sizeof(float2)) == cudaSuccess);
+        ok = ok && cudaMalloc(&G.peak_parts, peak_scratch_bytes(s.n_prn)) == cudaSuccess;
         G.tab_words = 2 * (size_t)s.len_fds + (size_t)s.len_fds * s.n_sum + 2 * (size_t)s.n_sum + s.len_fds;
         ok = ok && cudaMalloc(&G.tab_dev, G.tab_words * 4) == cudaSuccess &&
              cudaMallocHost(&G.tab_host, G.tab_words * 4) == cudaSuccess &&
@@ -1101,6 +1105,7 @@ void sdrg_acq_plan_free(sdrg_acq_plan_t *plan)
         if (G.X) cudaFree(G.X);
         if (G.P) cudaFree(G.P);
         if (G.W) cudaFree(G.W);
+        if (G.peak_parts) cudaFree(G.peak_parts);
         if (G.tab_dev) cudaFree(G.tab_dev);
         if (G.tab_host) cudaFreeHost(G.tab_host);
         if (G.tab_ev) cudaEventDestroy(G.tab_ev);
@@ -1206,13 +1211,16 @@ int sdrg_acq_run(sdrg_acq_plan_t *plan, const uint8_t *const *if_dev, const int 
         ca.accumulate = 0; ca.P = G.P;
         if ((e = prof_begin(plan, st, ev))) return e;
         if ((e = launch_consumer<0>(G.pl, ca, s.n_prn * nb, st, G.W, G.w_tasks))) return e;
-        if ((e = prof_end(plan, st, ev, 3 * (int)gi + 1))) return e;
+        // a staged split launches a combine and an inverse pass per chunk and sum
+        const int n_cons = G.pl->R <= 8 ? 1
+            : 2 * ns * ((s.n_prn * nb + G.w_tasks - 1) / G.w_tasks);
+        if ((e = prof_end(plan, st, ev, 3 * (int)gi + 1, n_cons))) return e;
         const float *fd_dev = (const float *)(G.tab_dev + G.tab_words - nb);
         if ((e = prof_begin(plan, st, ev))) return e;
         if ((e = launch_peaks(G.P, s.n_prn, nb, s.Nmax, s.Nmax, (size_t)nb * s.Nmax, s.T,
-                              fd_dev, res_dev + G.res_off, st)))
+                              fd_dev, res_dev + G.res_off, G.peak_parts, st)))
             return e;
-        if ((e = prof_end(plan, st, ev, 3 * (int)gi + 2))) return e;
+        if ((e = prof_end(plan, st, ev, 3 * (int)gi + 2, 2))) return e;
     }
     // join: the caller's stream continues after every group
     for (size_t i = 0; i < plan->streams.size(); ++i) {
