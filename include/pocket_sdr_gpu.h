@@ -186,6 +186,13 @@ int sdrg_fft_supported(int N);
 /* Library version string. */
 const char *sdrg_version(void);
 
+/* Error-path testing: the after-th following device or pinned allocation
+ * attempt of the library (0: the next one) fails as an out-of-memory
+ * cudaMalloc would (SDRG_ERR_NOMEM); -1 cancels. SDRG_FAIL_ALLOC=n in the
+ * environment sets it once at start-up. Nothing is allocated or faulted on
+ * the device. */
+void sdrg_inject_alloc_failure(int after);
+
 /* ---- FFT correlator that allocates nothing --------------------------------
  * No counterpart in the reference (an addition of this library).
  * Same result as sdr_corr_fft (corr = IFFT(FFT(IQ * CSCALE) * code_fft / N^2))

@@ -41,6 +41,27 @@ int cuda_error(cudaError_t e, const char *what)
                      "%s: %s", what, cudaGetErrorString(e));
 }
 
+// ---- simulated allocation failures ---------------------------------------------
+// Error paths are tested without touching the device allocator's real limits:
+// sdrg_inject_alloc_failure(n) (or SDRG_FAIL_ALLOC=n in the environment, read
+// once) makes the n-th following device or pinned allocation attempt of the
+// library fail as cudaMalloc would with cudaErrorMemoryAllocation.
+static std::mutex g_fail_mtx;
+static long g_fail_after = -2;   // -2: environment not read yet, -1: off
+
+int alloc_fault(const char *what)
+{
+    std::lock_guard<std::mutex> lk(g_fail_mtx);
+    if (g_fail_after == -2) {
+        const char *e = getenv("SDRG_FAIL_ALLOC");
+        g_fail_after = e ? atol(e) : -1;
+    }
+    if (g_fail_after < 0) return SDRG_OK;
+    if (g_fail_after-- > 0) return SDRG_OK;
+    g_fail_after = -1;
+    return set_error(SDRG_ERR_NOMEM, "%s: simulated allocation failure", what);
+}
+
 // ---- device ------------------------------------------------------------------
 static std::mutex g_dev_mtx;
 static Device g_dev;
@@ -123,6 +144,8 @@ int Scratch::reserve(size_t bytes)
         ptr = nullptr;
         size = 0;
     }
+    int fe;
+    if ((fe = alloc_fault(pinned ? "cudaMallocHost" : "cudaMalloc"))) return fe;
     cudaError_t e = pinned ? cudaMallocHost(&ptr, want) : cudaMalloc(&ptr, want);
     if (e != cudaSuccess) {
         ptr = nullptr;
@@ -343,6 +366,12 @@ int sdrg_fft_supported(int N)
 }
 
 const char *sdrg_version(void) { return "pocketsdr_b200 0.1 (sm_100a)"; }
+
+void sdrg_inject_alloc_failure(int after)
+{
+    std::lock_guard<std::mutex> lk(g_fail_mtx);
+    g_fail_after = after < 0 ? -1 : after;
+}
 
 // When the reference's sdr_func.o is linked with its hot symbols renamed to
 // *_cpu (the integration recipe), its initialiser still sets up the log

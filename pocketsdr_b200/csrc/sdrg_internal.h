@@ -18,6 +18,9 @@ extern const float kCScale;
 
 // ---- error state (per host thread) ----------------------------------------
 int set_error(int code, const char *fmt, ...);
+// SDRG_OK, or SDRG_ERR_NOMEM (error set) when a simulated allocation failure
+// is due (sdrg_inject_alloc_failure); called before each library allocation.
+int alloc_fault(const char *what);
 int cuda_error(cudaError_t e, const char *what);
 #define SDRG_CUDA(call)                                            \
     do {                                                           \

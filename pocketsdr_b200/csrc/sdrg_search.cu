@@ -1040,6 +1040,10 @@ sdrg_acq_plan_t *sdrg_acq_plan_new(const sdrg_acq_sig_t *sigs, int n_sig)
         for (int b = 0; b < s.len_fds; ++b) G.phstep[b] = step_of((s.fi + (double)G.fds[b]) / s.fs);
         const size_t L = (size_t)s.L;
         float2 *nat = nullptr;
+        if (alloc_fault("sdrg_acq_plan_new")) {
+            sdrg_acq_plan_free(plan);
+            return nullptr;
+        }
         bool ok = cudaMalloc(&G.code, (size_t)s.n_prn * L * sizeof(float2)) == cudaSuccess &&
                   cudaMalloc(&nat, (size_t)s.n_prn * L * sizeof(float2)) == cudaSuccess &&
                   cudaMalloc(&G.X, (size_t)s.len_fds * s.n_sum * L * sizeof(float2)) == cudaSuccess &&
