@@ -193,6 +193,23 @@ const char *sdrg_version(void);
  * the device. */
 void sdrg_inject_alloc_failure(int after);
 
+/* ---- FFT schedules --------------------------------------------------------
+ * The reference keeps FFTW planning wisdom in a file (sdr_func_init(file),
+ * src/sdr_func.c:118-121). Here a transform length's schedule - how it is
+ * split over CTAs (R) and the CTA size - can be chosen by timing the
+ * candidates on the device (sdrg_fft_autotune) and kept in a schedule file;
+ * sdr_func_init(file) loads that file when it exists (lines
+ * "sdrg_fft <L> <R> <threads> <ms>"; anything else in the file is ignored).
+ * Plans built after a schedule is set use it; without one the library's
+ * default rule applies (smallest split that fits one CTA). R = 0 in
+ * sdrg_fft_schedule_set removes a schedule. Results do not depend on the
+ * schedule beyond FP32 rounding. */
+int sdrg_fft_autotune(int L, int *R, int *threads, double *ms);
+int sdrg_fft_schedule_set(int L, int R, int threads);
+int sdrg_fft_schedule_get(int L, int *R, int *threads);   /* 1: set, 0: none */
+int sdrg_fft_schedule_save(const char *path);
+int sdrg_fft_schedule_load(const char *path);             /* entries loaded, or < 0 */
+
 /* ---- FFT correlator that allocates nothing --------------------------------
  * No counterpart in the reference (an addition of this library).
  * Same result as sdr_corr_fft (corr = IFFT(FFT(IQ * CSCALE) * code_fft / N^2))

@@ -97,6 +97,11 @@ SIGNATURES = {
     "sdrg_fft_supported": ([_i], _i),
     "sdrg_version": ([], C.c_char_p),
     "sdrg_inject_alloc_failure": ([_i], None),
+    "sdrg_fft_autotune": ([_i, _p, _p, _p], _i),
+    "sdrg_fft_schedule_set": ([_i, _i, _i], _i),
+    "sdrg_fft_schedule_get": ([_i, _p, _p], _i),
+    "sdrg_fft_schedule_save": ([C.c_char_p], _i),
+    "sdrg_fft_schedule_load": ([C.c_char_p], _i),
     "sdrg_corr_fft_noalloc": ([_p, _p, _i, _p, _p], _i),
     "sdrg_acq_plan_new": ([C.POINTER(AcqSig), _i], _p),
     "sdrg_acq_plan_free": ([_p], None),

@@ -202,66 +202,131 @@ static size_t plan_smem(int M, const FftPlanK &k)
 // Max dynamic shared memory per CTA assumed when no device is present.
 static const size_t kSmemDefault = 232448;
 
+// Pass structure of a length-L transform split R ways (M = L / R): false
+// when M is not 2-3-5-smooth, needs too many passes or does not fit one CTA.
+static bool shape_for_R(int L, int R, int *Mout, FftPlanK *kout)
+{
+    if (R <= 0 || L % R) return false;
+    size_t smax = g_dev.id >= 0 ? g_dev.smem_optin : kSmemDefault;
+    int M = L / R;
+    Fact f;
+    if (!factor235(M, &f)) return false;
+    std::vector<int> cur, best;
+    if (M == 1) best.push_back(1);
+    else best_radices(M, cur, best);
+    if (best.empty() || (int)best.size() > kMaxPass) return false;
+    // Even radices first (largest first), odd radices last: the last
+    // passes have the smallest strides, and an odd stride of 8-byte
+    // elements spreads a half-warp over all 16 bank pairs.
+    std::stable_sort(best.begin(), best.end(), [](int a, int b) {
+        if ((a & 1) != (b & 1)) return (a & 1) == 0;
+        return a > b;
+    });
+    FftPlanK k{};
+    k.M = M;
+    k.npass = (int)best.size();
+    int Ls = M, off = 0;
+    for (int p = 0; p < k.npass; ++p) {
+        k.radix[p] = best[p];
+        k.Ls[p] = Ls;
+        k.twoff[p] = off;
+        // pass 0: S entries (powers formed in registers); later passes:
+        // S * (r - 1) entries, every twiddle of the pass
+        off += (p == 0) ? Ls / best[p] : (Ls / best[p]) * (best[p] - 1);
+        Ls /= best[p];
+    }
+    k.twtot = off;   // M == 1: one radix-1 pass, one unit twiddle
+    if (plan_smem(M, k) > smax) return false;
+    *Mout = M;
+    *kout = k;
+    return true;
+}
+
+bool shape_ok(int L, int R)
+{
+    int M;
+    FftPlanK k;
+    return shape_for_R(L, R, &M, &k);
+}
+
+// R <= 8: one thread-block cluster per transform; R in 10..20: staged
+// through an L2-resident scratch (a cluster cannot exceed 8 portably)
+static const int kSplits[] = {1, 2, 3, 4, 5, 6, 8, 10, 12, 15, 16, 20};
+
+static bool split_allowed(int R)
+{
+    for (int r : kSplits)
+        if (r == R) return true;
+    return false;
+}
+
+// ---- schedules (autotuned or loaded; per length: split and CTA size) -------
+struct Sched {
+    int R, threads;
+    double ms;
+};
+static std::mutex g_sched_mtx;
+static std::map<int, Sched> g_sched;
+
+static bool sched_of(int L, Sched *out)
+{
+    std::lock_guard<std::mutex> lk(g_sched_mtx);
+    auto it = g_sched.find(L);
+    if (it == g_sched.end()) return false;
+    *out = it->second;
+    return true;
+}
+
 bool plan_shape(int L, int *Rout, int *Mout, FftPlanK *kout)
 {
-    // R <= 8: one thread-block cluster per transform; R in 10..20: staged
-    // through an L2-resident scratch (a cluster cannot exceed 8 portably)
-    static const int Rs[] = {1, 2, 3, 4, 5, 6, 8, 10, 12, 15, 16, 20};
-    size_t smax = g_dev.id >= 0 ? g_dev.smem_optin : kSmemDefault;
-    for (int R : Rs) {
-        if (L % R) continue;
-        int M = L / R;
-        Fact f;
-        if (!factor235(M, &f)) continue;
-        std::vector<int> cur, best;
-        if (M == 1) best.push_back(1);
-        else best_radices(M, cur, best);
-        if (best.empty() || (int)best.size() > kMaxPass) continue;
-        // Even radices first (largest first), odd radices last: the last
-        // passes have the smallest strides, and an odd stride of 8-byte
-        // elements spreads a half-warp over all 16 bank pairs.
-        std::stable_sort(best.begin(), best.end(), [](int a, int b) {
-            if ((a & 1) != (b & 1)) return (a & 1) == 0;
-            return a > b;
-        });
-        FftPlanK k{};
-        k.M = M;
-        k.npass = (int)best.size();
-        int Ls = M, off = 0;
-        for (int p = 0; p < k.npass; ++p) {
-            k.radix[p] = best[p];
-            k.Ls[p] = Ls;
-            k.twoff[p] = off;
-            // pass 0: S entries (powers formed in registers); later passes:
-            // S * (r - 1) entries, every twiddle of the pass
-            off += (p == 0) ? Ls / best[p] : (Ls / best[p]) * (best[p] - 1);
-            Ls /= best[p];
-        }
-        k.twtot = off;   // M == 1: one radix-1 pass, one unit twiddle
-        if (plan_smem(M, k) > smax) continue;
-        *Rout = R;
-        *Mout = M;
-        *kout = k;
+    Sched sc;
+    if (sched_of(L, &sc) && shape_for_R(L, sc.R, Mout, kout)) {
+        *Rout = sc.R;
         return true;
+    }
+    for (int R : kSplits) {
+        if (shape_for_R(L, R, Mout, kout)) {
+            *Rout = R;
+            return true;
+        }
     }
     return false;
 }
 
 static std::mutex g_plan_mtx;
 static std::map<int, FftPlan *> g_plans;
+static std::map<long long, FftPlan *> g_shaped;   // (L, R, threads) -> plan
+static std::vector<FftPlan *> g_retired;          // replaced by a new schedule
 
-static int build_plan(int L, FftPlan *pl)
+// default CTA size: up to 512 threads, at least 8 points per thread
+static int default_threads(int M)
 {
-    int R, M;
+    int t = 32;
+    while (t < 512 && t * 8 < M) t *= 2;
+    return t;
+}
+
+// R_force / t_force > 0 impose the split and CTA size; otherwise the length's
+// schedule, else the default rule.
+static int build_plan(int L, FftPlan *pl, int R_force = 0, int t_force = 0)
+{
+    int R = 0, M;
     FftPlanK k;
-    if (!plan_shape(L, &R, &M, &k)) {
+    Sched sc = {0, 0, 0.0};
+    const bool have = !R_force && sched_of(L, &sc);
+    if (R_force) {
+        if (!shape_for_R(L, R_force, &M, &k))
+            return set_error(SDRG_ERR_ARG, "FFT length %d cannot be split %d ways", L, R_force);
+        R = R_force;
+    } else if (!plan_shape(L, &R, &M, &k)) {
         return set_error(SDRG_ERR_ARG,
                          "FFT length %d unsupported (needs L = R*M, R in {1..6,8,10,12,15,16,20}, "
                          "M 2-3-5-smooth and fitting one CTA)", L);
     }
     pl->L = L; pl->R = R; pl->M = M; pl->k = k;
-    int t = 32;
-    while (t < 512 && t * 8 < M) t *= 2;
+    int t = default_threads(M);
+    if (t_force > 0) t = t_force;
+    else if (have && sc.R == R && sc.threads > 0) t = sc.threads;
     pl->threads = t;
     pl->smem = plan_smem(M, k);
     // per-pass twiddles: pass 0 exp(-2 pi i * i / Ls_0), i < S_0; pass p >= 1
@@ -324,6 +389,48 @@ const FftPlan *get_plan(int L)
     return pl;
 }
 
+const FftPlan *get_plan_shaped(int L, int R, int threads)
+{
+    std::lock_guard<std::mutex> lk(g_plan_mtx);
+    const long long key = ((long long)L << 24) | ((long long)R << 12) | threads;
+    auto it = g_shaped.find(key);
+    if (it != g_shaped.end()) return it->second;
+    FftPlan *pl = new FftPlan();
+    if (build_plan(L, pl, R, threads) != SDRG_OK) {
+        delete pl;
+        return nullptr;
+    }
+    g_shaped[key] = pl;
+    return pl;
+}
+
+int set_schedule(int L, int R, int threads, double ms)
+{
+    if (L <= 0) return set_error(SDRG_ERR_ARG, "schedule: bad length %d", L);
+    if (R == 0) {                      // back to the default rule
+        std::lock_guard<std::mutex> lk(g_sched_mtx);
+        g_sched.erase(L);
+    } else {
+        int M;
+        FftPlanK k;
+        if (!split_allowed(R) || !shape_for_R(L, R, &M, &k))
+            return set_error(SDRG_ERR_ARG, "schedule: length %d cannot be split %d ways", L, R);
+        if (threads != 128 && threads != 256 && threads != 512)
+            return set_error(SDRG_ERR_ARG, "schedule: CTA size %d not 128, 256 or 512", threads);
+        std::lock_guard<std::mutex> lk(g_sched_mtx);
+        g_sched[L] = Sched{R, threads, ms};
+    }
+    // plans built from now on follow the schedule; a cached one is retired
+    // (kept alive: acquisition plans may still point to it)
+    std::lock_guard<std::mutex> lk(g_plan_mtx);
+    auto it = g_plans.find(L);
+    if (it != g_plans.end()) {
+        g_retired.push_back(it->second);
+        g_plans.erase(it);
+    }
+    return SDRG_OK;
+}
+
 } // namespace sdrg
 
 using namespace sdrg;
@@ -378,9 +485,69 @@ void sdrg_inject_alloc_failure(int after)
 // streams and CPU tables; call it if present.
 void sdr_func_init_cpu(const char *file) __attribute__((weak));
 
+int sdrg_fft_schedule_set(int L, int R, int threads)
+{
+    return set_schedule(L, R, threads, 0.0);
+}
+
+int sdrg_fft_schedule_get(int L, int *R, int *threads)
+{
+    Sched sc;
+    if (!sched_of(L, &sc)) return 0;
+    if (R) *R = sc.R;
+    if (threads) *threads = sc.threads;
+    return 1;
+}
+
+// File lines "sdrg_fft <L> <R> <threads> <ms>"; other lines are ignored, so
+// the reference's FFTW wisdom file given to sdr_func_init loads nothing.
+int sdrg_fft_schedule_save(const char *path)
+{
+    if (!path) return set_error(SDRG_ERR_ARG, "schedule save: no path");
+    FILE *f = fopen(path, "w");
+    if (!f) return set_error(SDRG_ERR_ARG, "schedule save: cannot open %s", path);
+    fprintf(f, "# pocketsdr_b200 FFT schedules: sdrg_fft <length> <split> <threads> <ms>\n");
+    {
+        std::lock_guard<std::mutex> lk(g_sched_mtx);
+        for (const auto &kv : g_sched)
+            fprintf(f, "sdrg_fft %d %d %d %.6f\n", kv.first, kv.second.R, kv.second.threads,
+                    kv.second.ms);
+    }
+    fclose(f);
+    return SDRG_OK;
+}
+
+int sdrg_fft_schedule_load(const char *path)
+{
+    if (!path) return set_error(SDRG_ERR_ARG, "schedule load: no path");
+    FILE *f = fopen(path, "r");
+    if (!f) return set_error(SDRG_ERR_ARG, "schedule load: cannot open %s", path);
+    char line[256];
+    int n = 0, bad = 0;
+    while (fgets(line, sizeof(line), f)) {
+        int L, R, t;
+        double ms = 0.0;
+        if (sscanf(line, "sdrg_fft %d %d %d %lf", &L, &R, &t, &ms) < 3) continue;
+        if (set_schedule(L, R, t, ms) == SDRG_OK) ++n;
+        else ++bad;
+    }
+    fclose(f);
+    if (bad) return set_error(SDRG_ERR_ARG, "schedule load: %d invalid entries in %s", bad, path);
+    return n;
+}
+
 void sdr_func_init(const char *file)
 {
     if (sdr_func_init_cpu) sdr_func_init_cpu(file ? file : "");
+    // the reference imports FFTW wisdom from `file` (src/sdr_func.c:118-121);
+    // its counterpart here is a schedule file, read when present
+    if (file && *file) {
+        FILE *f = fopen(file, "r");
+        if (f) {
+            fclose(f);
+            sdrg_fft_schedule_load(file);
+        }
+    }
     ensure_device(nullptr);
 }
 

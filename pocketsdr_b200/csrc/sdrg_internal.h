@@ -81,7 +81,13 @@ struct FftPlan {
 // Returns a cached plan for length L (thread-safe), or nullptr with the
 // error set when L has no supported decomposition.
 const FftPlan *get_plan(int L);
+// A plan with an imposed split and CTA size (cached per shape; autotuning).
+const FftPlan *get_plan_shaped(int L, int R, int threads);
+// Sets length L's schedule (R = 0: back to the default rule); later plans
+// for L use it.
+int set_schedule(int L, int R, int threads, double ms);
 bool plan_shape(int L, int *R, int *M, FftPlanK *k);
+bool shape_ok(int L, int R);       // L splits R ways into a fitting length
 
 // ---- kernel launch helpers (defined in the .cu files) -----------------------
 // Packed IF source of one coherent block for the forward transform.

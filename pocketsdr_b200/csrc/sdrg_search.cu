@@ -1157,6 +1157,94 @@ int sdrg_acq_set_codes(sdrg_acq_plan_t *plan, int g, const int8_t *code_I_dev,
                            G.sig.L, 0, G.code, st);
 }
 
+// Times the consumer (code product + inverse FFT + power accumulation) of a
+// synthetic search - 4 PRNs x 8 bins x 4 sums of length L, L/2 offsets kept -
+// for every cluster split of L with 256- and 512-thread CTAs (a staged split
+// only when L has no cluster split), best of 3 runs after one warm-up, and
+// sets L's schedule to the fastest.
+int sdrg_fft_autotune(int L, int *R_out, int *threads_out, double *ms_out)
+{
+    Device *dev;
+    int e;
+    if ((e = ensure_device(&dev))) return e;
+    if (L <= 1) return set_error(SDRG_ERR_ARG, "autotune: bad length %d", L);
+    cudaStream_t st;
+    if ((e = thread_stream(&st))) return e;
+    const int n_prn = 4, n_bin = 8, n_sum = 4, Nmax = L / 2 > 0 ? L / 2 : 1;
+    struct Cand { int R, t; };
+    std::vector<Cand> cands;
+    static const int Rc[] = {1, 2, 3, 4, 5, 6, 8};
+    for (int R : Rc)
+        if (shape_ok(L, R))
+            for (int t : {256, 512}) cands.push_back({R, t});
+    float2 *X = nullptr, *code = nullptr, *W = nullptr;
+    float *P = nullptr;
+    const size_t xb = (size_t)n_bin * n_sum * L * sizeof(float2);
+    const size_t cb = (size_t)n_prn * L * sizeof(float2);
+    const size_t pb = (size_t)n_prn * n_bin * Nmax * sizeof(float);
+    if ((e = alloc_fault("autotune"))) return e;
+    if (cudaMalloc(&X, xb) != cudaSuccess || cudaMalloc(&code, cb) != cudaSuccess ||
+        cudaMalloc(&P, pb) != cudaSuccess) {
+        e = cuda_error(cudaGetLastError(), "autotune buffers");
+        cudaFree(X); cudaFree(code); cudaFree(P);
+        return e;
+    }
+    cudaMemsetAsync(X, 0, xb, st);
+    cudaMemsetAsync(code, 0, cb, st);
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    int bestR = 0, bestT = 0;
+    double best = 1e30;
+    std::vector<Cand> tried = cands;
+    if (tried.empty()) {           // no cluster split: the default (staged) shape
+        int R, M;
+        FftPlanK k;
+        if (plan_shape(L, &R, &M, &k)) tried.push_back({R, 0});
+    }
+    for (const Cand &cd : tried) {
+        const FftPlan *pl = cd.t ? get_plan_shaped(L, cd.R, cd.t) : get_plan(L);
+        if (!pl) { sdr_gpu_clear_error(); continue; }
+        if (pl->threads > 512) continue;
+        ConsArgs ca = {};
+        ca.pl = pl->k; ca.tw = pl->tw_dev; ca.split = pl->split_dev; ca.X = X; ca.code = code;
+        ca.n_prn = n_prn; ca.n_bin = n_bin; ca.n_sum = n_sum; ca.prn0 = 0;
+        ca.scale = 1.0f / L / L; ca.Nmax = Nmax;
+        ca.prn_stride = (size_t)n_bin * Nmax; ca.bin_stride = Nmax; ca.accumulate = 0; ca.P = P;
+        const int wt = staged_chunk(pl, n_prn * n_bin);
+        if (wt && !W && cudaMalloc(&W, (size_t)wt * L * sizeof(float2)) != cudaSuccess) {
+            e = cuda_error(cudaGetLastError(), "autotune scratch");
+            break;
+        }
+        double tbest = 1e30;
+        bool ok = true;
+        for (int rep = 0; rep < 4 && ok; ++rep) {
+            cudaEventRecord(a, st);
+            ok = launch_consumer<0>(pl, ca, n_prn * n_bin, st, W, wt) == SDRG_OK;
+            cudaEventRecord(b, st);
+            if (ok && cudaEventSynchronize(b) == cudaSuccess && rep > 0) {
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, a, b);
+                tbest = ms < tbest ? ms : tbest;
+            }
+        }
+        if (!ok) { sdr_gpu_clear_error(); continue; }
+        if (tbest < best) { best = tbest; bestR = pl->R; bestT = pl->threads; }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaStreamSynchronize(st);
+    cudaFree(X); cudaFree(code); cudaFree(P);
+    if (W) cudaFree(W);
+    if (e) return e;
+    if (!bestR) return set_error(SDRG_ERR_ARG, "autotune: no runnable shape for length %d", L);
+    if ((e = set_schedule(L, bestR, bestT, best))) return e;
+    if (R_out) *R_out = bestR;
+    if (threads_out) *threads_out = bestT;
+    if (ms_out) *ms_out = best;
+    return SDRG_OK;
+}
+
 int sdrg_acq_run(sdrg_acq_plan_t *plan, const uint8_t *const *if_dev, const int *len_if,
                  const int *ix, sdrg_acq_result_t *res_dev, void *stream)
 {
