@@ -285,6 +285,10 @@ void sdr_res_code(const int8_t *code_I, const int8_t *code_Q, int len_code, doub
 {
     if (!code_res || N + Nz <= 0) return;
     const size_t ob = (size_t)(N + Nz) * sizeof(sdr_cpx16_t);
+    if (N == 0 && Nz > 0) {            // the reference: all padding, zeros
+        memset(code_res, 0, ob);
+        return;
+    }
     int e = SDRG_ERR_ARG;
     if (!code_I || len_code <= 0 || N <= 0 || Nz < 0) {
         set_error(SDRG_ERR_ARG, "sdr_res_code: bad arguments (len_code=%d N=%d Nz=%d)",
@@ -304,6 +308,10 @@ void sdr_gen_code_fft(const int8_t *code_I, const int8_t *code_Q, int len_code, 
 {
     if (!code_fft || N + Nz <= 0) return;
     const size_t ob = (size_t)(N + Nz) * sizeof(sdr_cpx_t);
+    if (N == 0 && Nz > 0) {            // the DFT of all-zero padding
+        memset(code_fft, 0, ob);
+        return;
+    }
     int e = SDRG_ERR_ARG;
     if (!code_I || len_code <= 0 || N <= 0 || Nz < 0) {
         set_error(SDRG_ERR_ARG, "sdr_gen_code_fft: bad arguments (len_code=%d N=%d Nz=%d)",

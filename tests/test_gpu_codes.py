@@ -154,3 +154,17 @@ def test_plan_codes_from_device_chips(ref, gpu):
         assert np.all(np.abs(gb - ga) <= TOL * np.maximum(np.abs(ga), floor)), i
     assert np.array_equal(ra["bin"], rb["bin"]) and np.array_equal(ra["offset"], rb["offset"])
     assert np.all(np.abs(ra["cn0"] - rb["cn0"]) < 0.1)
+
+
+def test_drop_in_empty_replica_is_zero_padding(ref, gpu):
+    """N = 0: the reference fills the N + Nz outputs with zeros (no error)."""
+    from pocketsdr_b200 import codes
+    from pocketsdr_b200._lib import last_error, lib, ptr
+    c = codes.gen_code("L1CA", 3)
+    a = np.full((16, 2), 9, np.int8)
+    lib.sdr_res_code(ptr(c), None, len(c), 1e-3, 0.0, 4e6, 0, 16, ptr(a))
+    assert np.array_equal(a, ref.res_code(c, None, 1e-3, 0.0, 4e6, 0, 16))
+    f = np.full(16, 9, np.complex64)
+    lib.sdr_gen_code_fft(ptr(c), None, len(c), 1e-3, 0.0, 4e6, 0, 16, ptr(f))
+    assert not f.any() and not ref.gen_code_fft(c, None, 1e-3, 0.0, 4e6, 0, 16).any()
+    assert last_error()[0] == 0
