@@ -160,6 +160,7 @@ def test_drop_in_empty_replica_is_zero_padding(ref, gpu):
     """N = 0: the reference fills the N + Nz outputs with zeros (no error)."""
     from pocketsdr_b200 import codes
     from pocketsdr_b200._lib import last_error, lib, ptr
+    lib.sdr_gpu_clear_error()
     c = codes.gen_code("L1CA", 3)
     a = np.full((16, 2), 9, np.int8)
     lib.sdr_res_code(ptr(c), None, len(c), 1e-3, 0.0, 4e6, 0, 16, ptr(a))
