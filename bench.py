@@ -959,6 +959,9 @@ def run_search_batch(args):
                     "d2h_bytes_per_step": n * 40,
                     "note": "the call is already end to end from the caller's view (device IF "
                             "buffers, host results)"},
+            # per call and signal group: code DFT (forward + combine), forward
+            # FFT, consumer, peak (partial + final)
+            "gpu_launches": 6 * len(setups) * args.steps,
             "found": int(res["found"].sum()), "clocks": clocks}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, cores, kind, desc = cpu_reference_rate(wl)
@@ -1072,7 +1075,9 @@ def run_l6(args):
                     "d2h_bytes_per_step": 0,
                     "note": "device IF; results stay on the device (the tracking loop's next "
                             "step reads them there)"},
-            "gpu_launches": E * len(sats) * 3 + E, "clocks": clocks}
+            "gpu_launches": 4 * E * args.steps,   # per epoch: code permutation, forward FFT,
+                                                  # consumer, CSK decode (batched over channels)
+            "clocks": clocks}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, cores, kind, desc = cpu_l6_rate(fs, fi, N, Lc, sats, buf, pos, cfs, 20)
         line["cpu_baseline"] = {"value": rate, "unit": "channel-epochs/s", "cores": cores,
