@@ -491,16 +491,58 @@ __device__ __forceinline__ void s_pass0_store(const float2 *sm, const float2 *tw
     }
 }
 
+// inner inverse pass (radix R, stride S) restricted to one warp's region of
+// M / W consecutive elements (W warps): the passes after the first DIF pass
+// (the last DIT passes) never reach outside a block of Ls_1 = M / R0 points,
+// so when R0 equals the warp count each warp owns one such block.
+template <int R, int S, int REG>
+__device__ __forceinline__ void s_inner_warp(float2 *sm, const float2 *twp)
+{
+    constexpr int NB = REG / R, LS = R * S, IT = (NB + 31) / 32;
+    const int lane = threadIdx.x & 31;
+    float2 *base = sm + (threadIdx.x >> 5) * REG;
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int b = lane + it * 32;
+        if (b < NB) {
+            const int blk = b / S, i = b - blk * S;
+            float2 *p = base + blk * LS + i;
+            float2 v[R];
+#pragma unroll
+            for (int j = 0; j < R; ++j) v[j] = p[j * S];
+            if (S > 1) {
+#pragma unroll
+                for (int j = 1; j < R; ++j) v[j] = cmul(v[j], cconj(twp[(j - 1) * S + i]));
+            }
+            Dft<R, 1>::run(v);
+#pragma unroll
+            for (int j = 0; j < R; ++j) p[j * S] = v[j];
+        }
+    }
+}
+
 // Inverse transform with a compile-time plan (same contract as fft_inverse).
+// With R0 = warps per CTA, passes 3..1 run warp by warp (warp barriers only)
+// and one CTA barrier precedes the last pass.
 template <class P, class Store>
 __device__ __forceinline__ void fft_inverse_static(float2 *sm, const float2 *tw, Store &store)
 {
-    s_inner<P::R3, P::S3, P::M, P::NT, false>(sm, tw + P::O3);
-    __syncthreads();
-    s_inner<P::R2, P::S2, P::M, P::NT, false>(sm, tw + P::O2);
-    __syncthreads();
-    s_inner<P::R1, P::S1, P::M, P::NT, false>(sm, tw + P::O1);
-    __syncthreads();
+    if constexpr (P::R0 * 32 == P::NT) {
+        constexpr int REG = P::M / P::R0;
+        s_inner_warp<P::R3, P::S3, REG>(sm, tw + P::O3);
+        __syncwarp();
+        s_inner_warp<P::R2, P::S2, REG>(sm, tw + P::O2);
+        __syncwarp();
+        s_inner_warp<P::R1, P::S1, REG>(sm, tw + P::O1);
+        __syncthreads();
+    } else {
+        s_inner<P::R3, P::S3, P::M, P::NT, false>(sm, tw + P::O3);
+        __syncthreads();
+        s_inner<P::R2, P::S2, P::M, P::NT, false>(sm, tw + P::O2);
+        __syncthreads();
+        s_inner<P::R1, P::S1, P::M, P::NT, false>(sm, tw + P::O1);
+        __syncthreads();
+    }
     s_pass0_store<P::R0, P::S0, P::NT>(sm, tw + P::O0, store);
 }
 
