@@ -91,7 +91,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
@@ -143,7 +143,7 @@ def make_workload(name: str, seed: int, prn_limit=None, t_sum=20e-3):
 def workload_code_ffts(wl, g):
     """Conjugated code DFTs [n_prn, L] of group g of a workload."""
     from pocketsdr_b200 import synth
-    if wl.name == "acq_long_48mhz":
+    if getattr(wl, "name", "") == "acq_long_48mhz":
         return synth.long_code_ffts(g)
     return synth.group_code_ffts(g)
 
@@ -204,7 +204,7 @@ def cpu_reference_rate(wl, max_threads: int | None = None, budget_prn: int | Non
     total_core_s, total_cells, sample_desc = 0.0, 0, []
     for g in wl.groups:
         n = min(len(g.prns), threads, budget_prn or threads)
-        if wl.name == "acq_long_48mhz":
+        if getattr(wl, "name", "") == "acq_long_48mhz":
             cfs = [synth.long_replica_fft(g.sig, p, g.fs, g.T, g.L) for p in g.prns[:n]]
         else:
             cfs = [synth.tiled_code_fft(g.sig, p, g.fs, g.tile, g.N, g.L - g.N) for p in g.prns[:n]]
@@ -237,7 +237,7 @@ def cpu_reference_rate(wl, max_threads: int | None = None, budget_prn: int | Non
 def _bin_budget(wl):
     """Doppler bins per sampled PRN search on the CPU: all of them, except for
     the 480 000-point searches (401 bins x 20 sums would take minutes per PRN)."""
-    return 2 if wl.name == "acq_long_48mhz" else None
+    return 2 if getattr(wl, "name", "") == "acq_long_48mhz" else None
 
 
 # ---------------------------------------------------------------------------
@@ -839,7 +839,8 @@ def run_ingest(args):
           for _ in range(args.steps)]
     clk = ClockSampler(local)
     clk.start()
-    reps = 50                                   # calls per timed step sample (clock sampler)
+    reps = 200                                  # calls per timed step (a long enough region
+                                                # for the clock sampler)
     for k in range(args.steps):
         flush.fill_(k & 0xFF)
         ev[k][0].record(st)
@@ -1022,7 +1023,7 @@ def cpu_l6_rate(fs, fi, N, Lc, sats, buf, pos, cfs, n_epochs):
 
 
 def run_l6(args):
-    """QZSS L6 CSK tracking: a step is 25 epochs (100 ms) of 10 L6D channels,
+    """QZSS L6 CSK tracking: a step is 250 epochs (1 s) of 10 L6D channels,
     one sdrg_l6_csk_batch call per 4 ms epoch."""
     import torch
     from pocketsdr_b200 import track
@@ -1033,7 +1034,7 @@ def run_l6(args):
     torch.cuda.set_stream(st)
     d = torch.from_numpy(buf).cuda()
     cfd = [torch.from_numpy(c).cuda() for c in cfs]
-    E = 25
+    E = 250                                     # 1 s of stream per step
 
     def specs(e):
         ix = (e * N) % len(buf)
@@ -1043,11 +1044,11 @@ def run_l6(args):
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
     outs = [(torch.empty(len(sats), dtype=torch.uint8, device="cuda"),
              torch.empty((len(sats), 107), dtype=torch.complex64, device="cuda"),
-             torch.empty((len(sats), N), dtype=torch.complex64, device="cuda")) for _ in range(E)]
+             torch.empty((len(sats), N), dtype=torch.complex64, device="cuda")) for _ in range(4)]
 
     def step():
         for e in range(E):
-            track.l6_csk_batch(epochs[e], [d.data_ptr()], [len(buf)], st.cuda_stream, outs[e])
+            track.l6_csk_batch(epochs[e], [d.data_ptr()], [len(buf)], st.cuda_stream, outs[e % 4])
 
     for _ in range(args.warmup):
         step()

@@ -414,7 +414,10 @@ typedef struct {
 /* Runs every request's search (res[i] for req[i]); if_dev / len_if: DEVICE
  * IF buffers; t_acq: the receiver's sdr_t_acq (s); thres_cn0: its
  * sdr_thres_cn0_l. Synchronous (returns with the results on the host);
- * work is issued on `stream` (NULL = the calling thread's stream). */
+ * work is issued on `stream` (NULL = the calling thread's stream). The
+ * acquisition plan of the last call is kept per host thread and reused by
+ * the next call with the same group structure (same setups, request counts
+ * and bins); sdrg_search_release frees it (it is also freed at thread exit). */
 int sdrg_search_batch(const sdrg_srch_setup_t *setups, int n_setup,
     const sdrg_srch_req_t *req, int n_req, const uint8_t *const *if_dev,
     const int *len_if, int ix, double t_acq, double thres_cn0, sdrg_srch_res_t *res,
@@ -423,6 +426,8 @@ int sdrg_search_batch(const sdrg_srch_setup_t *setups, int n_setup,
 /* The grouping sdrg_search_batch uses (host only, no device work): returns
  * the number of signal groups (or a negative status) and, if non-NULL, each
  * request's group and each group's sums and Doppler bins. */
+void sdrg_search_release(void);
+
 int sdrg_srch_groups(const sdrg_srch_setup_t *setups, int n_setup,
     const sdrg_srch_req_t *req, int n_req, double t_acq, int *group_of_req,
     int *n_sum, int *len_fds);

@@ -118,6 +118,7 @@ SIGNATURES = {
     "sdrg_acq_set_codes": ([_p, _i, _p, _p, _i, _d, _d, _i, _p], _i),
     "sdrg_search_batch": ([C.POINTER(SrchSetup), _i, C.POINTER(SrchReq), _i, _p, _p, _i, _d, _d,
                            C.POINTER(SrchRes), _p], _i),
+    "sdrg_search_release": ([], None),
     "sdrg_srch_groups": ([C.POINTER(SrchSetup), _i, C.POINTER(SrchReq), _i, _d, _p, _p, _p], _i),
     "sdrg_l6_csk_batch": ([C.POINTER(L6Job), _i, _p, _p, _p, _p, _p, _p], _i),
     "sdrg_csk_decode": ([_p, _i, _i, _i, _p, _i, _p, _p, _p], _i),

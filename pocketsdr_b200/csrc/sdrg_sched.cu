@@ -94,11 +94,48 @@ int make_groups(const sdrg_srch_setup_t *su, int n_su, const sdrg_srch_req_t *rq
     return SDRG_OK;
 }
 
+// The last call's plan of this host thread, reused by a call with the same
+// group structure (a receiver submits the same kind of batch again and
+// again); freed when the structure changes, by sdrg_search_release or at
+// thread exit.
+struct PlanCache {
+    std::vector<double> key;
+    sdrg_acq_plan_t *plan = nullptr;
+    ~PlanCache() { if (plan) sdrg_acq_plan_free(plan); }
+};
+
+PlanCache &plan_cache()
+{
+    static thread_local PlanCache c;
+    return c;
+}
+
+std::vector<double> plan_key(const std::vector<sdrg_acq_sig_t> &sigs,
+                             const std::vector<SrchGroup> &gs)
+{
+    std::vector<double> k;
+    for (size_t g = 0; g < sigs.size(); ++g) {
+        const sdrg_acq_sig_t &s = sigs[g];
+        k.insert(k.end(), {(double)s.L, (double)s.N, (double)s.Nmax, (double)s.n_sum,
+                           (double)s.n_prn, (double)s.len_fds, s.fs, s.fi, s.T, (double)s.buf});
+        k.insert(k.end(), gs[g].fds.begin(), gs[g].fds.end());
+    }
+    return k;
+}
+
 } // namespace
 
 using namespace sdrg;
 
 extern "C" {
+
+void sdrg_search_release(void)
+{
+    PlanCache &pc = plan_cache();
+    if (pc.plan) sdrg_acq_plan_free(pc.plan);
+    pc.plan = nullptr;
+    pc.key.clear();
+}
 
 int sdrg_srch_groups(const sdrg_srch_setup_t *setups, int n_setup, const sdrg_srch_req_t *req,
                      int n_req, double t_acq, int *group_of_req, int *n_sum, int *len_fds)
@@ -143,8 +180,19 @@ int sdrg_search_batch(const sdrg_srch_setup_t *setups, int n_setup, const sdrg_s
         s.buf = u.buf;
         n_buf = u.buf + 1 > n_buf ? u.buf + 1 : n_buf;
     }
-    sdrg_acq_plan_t *plan = sdrg_acq_plan_new(sigs.data(), (int)sigs.size());
-    if (!plan) return tctx().error ? tctx().error : SDRG_ERR_CUDA;
+    PlanCache &pc = plan_cache();
+    std::vector<double> key = plan_key(sigs, gs);
+    if (pc.plan && pc.key != key) {
+        cudaStreamSynchronize(st);
+        sdrg_acq_plan_free(pc.plan);
+        pc.plan = nullptr;
+    }
+    if (!pc.plan) {
+        pc.plan = sdrg_acq_plan_new(sigs.data(), (int)sigs.size());
+        if (!pc.plan) return tctx().error ? tctx().error : SDRG_ERR_CUDA;
+        pc.key = key;
+    }
+    sdrg_acq_plan_t *plan = pc.plan;
 
     size_t rows = 0, maxlen = 0;
     for (const SrchGroup &g : gs) {
@@ -183,8 +231,11 @@ int sdrg_search_batch(const sdrg_srch_setup_t *setups, int n_setup, const sdrg_s
     if (chips) cudaFreeAsync(chips, st);
     if (rdev) cudaFreeAsync(rdev, st);
     cudaStreamSynchronize(st);
-    sdrg_acq_plan_free(plan);
-    if (e) return e;
+    if (e) {                          // a failed plan is not kept
+        sdrg_acq_plan_free(plan);
+        pc.plan = nullptr;
+        return e;
+    }
 
     // search_sig's decision per channel (src/sdr_ch.c:424-447)
     row = 0;

@@ -56,3 +56,32 @@ def test_search_batch_matches_reference_search_sig(ref, gpu):
         assert abs(g["cn0"] - w["cn0"]) < 0.1 and g["n_sum"] == w["n_sum"], i
         assert abs(g["fd"] - w["fd"]) < 0.5 and g["coff"] == w["coff"], (i, g["fd"], w["fd"])
     assert got["found"][1] and got["found"][2]      # PRN 4 (47 dB-Hz) and 9 (44 dB-Hz)
+
+
+def test_search_batch_reuses_plan_with_new_codes(ref, gpu):
+    """Back-to-back calls with the same group structure reuse the cached plan
+    but search the new requests' codes; a call with another structure (and
+    sdrg_search_release) starts afresh - every result equals the reference's
+    search_sig replay."""
+    torch = pytest.importorskip("torch")
+    from pocketsdr_b200 import codes, schedule, synth
+    from pocketsdr_b200._lib import lib
+    fs, fi, T = 12e6, 3.0e6, 1e-3
+    N = int(fs * T)
+    sats = [synth.Sat("L1CA", 6, 100.5, 900.0, 0.3, 46.0),
+            synth.Sat("L1CA", 21, 700.25, -1500.0, 0.7, 45.0)]
+    buf = synth.gen_if(12 * N, fs, {"L1CA": fi}, sats, iq=False, bits=2, seed=31)
+    prns = list(range(1, 33))
+    chips = np.stack([codes.gen_code("L1CA", p) for p in prns])
+    setups = [schedule.Setup(chips, T, fs, fi, max_dop=5000.0)]
+    d = torch.from_numpy(buf).cuda()
+    full = np.asarray(ref.dop_bins(T, 0.0, 5000.0), np.float32)
+    t_acq, thres, ix = 3e-3, 38.0, 1000
+    for rows in ([0, 2, 4], [5, 20, 9], [5, 20], [1, 6, 11, 20]):
+        reqs = [schedule.Request(0, r) for r in rows]
+        got = schedule.search(setups, reqs, [d], ix, t_acq, thres)
+        for i, r in enumerate(rows):
+            w = _reference_search(ref, chips[r], T, fs, fi, N, full, buf, ix, t_acq, thres)
+            assert (got[i]["bin"], got[i]["offset"]) == (w["bin"], w["offset"]), (rows, r)
+            assert bool(got[i]["found"]) == w["found"] and abs(got[i]["cn0"] - w["cn0"]) < 0.1
+    lib.sdrg_search_release()
