@@ -929,7 +929,8 @@ def run_search_batch(args):
     bufs_d = [torch.from_numpy(b).cuda() for b in wl.bufs]
     setups, reqs = [], []
     for i, g in enumerate(wl.groups):
-        chips = np.stack([codes.gen_code(g.sig, p) for p in g.prns])
+        # the receiver's codes live on the device (uploaded once, not per call)
+        chips = torch.from_numpy(np.stack([codes.gen_code(g.sig, p) for p in g.prns])).cuda()
         setups.append(schedule.Setup(chips, g.T, g.fs, g.fi, max_dop=5000.0, buf=g.buf, N=g.N))
         reqs += [schedule.Request(i, k) for k in range(len(g.prns))]
     t_acq, thres = 20e-3, 38.0

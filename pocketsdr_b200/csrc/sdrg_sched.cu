@@ -123,6 +123,17 @@ std::vector<double> plan_key(const std::vector<sdrg_acq_sig_t> &sigs,
     return k;
 }
 
+// Gathers n code rows of len bytes: row r of dst is copied from src[r].
+__global__ void gather_rows_kernel(const int8_t *const *src, int8_t *dst, int len, int n)
+{
+    const int r = blockIdx.y;
+    if (r >= n) return;
+    const int8_t *s = src[r];
+    int8_t *d = dst + (size_t)r * len;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < len; i += gridDim.x * blockDim.x)
+        d[i] = s[i];
+}
+
 } // namespace
 
 using namespace sdrg;
@@ -209,20 +220,35 @@ int sdrg_search_batch(const sdrg_srch_setup_t *setups, int n_setup, const sdrg_s
         cudaMallocAsync((void **)&rdev, rows * sizeof(sdrg_acq_result_t), st) != cudaSuccess) {
         e = cuda_error(cudaGetLastError(), "sdrg_search_batch scratch");
     }
-    // each group's codes, gathered per request, then the code DFTs on the device
+    // each group's codes gathered per request (one kernel over a table of
+    // source rows), then the code DFTs on the device
+    std::vector<const int8_t *> srcs(rows);
+    {
+        size_t r = 0;
+        for (const SrchGroup &g : gs)
+            for (int i : g.reqs) {
+                const sdrg_srch_setup_t &u = setups[g.setup];
+                srcs[r++] = u.code_dev + (size_t)req[i].prn * u.len_code;
+            }
+    }
+    const int8_t **src_d = nullptr;
+    if (!e && (cudaMallocAsync((void **)&src_d, rows * sizeof(int8_t *), st) != cudaSuccess ||
+               cudaMemcpyAsync(src_d, srcs.data(), rows * sizeof(int8_t *), cudaMemcpyHostToDevice,
+                               st) != cudaSuccess))
+        e = cuda_error(cudaGetLastError(), "sdrg_search_batch code table");
     size_t row = 0;
     for (size_t g = 0; g < gs.size() && !e; ++g) {
         const sdrg_srch_setup_t &u = setups[gs[g].setup];
         int8_t *dst = chips + row * maxlen;
-        for (size_t j = 0; j < gs[g].reqs.size() && !e; ++j) {
-            const int prn = req[gs[g].reqs[j]].prn;
-            if (cudaMemcpyAsync(dst + j * u.len_code, u.code_dev + (size_t)prn * u.len_code,
-                                (size_t)u.len_code, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-                e = cuda_error(cudaGetLastError(), "sdrg_search_batch code gather");
-        }
+        const int n = (int)gs[g].reqs.size();
+        gather_rows_kernel<<<dim3((unsigned)((u.len_code + 255) / 256 < 16 ? (u.len_code + 255) / 256 : 16),
+                                  (unsigned)n), 256, 0, st>>>(src_d + row, dst, u.len_code, n);
+        const cudaError_t ge = cudaGetLastError();
+        if (ge != cudaSuccess) e = cuda_error(ge, "code gather");
         if (!e) e = sdrg_acq_set_codes(plan, (int)g, dst, nullptr, u.len_code, u.T, 0.0, u.N, st);
         row += gs[g].reqs.size();
     }
+    if (src_d) cudaFreeAsync(src_d, st);
     if (!e) e = sdrg_acq_run(plan, if_dev, len_if, ixs.data(), rdev, st);
     if (!e && (cudaMemcpyAsync(rhost.data(), rdev, rows * sizeof(sdrg_acq_result_t),
                                cudaMemcpyDeviceToHost, st) != cudaSuccess ||
