@@ -1077,8 +1077,8 @@ def run_l6(args):
                     "d2h_bytes_per_step": 0,
                     "note": "device IF; results stay on the device (the tracking loop's next "
                             "step reads them there)"},
-            "gpu_launches": 4 * E * args.steps,   # per epoch: code permutation, forward FFT,
-                                                  # consumer, CSK decode (batched over channels)
+            "gpu_launches": 5 * E * args.steps,   # per epoch: code gather, code permutation,
+                                                  # forward FFT, consumer, CSK decode (batched)
             "clocks": clocks}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, cores, kind, desc = cpu_l6_rate(fs, fi, N, Lc, sats, buf, pos, cfs, 20)

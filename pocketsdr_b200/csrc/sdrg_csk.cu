@@ -94,6 +94,25 @@ __global__ void __launch_bounds__(kCskThreads) csk_kernel(CskArgs a)
             interp(corr, N, n, __dadd_rn(x0, a.pos[(size_t)j * SDR_MAX_CORR + k]));
 }
 
+// Gathers n code DFTs of N complex values: row r of dst from src[r].
+__global__ void gather_codes_kernel(const float2 *const *src, float2 *dst, int N, int n)
+{
+    const int r = blockIdx.y;
+    if (r >= n) return;
+    const float4 *s = (const float4 *)src[r];
+    float4 *d = (float4 *)(dst + (size_t)r * N);
+    const bool v = (N % 2 == 0) && (((uintptr_t)s & 15) == 0);
+    if (v) {
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N / 2; i += gridDim.x * blockDim.x)
+            d[i] = __ldg(s + i);
+    } else {
+        const float2 *s2 = src[r];
+        float2 *d2 = dst + (size_t)r * N;
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+            d2[i] = s2[i];
+    }
+}
+
 static int launch_csk(const CskArgs &a, int n_job, cudaStream_t st)
 {
     csk_kernel<<<n_job, kCskThreads, 0, st>>>(a);
@@ -220,8 +239,10 @@ int sdrg_l6_csk_batch(const sdrg_l6_job_t *jobs, int n_job, const uint8_t *const
     // (3 per job) | tap positions (SDR_MAX_CORR doubles per job), one upload
     const size_t mb = 5 * (size_t)n_job * sizeof(uint32_t), ib = 3 * (size_t)n_job * sizeof(int);
     const size_t pb = (size_t)n_job * SDR_MAX_CORR * sizeof(double);
+    const size_t cpb = (size_t)n_job * sizeof(float2 *);
     const size_t o_i = (mb + 15) / 16 * 16, o_p = (o_i + ib + 15) / 16 * 16;
-    const size_t tab_bytes = (o_p + pb + 255) / 256 * 256;
+    const size_t o_c = (o_p + pb + 15) / 16 * 16;
+    const size_t tab_bytes = (o_c + cpb + 255) / 256 * 256;
     const size_t cb = corr_dev ? 0 : ((size_t)n_job * Nmax * sizeof(float2) + 255) / 256 * 256;
     const size_t wb = batched ? 3 * (size_t)n_job * Nmax * sizeof(float2) : scr;
     const size_t dev_bytes = tab_bytes + cb + wb + 256;
@@ -241,6 +262,7 @@ int sdrg_l6_csk_batch(const sdrg_l6_job_t *jobs, int n_job, const uint8_t *const
     uint32_t *mix = (uint32_t *)hb;
     int *ints = (int *)(hb + o_i);
     double *posh = (double *)(hb + o_p);
+    const float2 **codes_h = (const float2 **)(hb + o_c);
     memset(posh, 0, pb);
     for (int j = 0; j < n_job; ++j) {
         const sdrg_l6_job_t &b = jobs[j];
@@ -248,6 +270,7 @@ int sdrg_l6_csk_batch(const sdrg_l6_job_t *jobs, int n_job, const uint8_t *const
         ints[n_job + j] = b.len_code;
         ints[2 * n_job + j] = b.n;
         for (int k = 0; k < b.n; ++k) posh[(size_t)j * SDR_MAX_CORR + k] = b.pos[k];
+        codes_h[j] = (const float2 *)b.code_fft;
         uint32_t w[5];
         corr_job_tables(len_if[b.buf], b.ix, b.N, b.fs, b.fc, b.phi, w);
         for (int k = 0; k < 5; ++k) {
@@ -256,7 +279,7 @@ int sdrg_l6_csk_batch(const sdrg_l6_job_t *jobs, int n_job, const uint8_t *const
         }
     }
     char *db = (char *)c.l6_dev.ptr;
-    SDRG_CUDA(cudaMemcpyAsync(db, hb, o_p + pb, cudaMemcpyHostToDevice, st));
+    SDRG_CUDA(cudaMemcpyAsync(db, hb, o_c + cpb, cudaMemcpyHostToDevice, st));
     SDRG_CUDA(cudaEventRecord(c.l6_ev, st));
     const uint32_t *mix_d = (const uint32_t *)db;
     float2 *corr = corr_dev ? (float2 *)corr_dev : (float2 *)(db + tab_bytes);
@@ -264,11 +287,12 @@ int sdrg_l6_csk_batch(const sdrg_l6_job_t *jobs, int n_job, const uint8_t *const
     e = SDRG_OK;
     if (batched) {
         float2 *codes = (float2 *)work;       // the jobs' code DFTs back to back
-        for (int j = 0; j < n_job && !e; ++j)
-            if (cudaMemcpyAsync(codes + (size_t)j * Nmax, jobs[j].code_fft,
-                                (size_t)Nmax * sizeof(float2), cudaMemcpyDeviceToDevice,
-                                st) != cudaSuccess)
-                e = cuda_error(cudaGetLastError(), "sdrg_l6_csk_batch codes");
+        const dim3 gg((unsigned)((Nmax / 2 + 255) / 256 < 64 ? (Nmax / 2 + 255) / 256 : 64),
+                      (unsigned)n_job);
+        gather_codes_kernel<<<gg, 256, 0, st>>>((const float2 *const *)(db + o_c), codes, Nmax,
+                                                n_job);
+        const cudaError_t ge = cudaGetLastError();
+        if (ge != cudaSuccess) e = cuda_error(ge, "sdrg_l6_csk_batch codes");
         if (!e)
             e = corr_jobs_device(if_dev[jobs[0].buf], len_if[jobs[0].buf], mix_d, n_job, Nmax,
                                  codes, corr, codes + (size_t)n_job * Nmax, st);
