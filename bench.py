@@ -241,9 +241,69 @@ def _bin_budget(wl):
 
 
 # ---------------------------------------------------------------------------
+def _reference_other(args):
+    """The reference arm of the non-acquisition workloads: their reference
+    CPU paths (the same functions as their cpu_baseline legs), one JSON line
+    in each workload's metric and unit; refinement has no reference
+    counterpart."""
+    w = args.workload
+    if w == "refine_12mhz":
+        return {"impl": "reference", "unavailable": "the reference has no delay / Doppler "
+                "refinement after its grid search (its finest estimate is sdr_fine_dop); "
+                "refine_12mhz's cpu_baseline times the reference grid plus the FP64 oracle"}
+    vals, desc, cores, kind, metric, unit, cfg = [], "", 0, "", "", "", {}
+    for k in range(args.warmup + args.steps):
+        if w == "track_24mhz":
+            from pocketsdr_b200 import synth
+            wl = synth.track_24mhz(seed=5)
+            specs_list = []
+            for e in range(20):
+                sp = wl.jobs_at(e * 1e-3, [0] * len(wl.channels))
+                for s_, c in zip(sp, [c for c in wl.channels
+                                      if abs(round(e * 1e-3 / c.T) * c.T - e * 1e-3) < 1e-9]):
+                    s_["ch"] = wl.channels.index(c)
+                specs_list.append(sp)
+            rate, cores, kind, desc = cpu_track_rate(wl, specs_list, synth.track_banks(wl))
+            metric, unit, cfg = TRACK_METRIC, "channel-epochs/s", {"workload": w, "channels": 256}
+            per_step = 100 * sum(len(sp) for sp in specs_list) / len(specs_list)   # 100 ms
+        elif w == "ingest_raw32_24mhz":
+            raw = np.random.default_rng(3).integers(0, 256, 24000 * 4 * 200, dtype=np.uint8)
+            rate, cores, kind, desc = cpu_ingest_rate(ingest_config(24000), raw, 1000)
+            metric, unit, cfg = INGEST_METRIC, "samples/s", {"workload": w}
+            per_step = 2400000                                                     # 100 ms
+        elif w == "l6_csk_24mhz":
+            fs, fi, T, N, Lc, sats, buf, pos, cfs = _l6_workload(7)
+            rate, cores, kind, desc = cpu_l6_rate(fs, fi, N, Lc, sats, buf, pos, cfs, 20)
+            metric, unit, cfg = L6_METRIC, "channel-epochs/s", {"workload": w, "channels": 10}
+            per_step = 250 * len(sats)                                             # 1 s
+        elif w == "search_batch_24mhz":
+            wl = make_workload("acq_multi_24mhz", 2)
+            r, cores, kind, desc = cpu_reference_rate(wl, budget_prn=4)
+            rate = r / (wl.cells / sum(len(g.prns) for g in wl.groups))
+            metric, unit, cfg = SRCH_METRIC, "searches/s", {"workload": w, "channels": 163}
+            per_step = 163                                                         # one call
+        else:
+            return None
+        if k >= args.warmup:
+            vals.append(rate)
+    v = statistics.median(vals)
+    return {"metric": metric, "value": v, "unit": unit, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": per_step / v * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": cfg, "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": unit, "cores": cores, "kind": kind, "sample": desc},
+            "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 def run_reference(args):
     rank, world, _ = dist_info()
     if rank != 0:
+        return 0
+    if args.workload not in ("acq_multi_24mhz", "acq_l1ca_12mhz", "acq_long_48mhz"):
+        line = _reference_other(args)
+        if line is None:
+            raise SystemExit(f"unknown workload {args.workload}")
+        print(json.dumps(line), flush=True)
         return 0
     wl = make_workload(args.workload, 2)
     vals = []
