@@ -281,6 +281,21 @@ int sdrg_acq_run(sdrg_acq_plan_t *plan, const uint8_t *const *if_dev,
     const int *len_if, const int *ix, sdrg_acq_result_t *res_dev,
     void *stream);
 
+/* sdrg_acq_run through a CUDA graph. The first call, and a call whose IF
+ * buffer pointers, lengths or result pointer differ from the ones captured,
+ * captures the plan's launch sequence (fork to the internal streams, every
+ * group's forward / consumer / peak kernels, join) into a graph; every call
+ * then uploads the start-sample tables on `stream` when ix changed and
+ * replays the graph there: one launch per run. Same results as
+ * sdrg_acq_run; kernel timing (sdrg_acq_profile) does not see graph runs.
+ * The graph is released with the plan. */
+int sdrg_acq_run_graph(sdrg_acq_plan_t *plan, const uint8_t *const *if_dev,
+    const int *len_if, const int *ix, sdrg_acq_result_t *res_dev,
+    void *stream);
+
+/* Number of graph captures sdrg_acq_run_graph has made for the plan. */
+int sdrg_acq_graph_captures(const sdrg_acq_plan_t *plan);
+
 /* Device pointer to the accumulated grid of group g, laid out
  * [n_prn][len_fds][Nmax] (float), valid after sdrg_acq_run completes. */
 const float *sdrg_acq_grid(const sdrg_acq_plan_t *plan, int g);

@@ -107,6 +107,8 @@ SIGNATURES = {
     "sdrg_acq_plan_free": ([_p], None),
     "sdrg_acq_plan_cells": ([_p], C.c_int64),
     "sdrg_acq_run": ([_p, _p, _p, _p, _p, _p], _i),
+    "sdrg_acq_run_graph": ([_p, _p, _p, _p, _p, _p], _i),
+    "sdrg_acq_graph_captures": ([_p], _i),
     "sdrg_acq_grid": ([_p, _i], _p),
     "sdrg_acq_grid_host": ([_p, _i, _p], _i),
     "sdrg_acq_profile": ([_p, _i], _i),

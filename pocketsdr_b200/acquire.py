@@ -82,17 +82,23 @@ class AcqPlan:
             check("sdrg_acq_run_host")
         return res
 
-    def run_device(self, buf_ptrs, lens, ix, res_ptr: int, stream: int = 0) -> None:
+    def run_device(self, buf_ptrs, lens, ix, res_ptr: int, stream: int = 0,
+                   graph: bool = False) -> None:
         """Asynchronous run on device-resident IF buffers (raw device
-        pointers, e.g. torch tensor data_ptr()) on a CUDA stream handle."""
+        pointers, e.g. torch tensor data_ptr()) on a CUDA stream handle.
+        graph=True replays the plan's captured CUDA graph (captured on the
+        first call for these buffers)."""
         n = len(buf_ptrs)
         ptrs = (C.c_void_p * n)(*buf_ptrs)
         lens_ = (C.c_int * n)(*lens)
         ixs = (C.c_int * n)(*ix)
-        st = lib.sdrg_acq_run(self.handle, ptrs, lens_, ixs, C.c_void_p(res_ptr),
-                              C.c_void_p(stream))
+        fn = lib.sdrg_acq_run_graph if graph else lib.sdrg_acq_run
+        st = fn(self.handle, ptrs, lens_, ixs, C.c_void_p(res_ptr), C.c_void_p(stream))
         if st:
-            check("sdrg_acq_run")
+            check("sdrg_acq_run_graph" if graph else "sdrg_acq_run")
+
+    def graph_captures(self) -> int:
+        return int(lib.sdrg_acq_graph_captures(self.handle))
 
     def grid_ptr(self, g: int) -> int:
         return int(lib.sdrg_acq_grid(self.handle, g) or 0)

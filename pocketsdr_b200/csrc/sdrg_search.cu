@@ -754,7 +754,23 @@ struct sdrg_acq_plan {
     int run = 0;
     std::vector<cudaEvent_t> ev_pool;
     std::vector<Rec> ev_used;
+    // sdrg_acq_run_graph: the captured launch sequence and the buffers it
+    // was captured for
+    cudaStream_t cap_stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    std::vector<intptr_t> graph_key;
+    int graph_captures = 0;
 };
+
+static void drop_graph(sdrg_acq_plan_t *plan)
+{
+    if (plan->graph_exec) cudaGraphExecDestroy(plan->graph_exec);
+    if (plan->graph) cudaGraphDestroy(plan->graph);
+    plan->graph_exec = nullptr;
+    plan->graph = nullptr;
+    plan->graph_key.clear();
+}
 
 namespace sdrg {
 
@@ -1092,6 +1108,11 @@ sdrg_acq_plan_t *sdrg_acq_plan_new(const sdrg_acq_sig_t *sigs, int n_sig)
 void sdrg_acq_plan_free(sdrg_acq_plan_t *plan)
 {
     if (!plan) return;
+    drop_graph(plan);
+    if (plan->cap_stream) {
+        cudaStreamSynchronize(plan->cap_stream);
+        cudaStreamDestroy(plan->cap_stream);
+    }
     for (cudaStream_t s : plan->streams) {
         if (!s) continue;
         cudaStreamSynchronize(s);
@@ -1245,43 +1266,61 @@ int sdrg_fft_autotune(int L, int *R_out, int *threads_out, double *ms_out)
     return SDRG_OK;
 }
 
-int sdrg_acq_run(sdrg_acq_plan_t *plan, const uint8_t *const *if_dev, const int *len_if,
-                 const int *ix, sdrg_acq_result_t *res_dev, void *stream)
+// Start-sample tables of group gi when the read position or length of its
+// buffer changed since the last upload: written into the pinned staging
+// buffer once the previous upload from it has completed, then copied on st.
+static int upload_tables(GroupState &G, const int *len_if, const int *ix, cudaStream_t st)
 {
-    if (!plan || !if_dev || !len_if || !ix || !res_dev)
-        return set_error(SDRG_ERR_ARG, "sdrg_acq_run: null argument");
-    Device *dev;
-    int e;
-    if ((e = ensure_device(&dev))) return e;
-    cudaStream_t caller = (cudaStream_t)stream;
-    if (!caller && (e = thread_stream(&caller))) return e;
+    const sdrg_acq_sig_t &s = G.sig;
+    if (G.last_len == len_if[s.buf] && G.last_ix == ix[s.buf]) return SDRG_OK;
+    SDRG_CUDA(cudaEventSynchronize(G.tab_ev));   // previous upload done
+    group_tables(G, len_if, ix);
+    SDRG_CUDA(cudaMemcpyAsync(G.tab_dev, G.tab_host, (G.tab_words - s.len_fds) * 4,
+                              cudaMemcpyHostToDevice, st));
+    SDRG_CUDA(cudaEventRecord(G.tab_ev, st));
+    G.last_len = len_if[s.buf];
+    G.last_ix = ix[s.buf];
+    return SDRG_OK;
+}
+
+static int check_run(const sdrg_acq_plan_t *plan, const int *len_if)
+{
     for (size_t gi = 0; gi < plan->g.size(); ++gi) {
         const sdrg_acq_sig_t &s = plan->g[gi].sig;
         if (len_if[s.buf] < s.L)
             return set_error(SDRG_ERR_ARG, "IF buffer %d shorter than L=%d", s.buf, s.L);
     }
-    // fork: every internal stream starts after the caller's prior work
-    if (plan->prof) {
+    return SDRG_OK;
+}
+
+// The launch sequence of one run: fork the internal streams from `caller`,
+// every group's forward / consumer / peak kernels on its stream, join back.
+// With `ix` the tables are uploaded on the group streams as needed; without
+// (graph capture) the caller has uploaded them and no profiling events are
+// recorded.
+static int launch_run(sdrg_acq_plan_t *plan, Device *dev, const uint8_t *const *if_dev,
+                      const int *len_if, const int *ix, sdrg_acq_result_t *res_dev,
+                      cudaStream_t caller)
+{
+    int e;
+    const bool prof = plan->prof && ix;
+    if (prof) {
         cudaEvent_t r[2];
         if ((e = prof_begin(plan, caller, r))) return e;   // records r[0]
         plan->ev_pool.push_back(r[1]);
         plan->ev_used.push_back({-1, plan->run, r[0], r[0]});
     }
+    const bool saved = plan->prof;
+    plan->prof = prof;
+    struct Restore { sdrg_acq_plan_t *p; bool v; ~Restore() { p->prof = v; } } restore{plan, saved};
+    // fork: every internal stream starts after the caller's prior work
     SDRG_CUDA(cudaEventRecord(plan->ev_fork, caller));
     for (cudaStream_t s2 : plan->streams) SDRG_CUDA(cudaStreamWaitEvent(s2, plan->ev_fork, 0));
     for (size_t gi = 0; gi < plan->g.size(); ++gi) {
         GroupState &G = plan->g[gi];
         const sdrg_acq_sig_t &s = G.sig;
         cudaStream_t st = plan->streams[gi % plan->streams.size()];
-        if (G.last_len != len_if[s.buf] || G.last_ix != ix[s.buf]) {
-            SDRG_CUDA(cudaEventSynchronize(G.tab_ev));   // previous upload done
-            group_tables(G, len_if, ix);
-            SDRG_CUDA(cudaMemcpyAsync(G.tab_dev, G.tab_host, (G.tab_words - s.len_fds) * 4,
-                                      cudaMemcpyHostToDevice, st));
-            SDRG_CUDA(cudaEventRecord(G.tab_ev, st));
-            G.last_len = len_if[s.buf];
-            G.last_ix = ix[s.buf];
-        }
+        if (ix && (e = upload_tables(G, len_if, ix, st))) return e;
         const int nb = s.len_fds, ns = s.n_sum;
         FwdArgs fa = {};
         fa.pl = G.pl->k; fa.tw = G.pl->tw_dev; fa.ctab = dev->ctab_dev; fa.R = G.pl->R;
@@ -1319,8 +1358,94 @@ int sdrg_acq_run(sdrg_acq_plan_t *plan, const uint8_t *const *if_dev, const int 
         SDRG_CUDA(cudaEventRecord(plan->ev_join[i], plan->streams[i]));
         SDRG_CUDA(cudaStreamWaitEvent(caller, plan->ev_join[i], 0));
     }
+    return SDRG_OK;
+}
+
+int sdrg_acq_run(sdrg_acq_plan_t *plan, const uint8_t *const *if_dev, const int *len_if,
+                 const int *ix, sdrg_acq_result_t *res_dev, void *stream)
+{
+    if (!plan || !if_dev || !len_if || !ix || !res_dev)
+        return set_error(SDRG_ERR_ARG, "sdrg_acq_run: null argument");
+    Device *dev;
+    int e;
+    if ((e = ensure_device(&dev))) return e;
+    cudaStream_t caller = (cudaStream_t)stream;
+    if (!caller && (e = thread_stream(&caller))) return e;
+    if ((e = check_run(plan, len_if))) return e;
+    if ((e = launch_run(plan, dev, if_dev, len_if, ix, res_dev, caller))) return e;
     plan->run++;
     return SDRG_OK;
+}
+
+// The buffers a captured graph was made for: kernel arguments hold the IF
+// pointers and lengths and the result pointer, the tables hold the rest.
+static std::vector<intptr_t> graph_key(const sdrg_acq_plan_t *plan, const uint8_t *const *if_dev,
+                                       const int *len_if, const sdrg_acq_result_t *res_dev)
+{
+    int nbuf = 0;
+    for (auto &G : plan->g) nbuf = G.sig.buf + 1 > nbuf ? G.sig.buf + 1 : nbuf;
+    std::vector<intptr_t> k;
+    k.push_back((intptr_t)res_dev);
+    for (int b = 0; b < nbuf; ++b) {
+        k.push_back((intptr_t)if_dev[b]);
+        k.push_back((intptr_t)len_if[b]);
+    }
+    return k;
+}
+
+static int capture_graph(sdrg_acq_plan_t *plan, Device *dev, const uint8_t *const *if_dev,
+                         const int *len_if, sdrg_acq_result_t *res_dev)
+{
+    drop_graph(plan);
+    if (!plan->cap_stream)
+        SDRG_CUDA(cudaStreamCreateWithFlags(&plan->cap_stream, cudaStreamNonBlocking));
+    SDRG_CUDA(cudaStreamBeginCapture(plan->cap_stream, cudaStreamCaptureModeRelaxed));
+    int e = launch_run(plan, dev, if_dev, len_if, nullptr, res_dev, plan->cap_stream);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(plan->cap_stream, &graph);
+    if (e) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        return e;
+    }
+    if (ce != cudaSuccess) return cuda_error(ce, "sdrg_acq_run_graph: capture");
+    const cudaError_t ie = cudaGraphInstantiate(&plan->graph_exec, graph, 0);
+    if (ie != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        plan->graph_exec = nullptr;
+        return cuda_error(ie, "sdrg_acq_run_graph: instantiate");
+    }
+    plan->graph = graph;
+    plan->graph_key = graph_key(plan, if_dev, len_if, res_dev);
+    return SDRG_OK;
+}
+
+int sdrg_acq_run_graph(sdrg_acq_plan_t *plan, const uint8_t *const *if_dev, const int *len_if,
+                       const int *ix, sdrg_acq_result_t *res_dev, void *stream)
+{
+    if (!plan || !if_dev || !len_if || !ix || !res_dev)
+        return set_error(SDRG_ERR_ARG, "sdrg_acq_run_graph: null argument");
+    Device *dev;
+    int e;
+    if ((e = ensure_device(&dev))) return e;
+    cudaStream_t caller = (cudaStream_t)stream;
+    if (!caller && (e = thread_stream(&caller))) return e;
+    if ((e = check_run(plan, len_if))) return e;
+    if (!plan->graph_exec || plan->graph_key != graph_key(plan, if_dev, len_if, res_dev)) {
+        if ((e = capture_graph(plan, dev, if_dev, len_if, res_dev))) return e;
+        ++plan->graph_captures;
+    }
+    // tables first, on the caller's stream, ordered before the replay
+    for (auto &G : plan->g)
+        if ((e = upload_tables(G, len_if, ix, caller))) return e;
+    SDRG_CUDA(cudaGraphLaunch(plan->graph_exec, caller));
+    plan->run++;
+    return SDRG_OK;
+}
+
+int sdrg_acq_graph_captures(const sdrg_acq_plan_t *plan)
+{
+    return plan ? plan->graph_captures : 0;
 }
 
 int sdrg_acq_run_host(sdrg_acq_plan_t *plan, const uint8_t *const *if_host, const int *len_if,

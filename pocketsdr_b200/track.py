@@ -74,37 +74,52 @@ def code_bank(code, T, fs, N, code_Q=None) -> np.ndarray:
     return np.concatenate(banks)
 
 
+class L6Batch:
+    """One epoch of QZSS L6 channels prepared for sdrg_l6_csk_batch: the job
+    array and pointer arguments are built once, run() makes the call. specs
+    are dicts with buf, ix, N, fs, fc, phi, code_fft (CUDA complex64 tensor:
+    the bank's conjugated code DFT), len_code, pos. Results go to CUDA tensors
+    (symbols uint8 [n], taps complex64 [n, SDR_MAX_CORR], correlations
+    complex64 [n, max N]), the given `out` triple or new ones."""
+
+    def __init__(self, specs, if_ptrs, lens, out=None):
+        import torch
+        from ._lib import L6Job
+        specs = list(specs)
+        self.n = n = len(specs)
+        self.arr = arr = (L6Job * n)()
+        self._keep = []
+        for j, s in zip(arr, specs):
+            pos = np.ascontiguousarray(s["pos"], np.float64)
+            self._keep += [pos, s["code_fft"]]
+            j.buf, j.ix, j.N = int(s["buf"]), int(s["ix"]), int(s["N"])
+            j.fs, j.fc, j.phi = float(s["fs"]), float(s["fc"]), float(s["phi"])
+            j.code_fft = C.c_void_p(s["code_fft"].data_ptr())
+            j.len_code, j.n = int(s["len_code"]), len(pos)
+            j.pos = pos.ctypes.data_as(C.POINTER(C.c_double))
+        nmax = max(int(s["N"]) for s in specs)
+        if out is None:
+            out = (torch.empty(n, dtype=torch.uint8, device="cuda"),
+                   torch.empty((n, SDR_MAX_CORR), dtype=torch.complex64, device="cuda"),
+                   torch.empty((n, nmax), dtype=torch.complex64, device="cuda"))
+        self.out = out
+        self._args = ((C.c_void_p * len(if_ptrs))(*if_ptrs), (C.c_int * len(if_ptrs))(*lens),
+                      C.c_void_p(out[0].data_ptr()), C.c_void_p(out[1].data_ptr()),
+                      C.c_void_p(out[2].data_ptr()))
+
+    def run(self, stream: int = 0):
+        """Asynchronous on `stream` (0: torch's current stream)."""
+        if not stream:
+            import torch
+            stream = torch.cuda.current_stream().cuda_stream
+        ptrs, ls, sym, taps, corr = self._args
+        if lib.sdrg_l6_csk_batch(self.arr, self.n, ptrs, ls, sym, taps, corr, C.c_void_p(stream)):
+            check("sdrg_l6_csk_batch")
+        return self.out
+
+
 def l6_csk_batch(specs, if_ptrs, lens, stream: int = 0, out=None):
-    """QZSS L6 channels of one epoch (sdrg_l6_csk_batch): specs are dicts with
-    buf, ix, N, fs, fc, phi, code_fft (CUDA complex64 tensor: the bank's
-    conjugated code DFT), len_code, pos. Returns CUDA tensors (symbols uint8
-    [n], taps complex64 [n, SDR_MAX_CORR], correlations complex64 [n, max N]),
-    written into `out` (the same three tensors) when given; asynchronous."""
-    import torch
-    from ._lib import L6Job
-    specs = list(specs)
-    arr = (L6Job * len(specs))()
-    keep = []
-    for j, s in zip(arr, specs):
-        pos = np.ascontiguousarray(s["pos"], np.float64)
-        keep += [pos, s["code_fft"]]
-        j.buf, j.ix, j.N = int(s["buf"]), int(s["ix"]), int(s["N"])
-        j.fs, j.fc, j.phi = float(s["fs"]), float(s["fc"]), float(s["phi"])
-        j.code_fft = C.c_void_p(s["code_fft"].data_ptr())
-        j.len_code, j.n = int(s["len_code"]), len(pos)
-        j.pos = pos.ctypes.data_as(C.POINTER(C.c_double))
-    n = len(specs)
-    nmax = max(int(s["N"]) for s in specs)
-    if out is None:
-        out = (torch.empty(n, dtype=torch.uint8, device="cuda"),
-               torch.empty((n, SDR_MAX_CORR), dtype=torch.complex64, device="cuda"),
-               torch.empty((n, nmax), dtype=torch.complex64, device="cuda"))
-    sym, taps, corr = out
-    ptrs = (C.c_void_p * len(if_ptrs))(*if_ptrs)
-    ls = (C.c_int * len(if_ptrs))(*lens)
-    st = stream or torch.cuda.current_stream().cuda_stream
-    if lib.sdrg_l6_csk_batch(arr, n, ptrs, ls, C.c_void_p(sym.data_ptr()),
-                             C.c_void_p(taps.data_ptr()), C.c_void_p(corr.data_ptr()),
-                             C.c_void_p(st)):
-        check("sdrg_l6_csk_batch")
-    return sym, taps, corr
+    """QZSS L6 channels of one epoch (sdrg_l6_csk_batch); see L6Batch for the
+    specs. Returns the CUDA tensors (symbols, taps, correlations), written
+    into `out` when given; asynchronous."""
+    return L6Batch(specs, if_ptrs, lens, out).run(stream)
