@@ -187,14 +187,21 @@ def load_traffic() -> dict:
 
 # ---------------------------------------------------------------------------
 def cpu_reference_rate(wl, max_threads: int | None = None, budget_prn: int | None = None,
-                       max_bins: int | None = None):
+                       max_bins: int | None = None, variants: dict | None = None):
     """Reference CPU throughput (cells/s) of the whole workload on this host,
     estimated from a bounded sample: for each group, up to `threads` PRN
     searches (every sum, the reference's own sdr_search_code built from
     source, or the oracle restatement when that build is absent) run in
     parallel threads, over every Doppler bin or the first `max_bins` (the
     search cost is the same per bin); core-seconds per PRN scale to the full
-    bin and PRN sets, spread over all cores."""
+    bin and PRN sets, spread over all cores.
+
+    With `variants` (a dict) two more rates are filled in: "single_thread"
+    (one PRN search per group timed alone on one thread, scaled to the whole
+    workload) and "no_sleep" (the all-core rate without sdr_search_code's 1 ms
+    CPU release after every 22nd bin: the sleeps a full search makes, times
+    the measured cost of the reference's own sdr_sleep_msec(1), taken off the
+    core-seconds; the restatement does not sleep)."""
     import concurrent.futures as cf
     from oracle import oracle
     from pocketsdr_b200 import synth
@@ -202,6 +209,7 @@ def cpu_reference_rate(wl, max_threads: int | None = None, budget_prn: int | Non
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
     threads = min(cores, max_threads or cores)
     total_core_s, total_cells, sample_desc = 0.0, 0, []
+    single_s, sleeps = 0.0, 0
     for g in wl.groups:
         n = min(len(g.prns), threads, budget_prn or threads)
         if getattr(wl, "name", "") == "acq_long_48mhz":
@@ -226,10 +234,18 @@ def cpu_reference_rate(wl, max_threads: int | None = None, budget_prn: int | Non
         core_s_per_prn = sum(per) / n
         total_core_s += core_s_per_prn * len(g.prns)
         total_cells += len(g.prns) * len(g.fds) * g.Nmax
+        if variants is not None:
+            single_s += one(cfs[0]) * len(g.prns)
+            sleeps += g.n_sum * (len(g.fds) // 22) * len(g.prns)
         sample_desc.append(f"{g.sig}:{n}/{len(g.prns)} PRN" +
                            (f" x {nb}/{len(g.fds)} bins" if nb < len(g.fds) else "") +
                            f" ({wall:.1f}s)")
     rate = total_cells / (total_core_s / threads)
+    if variants is not None:
+        sleep_s = R.sleep_cost() if hasattr(R, "sleep_cost") else 0.0
+        variants["single_thread"] = total_cells / single_s
+        variants["no_sleep"] = total_cells / ((total_core_s - sleeps * sleep_s) / threads)
+        variants["sleeps"] = {"count": sleeps, "ms_each": sleep_s * 1e3}
     return rate, threads, R.kind, "; ".join(sample_desc) + \
         f"; full PRN (and bin) sets extrapolated from core-seconds per PRN over {threads} threads"
 
@@ -464,9 +480,11 @@ def run_ours(args):
             "roofline": roofline, "clocks": clocks,
             "detected": int(sum(1 for r in res if r["cn0"] >= 38.0))}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, cores, kind, desc = cpu_reference_rate(wl, max_bins=_bin_budget(wl))
+        var = {}
+        rate, cores, kind, desc = cpu_reference_rate(wl, max_bins=_bin_budget(wl), variants=var)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
-                                "sample": desc}
+                                "sample": desc, "single_thread": var["single_thread"],
+                                "no_sleep": var["no_sleep"], "sleeps": var["sleeps"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     plan.close()

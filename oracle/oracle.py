@@ -361,6 +361,17 @@ class Reference:
         self.lib.sdr_psd_cpx(_ptr(buff), len(buff), N, fs, IQ, _ptr(out))
         return out
 
+    def sleep_cost(self, n: int = 40) -> float:
+        """Mean seconds of the reference's sdr_sleep_msec(1), the CPU release
+        sdr_search_code makes after every 22nd Doppler bin
+        (src/sdr_func.c:681-683)."""
+        import time
+        self.lib.sdr_sleep_msec.argtypes = [_i]
+        t0 = time.perf_counter()
+        for _ in range(n):
+            self.lib.sdr_sleep_msec(1)
+        return (time.perf_counter() - t0) / n
+
     def search_code(self, code_fft, buff, ix, N, fs, fi, fds, P, T=1e-3):
         code_fft = np.ascontiguousarray(code_fft, np.complex64)
         b, sb = self._buff(buff)
