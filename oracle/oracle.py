@@ -47,6 +47,10 @@ def build(ref: bool = True) -> None:
     targets = ["oracle"]
     if ref and os.path.isdir(REF_ROOT + "/src"):
         targets.append("ref")
+        # the reference's unit test and pocket_acq relinked against the GPU
+        # library (which the package build makes first)
+        if os.path.exists(os.path.join(HERE, "..", "pocketsdr_b200", "lib", "libsdr_gpu.so")):
+            targets.append("linktest")
     subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
 
 
