@@ -1,11 +1,12 @@
 """Link test: the reference's own programs relinked against the GPU library.
 
 oracle/Makefile (target `linktest`) builds, from the reference sources,
-* test/src/test_sdr_func.c, the reference's unit test of sdr_func.c, and
+* test/src/test_sdr_{func,code,ch}.c, the reference's unit tests of
+  sdr_func.c, sdr_code.c and sdr_ch.c, and
 * app/pocket_acq/pocket_acq.c, its acquisition app,
 twice: `*_gpu` with the hot symbols of sdr_func.o / sdr_code.o renamed `*_cpu`
 (objcopy) so that the calls resolve to libsdr_gpu.so, and `*_cpu` from the
-unmodified objects. The GPU-linked unit test must pass all 14 of its tests;
+unmodified objects. The GPU-linked unit tests must pass all of their tests;
 the GPU-linked pocket_acq, run on 20 ms of the reference's own L1 sample
 (sample/L1_20211125_004000_12MHz_I.bin as INT8, reconstructed from the
 committed fixture), must print the same code offsets and Doppler for the
@@ -37,17 +38,27 @@ def _undefined(path):
     return {ln.split()[-1] for ln in out.splitlines() if ln.strip()}
 
 
-def test_reference_unit_test_through_gpu_library(tmp_path):
-    exe = _bin("test_sdr_func_gpu")
+UNIT = [  # (program, tests it runs, hot functions it reaches)
+    ("test_sdr_func", 14, ("sdr_mix_carr", "sdr_corr_std", "sdr_corr_fft", "sdr_search_code",
+                           "sdr_psd_cpx", "sdr_lpf_apply")),
+    ("test_sdr_code", 7, ("sdr_res_code", "sdr_gen_code_fft")),
+    # the channel: search (sdr_search_code via search_sig) and tracking
+    # (sdr_mix_carr + sdr_corr_std via the correlator of a locked channel)
+    ("test_sdr_ch", 7, ("sdr_search_code", "sdr_mix_carr", "sdr_corr_std")),
+]
+
+
+@pytest.mark.parametrize("prog,n_tests,hot", UNIT)
+def test_reference_unit_tests_through_gpu_library(tmp_path, prog, n_tests, hot):
+    exe = _bin(prog + "_gpu")
     # the hot functions are not in the executable: they come from libsdr_gpu.so
     und = _undefined(exe)
-    for s in ("sdr_mix_carr", "sdr_corr_std", "sdr_corr_fft", "sdr_search_code",
-              "sdr_psd_cpx", "sdr_lpf_apply"):
+    for s in hot:
         assert s in und, s
     r = subprocess.run([exe], cwd=tmp_path, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     oks = [ln for ln in r.stdout.splitlines() if ln.endswith(" ... OK")]
-    assert len(oks) == 14, r.stdout
+    assert len(oks) == n_tests, r.stdout
 
 
 _LINE = re.compile(r"SIG= (\S+)\s*, PRN=\s*(\d+), COFF=\s*([-\d.]+) ms, DOP=\s*([-\d]+) Hz, "
