@@ -214,7 +214,7 @@ int code_fft_device(const int8_t *ci, const int8_t *cq, int len_code, int n_code
     // sub-spectra scratch, stream-ordered so concurrent calls on other
     // streams never share it
     float2 *F = nullptr;
-    SDRG_CUDA(cudaMallocAsync((void **)&F, (size_t)n_code * L * sizeof(float2), st));
+    SDRG_CUDA(stream_alloc((void **)&F, (size_t)n_code * L * sizeof(float2), st));
     CodeFwdArgs fa = {};
     fa.pl = pl->k; fa.tw = pl->tw_dev; fa.R = pl->R; fa.ci = ci; fa.cq = cq;
     fa.len = len_code; fa.N = N; fa.cf = cf; fa.dx = dx; fa.F = F;

@@ -151,7 +151,7 @@ static int csk_upload(const CskTables &t, int n_job, void **dev, cudaStream_t st
 {
     const size_t ib = t.ints.size() * sizeof(int), db = t.pos.size() * sizeof(double);
     char *d = nullptr;
-    SDRG_CUDA(cudaMallocAsync((void **)&d, ib + db + 16, st));
+    SDRG_CUDA(stream_alloc((void **)&d, ib + db + 16, st));
     *dev = d;
     double *pos_d = (double *)(d + (ib + 15) / 16 * 16);
     if (cudaMemcpyAsync(d, t.ints.data(), ib, cudaMemcpyHostToDevice, st) != cudaSuccess ||

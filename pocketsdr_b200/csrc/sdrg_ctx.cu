@@ -108,6 +108,13 @@ int ensure_device(Device **out)
         // a pageable cudaMemcpy may return before its DMA completes, and the
         // library's kernels run on non-blocking streams: settle it here
         SDRG_CUDA(cudaDeviceSynchronize());
+        cudaMemPoolProps pp = {};
+        pp.allocType = cudaMemAllocationTypePinned;
+        pp.location.type = cudaMemLocationTypeDevice;
+        pp.location.id = id;
+        SDRG_CUDA(cudaMemPoolCreate(&g_dev.pool, &pp));
+        uint64_t keep = UINT64_MAX;
+        SDRG_CUDA(cudaMemPoolSetAttribute(g_dev.pool, cudaMemPoolAttrReleaseThreshold, &keep));
         g_dev.id = id;
     }
     SDRG_CUDA(cudaSetDevice(g_dev.id));
@@ -116,6 +123,12 @@ int ensure_device(Device **out)
 }
 
 size_t g_smem_limit() { return g_dev.id >= 0 ? g_dev.smem_optin : 232448; }
+
+cudaError_t stream_alloc(void **p, size_t bytes, cudaStream_t st)
+{
+    if (!g_dev.pool) return cudaErrorInitializationError;
+    return cudaMallocFromPoolAsync(p, bytes, g_dev.pool, st);
+}
 
 int thread_stream(cudaStream_t *s)
 {

@@ -35,8 +35,14 @@ struct Device {
     size_t smem_optin = 0;      // max dynamic shared memory per block
     int8_t ctab[512];           // quantised carrier (I,Q) for 256 phases
     char2 *ctab_dev = nullptr;  // same table on the device
+    cudaMemPool_t pool = nullptr;   // the library's stream-ordered scratch pool
 };
 int ensure_device(Device **out);   // lazy init of the selected device
+// Stream-ordered scratch from the library's own memory pool, which keeps
+// freed memory mapped (no release threshold): repeated calls of the same
+// size reuse it instead of mapping new pages after every synchronisation, as
+// the process's default pool would. Free with cudaFreeAsync.
+cudaError_t stream_alloc(void **p, size_t bytes, cudaStream_t st);
 size_t g_smem_limit();             // max dynamic shared memory per CTA
 
 // Grow-only device / pinned buffers owned by one host thread.

@@ -138,9 +138,9 @@ static int psd_device(const float2 *x, const uint8_t *buf, int len, int ix, int 
     float *w_dev = nullptr, *pw = nullptr;
     float2 *F = nullptr;
     const size_t segs = n_seg > 0 ? (size_t)n_seg : 1;
-    cudaError_t ce = cudaMallocAsync((void **)&w_dev, (size_t)N * sizeof(float), st);
-    if (ce == cudaSuccess) ce = cudaMallocAsync((void **)&F, segs * N * sizeof(float2), st);
-    if (ce == cudaSuccess) ce = cudaMallocAsync((void **)&pw, segs * N * sizeof(float), st);
+    cudaError_t ce = stream_alloc((void **)&w_dev, (size_t)N * sizeof(float), st);
+    if (ce == cudaSuccess) ce = stream_alloc((void **)&F, segs * N * sizeof(float2), st);
+    if (ce == cudaSuccess) ce = stream_alloc((void **)&pw, segs * N * sizeof(float), st);
     if (ce == cudaSuccess)
         ce = cudaMemcpyAsync(w_dev, w.data(), (size_t)N * sizeof(float), cudaMemcpyHostToDevice, st);
     if (ce == cudaSuccess && n_seg > 0) {

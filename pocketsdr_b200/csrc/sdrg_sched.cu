@@ -216,8 +216,8 @@ int sdrg_search_batch(const sdrg_srch_setup_t *setups, int n_setup, const sdrg_s
     std::vector<sdrg_acq_result_t> rhost(rows);
     std::vector<int> ixs(n_buf, ix);
     e = SDRG_OK;
-    if (cudaMallocAsync((void **)&chips, rows * maxlen, st) != cudaSuccess ||
-        cudaMallocAsync((void **)&rdev, rows * sizeof(sdrg_acq_result_t), st) != cudaSuccess) {
+    if (stream_alloc((void **)&chips, rows * maxlen, st) != cudaSuccess ||
+        stream_alloc((void **)&rdev, rows * sizeof(sdrg_acq_result_t), st) != cudaSuccess) {
         e = cuda_error(cudaGetLastError(), "sdrg_search_batch scratch");
     }
     // each group's codes gathered per request (one kernel over a table of
@@ -232,7 +232,7 @@ int sdrg_search_batch(const sdrg_srch_setup_t *setups, int n_setup, const sdrg_s
             }
     }
     const int8_t **src_d = nullptr;
-    if (!e && (cudaMallocAsync((void **)&src_d, rows * sizeof(int8_t *), st) != cudaSuccess ||
+    if (!e && (stream_alloc((void **)&src_d, rows * sizeof(int8_t *), st) != cudaSuccess ||
                cudaMemcpyAsync(src_d, srcs.data(), rows * sizeof(int8_t *), cudaMemcpyHostToDevice,
                                st) != cudaSuccess))
         e = cuda_error(cudaGetLastError(), "sdrg_search_batch code table");
