@@ -157,25 +157,41 @@ struct ConsArgs {
     int code_per_bin;       // 1: bin b correlates with code b (independent jobs)
     float *P;               // mode 0
     float2 *Y;              // mode 1: [n_bin][L]
+    // mode 0 with a split (R > 1) and several sums: the power of output
+    // n = R m + c is summed in Q[task][c][m] (Mq = ceil(Nmax / R) per row),
+    // where each CTA's accesses are consecutive; the last sum writes P
+    float *Q;               // or null: every sum reads and writes P
+    int Mq;
 };
+
+// Power store of one sum. kDirect: P = (add ? P : 0) + |y|^2. With the
+// accumulator Q: kQFirst Q = (add ? P : 0) + |y|^2, kQMid Q += |y|^2,
+// kQLast P = Q + |y|^2 - the same additions in the same order.
+enum { kDirect = 0, kQFirst = 1, kQMid = 2, kQLast = 3 };
 
 template <int R>
 struct StorePower {
     typedef float Old;
     float *row;       // P for this (prn, bin)
+    float *q;         // Q row of this (task, c), or null
     int c, Nmax;
     bool add;
+    int mode;
     __device__ __forceinline__ float pre(int m) const
     {
         const int n = R * m + c;
-        return (add && n < Nmax) ? row[n] : 0.0f;
+        if (n >= Nmax) return 0.0f;
+        if (mode == kQMid || mode == kQLast) return q[m];
+        return add ? row[n] : 0.0f;
     }
     __device__ __forceinline__ void operator()(int m, float2 y, float old) const
     {
         const int n = R * m + c;
         if (n < Nmax) {
             const float pw = y.x * y.x + y.y * y.y;
-            row[n] = add ? old + pw : pw;
+            const float v = (add || mode >= kQMid) ? old + pw : pw;
+            if (mode == kQFirst || mode == kQMid) q[m] = v;
+            else row[n] = v;
         }
     }
 };
@@ -282,7 +298,12 @@ __global__ void __launch_bounds__(512, 1) cons_kernel(ConsArgs a)
 
         if (MODE == 0) {
             float *row = a.P + (size_t)(prn) * a.prn_stride + (size_t)b * a.bin_stride;
-            StorePower<R> st{row, c, a.Nmax, a.accumulate || s > 0};
+            const bool useq = R > 1 && a.Q && a.n_sum > 1;
+            const int mode = !useq ? kDirect
+                : (s == 0 ? kQFirst : (s == a.n_sum - 1 ? kQLast : kQMid));
+            float *qrow = useq ? a.Q + ((size_t)task * R + c) * a.Mq : nullptr;
+            StorePower<R> st{row, qrow, c, a.Nmax, mode == kDirect ? (a.accumulate || s > 0)
+                                                                  : (a.accumulate != 0), mode};
             if constexpr (SP == 1) fft_inverse_static<Plan24000>(sm, tw, st);
             else fft_inverse(sm, tw, a.pl, st);
         } else {
@@ -308,6 +329,7 @@ struct StageArgs {
     int task0, s;            // first task of the chunk, sum index
     float scale;
     float2 *W;               // [chunk][R][M]
+    float *Q;                // power grids: [chunk][R][M] |y|^2 summed over the sums
 };
 
 template <int R>
@@ -347,22 +369,29 @@ __global__ void __launch_bounds__(256) stage_combine_kernel(StageArgs a)
     for (int j = 0; j < R; ++j) Wt[j * M + q] = g[j];
 }
 
-struct StorePowerRt {
+// Power of output n = R m + c accumulated over the sums in Q[c][m], so that
+// each CTA reads and writes consecutive addresses (the grid row itself holds
+// a CTA's outputs R floats apart). The first sum stores |y|^2, or adds it to
+// the caller's grid value when accumulating (the reference's order); later
+// sums add to Q. stage_power_kernel moves Q into the grid after the last sum.
+struct StorePowerQ {
     typedef float Old;
-    float *row;
+    float *q;            // Q row of this (task, c)
+    const float *p;      // grid row of the task (seed of the first sum)
     int c, R, Nmax;
-    bool add;
+    int mode;            // 0: store, 1: add to Q, 2: add to the grid value
     __device__ __forceinline__ float pre(int m) const
     {
         const int n = R * m + c;
-        return (add && n < Nmax) ? row[n] : 0.0f;
+        if (n >= Nmax || mode == 0) return 0.0f;
+        return mode == 1 ? q[m] : p[n];
     }
     __device__ __forceinline__ void operator()(int m, float2 y, float old) const
     {
         const int n = R * m + c;
         if (n < Nmax) {
             const float pw = y.x * y.x + y.y * y.y;
-            row[n] = add ? old + pw : pw;
+            q[m] = mode ? old + pw : pw;
         }
     }
 };
@@ -387,23 +416,65 @@ __global__ void __launch_bounds__(512, 1) stage_ifft_kernel(ConsArgs ca, StageAr
     const int prn = task % a.n_prn, b = task / a.n_prn;
     load_twiddles(tw, ca.tw, ca.pl.twtot);
     const float2 *src = a.W + ((size_t)tl * a.R + c) * M;
+    // W exceeds L2: UL loads per thread in flight before the shared-memory
+    // stores, so the copy runs at HBM bandwidth rather than latency
+    constexpr int UL = 8;
     if ((M & 1) == 0) {
         const float4 *s4 = (const float4 *)src;
         float4 *d4 = (float4 *)sm;
-        for (int i = threadIdx.x; i < M / 2; i += blockDim.x) d4[i] = __ldg(s4 + i);
+        const int n4 = M / 2;
+        for (int i0 = threadIdx.x; i0 < n4; i0 += UL * blockDim.x) {
+            float4 v[UL];
+#pragma unroll
+            for (int u = 0; u < UL; ++u) {
+                const int i = i0 + u * blockDim.x;
+                if (i < n4) v[u] = __ldg(s4 + i);
+            }
+#pragma unroll
+            for (int u = 0; u < UL; ++u) {
+                const int i = i0 + u * blockDim.x;
+                if (i < n4) d4[i] = v[u];
+            }
+        }
     } else {
         for (int i = threadIdx.x; i < M; i += blockDim.x) sm[i] = __ldg(src + i);
     }
     __syncthreads();
     if (MODE == 0) {
-        float *row = ca.P + (size_t)prn * ca.prn_stride + (size_t)b * ca.bin_stride;
-        StorePowerRt st{row, c, a.R, ca.Nmax, ca.accumulate || a.s > 0};
+        const float *row = ca.P + (size_t)prn * ca.prn_stride + (size_t)b * ca.bin_stride;
+        StorePowerQ st{a.Q + ((size_t)tl * a.R + c) * M, row, c, a.R, ca.Nmax,
+                       a.s > 0 ? 1 : (ca.accumulate ? 2 : 0)};
         if constexpr (SP == 1) fft_inverse_static<Plan24000>(sm, tw, st);
         else fft_inverse(sm, tw, ca.pl, st);
     } else {
         StoreComplexRt st{ca.Y + (size_t)b * a.R * M, c, a.R};
         if constexpr (SP == 1) fft_inverse_static<Plan24000>(sm, tw, st);
         else fft_inverse(sm, tw, ca.pl, st);
+    }
+}
+
+// Grid rows of a chunk from Q: P[n] = Q[n % R][n / R] for n < Nmax, through a
+// shared-memory tile of kStageTm positions x R sub-transforms, so that both
+// the Q reads and the grid writes are consecutive.
+constexpr int kStageTm = 64;
+
+__global__ void __launch_bounds__(256) stage_power_kernel(ConsArgs ca, StageArgs a)
+{
+    __shared__ float tile[kStageTm * 20];
+    const int R = a.R, M = a.M;
+    const int m0 = blockIdx.x * kStageTm, tl = blockIdx.y, task = a.task0 + tl;
+    const int prn = task % a.n_prn, b = task / a.n_prn;
+    const float *Qt = a.Q + (size_t)tl * R * M;
+    for (int i = threadIdx.x; i < R * kStageTm; i += blockDim.x) {
+        const int c = i / kStageTm, mm = i - c * kStageTm, m = m0 + mm;
+        tile[mm * R + c] = (m < M) ? Qt[(size_t)c * M + m] : 0.0f;
+    }
+    __syncthreads();
+    float *row = ca.P + (size_t)prn * ca.prn_stride + (size_t)b * ca.bin_stride;
+    const long n0 = (long)R * m0;
+    for (int i = threadIdx.x; i < R * kStageTm; i += blockDim.x) {
+        const long n = n0 + i;
+        if (n < ca.Nmax) row[n] = tile[i];
     }
 }
 
@@ -520,10 +591,13 @@ static int launch_staged(const FftPlan *pl, const ConsArgs &ca, int n_tasks, cud
     const bool sp = Plan24000::matches(pl->k, pl->threads);
     int e;
     if ((e = sp ? set_stage_attr<MODE, 1>() : set_stage_attr<MODE, 0>())) return e;
+    if (pl->R > 20) return set_error(SDRG_ERR_ARG, "unsupported staged split %d", pl->R);
     StageArgs sa = {};
     sa.split = pl->split_dev; sa.X = ca.X; sa.code = ca.code;
     sa.R = pl->R; sa.M = pl->M; sa.n_prn = ca.n_prn - ca.prn0; sa.n_bin = ca.n_bin;
     sa.n_sum = ca.n_sum; sa.scale = ca.scale; sa.W = W;
+    // power grids: Q follows the w_tasks sub-spectra in the same scratch
+    sa.Q = MODE == 0 ? (float *)(W + (size_t)w_tasks * pl->L) : nullptr;
     for (int t0 = 0; t0 < n_tasks; t0 += w_tasks) {
         const int n = n_tasks - t0 < w_tasks ? n_tasks - t0 : w_tasks;
         for (int s = 0; s < ca.n_sum; ++s) {
@@ -544,6 +618,13 @@ static int launch_staged(const FftPlan *pl, const ConsArgs &ca, int n_tasks, cud
             else stage_ifft_kernel<MODE, 0><<<gi, pl->threads, pl->smem, st>>>(ca, sa);
             SDRG_CUDA(cudaGetLastError());
         }
+        if (MODE == 0) {
+            sa.task0 = t0;
+            const int mn = (ca.Nmax + pl->R - 1) / pl->R;    // positions holding n < Nmax
+            const dim3 gp((unsigned)((mn + kStageTm - 1) / kStageTm), (unsigned)n);
+            stage_power_kernel<<<gp, 256, 0, st>>>(ca, sa);
+            SDRG_CUDA(cudaGetLastError());
+        }
     }
     return SDRG_OK;
 }
@@ -555,6 +636,13 @@ static int launch_consumer(const FftPlan *pl, const ConsArgs &ca, int n_tasks, c
 {
     if (pl->R <= 8) return launch_cons<MODE>(pl, ca, n_tasks, st);
     return launch_staged<MODE>(pl, ca, n_tasks, st, W, w_tasks);
+}
+
+// bytes of a staged split's scratch for w_tasks tasks: the sub-spectra W and,
+// for power grids (MODE 0), the power accumulator Q behind them
+static size_t staged_bytes(const FftPlan *pl, int w_tasks, int mode)
+{
+    return (size_t)w_tasks * pl->L * (sizeof(float2) + (mode == 0 ? sizeof(float) : 0));
 }
 
 // scratch tasks for a staged split: about 256 MB of L2/HBM-resident sub-spectra
@@ -726,6 +814,8 @@ struct GroupState {
     float2 *X = nullptr;                // [n_bin][n_sum][R][M]
     float *P = nullptr;                 // [n_prn][n_bin][Nmax]
     float2 *W = nullptr;                // staged splits: [w_tasks][R][M] sub-spectra
+    float *Q = nullptr;                 // cluster splits, several sums: power accumulator
+    int Mq = 0;                         // its row length, ceil(Nmax / R)
     void *peak_parts = nullptr;         // partial peak reductions
     int w_tasks = 0;
     uint32_t *tab_dev = nullptr;        // phstep | ph0a | ph0b | (int) ix | nsplit
@@ -1000,7 +1090,7 @@ void sdr_search_code(const sdr_cpx_t *code_fft, double T, const sdr_buff_t *buff
     ca.scale = 1.0f / N / N; ca.Nmax = N; ca.prn_stride = 0; ca.bin_stride = N;
     ca.accumulate = 1; ca.P = P_d;
     const int wt = staged_chunk(pl, len_fds);
-    if (wt && (e = c.dev[5].reserve((size_t)wt * cb))) return;
+    if (wt && (e = c.dev[5].reserve(staged_bytes(pl, wt, 0)))) return;
     if ((e = launch_consumer<0>(pl, ca, len_fds, st, wt ? (float2 *)c.dev[5].ptr : nullptr, wt)))
         return;
     if (cudaMemcpyAsync(c.host[2].ptr, P_d, pb, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
@@ -1066,7 +1156,12 @@ sdrg_acq_plan_t *sdrg_acq_plan_new(const sdrg_acq_sig_t *sigs, int n_sig)
                   cudaMalloc(&G.P, (size_t)s.n_prn * s.len_fds * s.Nmax * sizeof(float)) == cudaSuccess;
         G.w_tasks = staged_chunk(G.pl, s.n_prn * s.len_fds);
         ok = ok && (!G.w_tasks ||
-                    cudaMalloc(&G.W, (size_t)G.w_tasks * L * sizeof(float2)) == cudaSuccess);
+                    cudaMalloc(&G.W, staged_bytes(G.pl, G.w_tasks, 0)) == cudaSuccess);
+        if (G.pl->R > 1 && G.pl->R <= 8 && s.n_sum > 1) {
+            G.Mq = (s.Nmax + G.pl->R - 1) / G.pl->R;
+            ok = ok && cudaMalloc(&G.Q, (size_t)s.n_prn * s.len_fds * G.pl->R * G.Mq *
+                                            sizeof(float)) == cudaSuccess;
+        }
         ok = ok && cudaMalloc(&G.peak_parts, peak_scratch_bytes(s.n_prn)) == cudaSuccess;
         G.tab_words = 2 * (size_t)s.len_fds + (size_t)s.len_fds * s.n_sum + 2 * (size_t)s.n_sum + s.len_fds;
         ok = ok && cudaMalloc(&G.tab_dev, G.tab_words * 4) == cudaSuccess &&
@@ -1130,6 +1225,7 @@ void sdrg_acq_plan_free(sdrg_acq_plan_t *plan)
         if (G.X) cudaFree(G.X);
         if (G.P) cudaFree(G.P);
         if (G.W) cudaFree(G.W);
+        if (G.Q) cudaFree(G.Q);
         if (G.peak_parts) cudaFree(G.peak_parts);
         if (G.tab_dev) cudaFree(G.tab_dev);
         if (G.tab_host) cudaFreeHost(G.tab_host);
@@ -1199,15 +1295,17 @@ int sdrg_fft_autotune(int L, int *R_out, int *threads_out, double *ms_out)
         if (shape_ok(L, R))
             for (int t : {256, 512}) cands.push_back({R, t});
     float2 *X = nullptr, *code = nullptr, *W = nullptr;
-    float *P = nullptr;
+    float *P = nullptr, *Q = nullptr;
     const size_t xb = (size_t)n_bin * n_sum * L * sizeof(float2);
     const size_t cb = (size_t)n_prn * L * sizeof(float2);
     const size_t pb = (size_t)n_prn * n_bin * Nmax * sizeof(float);
+    // the cluster splits' power accumulator, for the largest row set (R = 8)
+    const size_t qb = (size_t)n_prn * n_bin * (Nmax + 8) * sizeof(float);
     if ((e = alloc_fault("autotune"))) return e;
     if (cudaMalloc(&X, xb) != cudaSuccess || cudaMalloc(&code, cb) != cudaSuccess ||
-        cudaMalloc(&P, pb) != cudaSuccess) {
+        cudaMalloc(&P, pb) != cudaSuccess || cudaMalloc(&Q, qb) != cudaSuccess) {
         e = cuda_error(cudaGetLastError(), "autotune buffers");
-        cudaFree(X); cudaFree(code); cudaFree(P);
+        cudaFree(X); cudaFree(code); cudaFree(P); cudaFree(Q);
         return e;
     }
     cudaMemsetAsync(X, 0, xb, st);
@@ -1232,8 +1330,12 @@ int sdrg_fft_autotune(int L, int *R_out, int *threads_out, double *ms_out)
         ca.n_prn = n_prn; ca.n_bin = n_bin; ca.n_sum = n_sum; ca.prn0 = 0;
         ca.scale = 1.0f / L / L; ca.Nmax = Nmax;
         ca.prn_stride = (size_t)n_bin * Nmax; ca.bin_stride = Nmax; ca.accumulate = 0; ca.P = P;
+        if (pl->R > 1 && pl->R <= 8) {
+            ca.Q = Q;
+            ca.Mq = (Nmax + pl->R - 1) / pl->R;
+        }
         const int wt = staged_chunk(pl, n_prn * n_bin);
-        if (wt && !W && cudaMalloc(&W, (size_t)wt * L * sizeof(float2)) != cudaSuccess) {
+        if (wt && !W && cudaMalloc(&W, staged_bytes(pl, wt, 0)) != cudaSuccess) {
             e = cuda_error(cudaGetLastError(), "autotune scratch");
             break;
         }
@@ -1255,7 +1357,7 @@ int sdrg_fft_autotune(int L, int *R_out, int *threads_out, double *ms_out)
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     cudaStreamSynchronize(st);
-    cudaFree(X); cudaFree(code); cudaFree(P);
+    cudaFree(X); cudaFree(code); cudaFree(P); cudaFree(Q);
     if (W) cudaFree(W);
     if (e) return e;
     if (!bestR) return set_error(SDRG_ERR_ARG, "autotune: no runnable shape for length %d", L);
@@ -1339,7 +1441,7 @@ static int launch_run(sdrg_acq_plan_t *plan, Device *dev, const uint8_t *const *
         ca.code = G.code; ca.n_prn = s.n_prn; ca.n_bin = nb; ca.n_sum = ns; ca.prn0 = 0;
         ca.scale = 1.0f / s.L / s.L; ca.Nmax = s.Nmax;
         ca.prn_stride = (size_t)nb * s.Nmax; ca.bin_stride = s.Nmax;
-        ca.accumulate = 0; ca.P = G.P;
+        ca.accumulate = 0; ca.P = G.P; ca.Q = G.Q; ca.Mq = G.Mq;
         if ((e = prof_begin(plan, st, ev))) return e;
         if ((e = launch_consumer<0>(G.pl, ca, s.n_prn * nb, st, G.W, G.w_tasks))) return e;
         // a staged split launches a combine and an inverse pass per chunk and sum

@@ -318,10 +318,35 @@ def test_long_coherent_search_vs_oracle(gpu, ref):
             k += 1
 
 
-def test_search_code_staged_dropin(gpu, ref):
-    """The drop-in sdr_search_code at L = 480 000 (staged split, P in/out)."""
+def test_long_coherent_multi_chunk_vs_oracle(gpu, ref):
+    """A staged search of more tasks than one scratch chunk holds (4 PRNs x 20
+    bins = 80 (PRN, bin) tasks; a chunk of 480 000-point tasks holds 69): the
+    grids of PRNs with tasks in both chunks within 1e-4 of the reference's
+    sdr_search_code over the same sums, peaks identical, C/N0 within 0.1 dB."""
+    from pocketsdr_b200.acquire import AcqPlan
+    wl = synth.acq_long_48mhz(seed=13, prn_limit=4, n_sum=2,
+                              bins=np.arange(-500, 500, 50, dtype=np.float32))
+    wl.groups = wl.groups[:1]
+    g = wl.groups[0]
+    assert len(g.prns) * len(g.fds) == 80
+    cf = [synth.long_code_ffts(g)]
+    plan = AcqPlan([g], cf)
+    res = plan.run_host(wl.bufs, wl.ix)
+    G = plan.grid(0)
+    for p in (0, 3):                  # tasks of both chunks (bin-major order)
+        Pref = _oracle_group_grid(ref, g, cf[0][p], wl.bufs[g.buf], wl.ix[g.buf])
+        assert_power_close(G[p], Pref)
+        cn0, pk = ref.corr_max(Pref, g.Nmax, g.Nmax, len(g.fds), g.T)
+        assert_same_peak((res[p]["bin"], res[p]["offset"]), pk, Pref)
+        assert abs(float(res[p]["cn0"]) - cn0) < 0.1
+
+
+@pytest.mark.parametrize("n_bins", [3, 72])
+def test_search_code_staged_dropin(gpu, ref, n_bins):
+    """The drop-in sdr_search_code at L = 480 000 (staged split, P in/out,
+    accumulated onto the caller's values); 72 bins span two scratch chunks."""
     wl = synth.acq_long_48mhz(seed=9, prn_limit=1, n_sum=1,
-                              bins=np.array([-50, 0, 50], np.float32))
+                              bins=np.arange(n_bins, dtype=np.float32) * 50 - 50)
     g = wl.groups[0]
     cf = synth.long_code_ffts(g)[0]
     P = np.full((len(g.fds), g.L), 0.5, np.float32)
