@@ -257,6 +257,7 @@ struct CorrJobDev {
     int cpx, tap0, n;
     size_t iq_off;              // first sample of this job in the IQ scratch
     const char2 *code;          // bank [SDR_N_CODES][N]
+    int vec;                    // real code, 4-byte aligned bank: packed dot products
 };
 
 struct TapDev { int job, j, k, pad; };
@@ -308,6 +309,48 @@ __device__ __forceinline__ void half_main(const char2 *__restrict__ x, const cha
     }
 }
 
+// Packed form of half_main<false>, four samples per dp4a. sgn_mul8(x, c)
+// equals x * sgn(c) except for x = -128 with c < 0, where the reference's
+// byte negation wraps to -128 (x * sgn(c) = +128): those lanes are counted
+// and 256 taken off each, so the integer sums are identical.
+__device__ __forceinline__ void sgn_dot4(int &s, uint32_t x, uint32_t c)
+{
+    const uint32_t u = (c & 0x7f7f7f7fu) + 0x7f7f7f7fu;        // bit 7: c's low 7 bits != 0
+    const uint32_t pos = ((u & ~c) & 0x80808080u) >> 7;        // 1 in lanes with c > 0
+    const uint32_t neg = (c & 0x80808080u) >> 7;               // 1 in lanes with c < 0
+    const uint32_t t = x ^ 0x80808080u;                        // 0 in lanes with x = -128
+    const uint32_t v = (t & 0x7f7f7f7fu) + 0x7f7f7f7fu;
+    const uint32_t m = (~(v | t) & 0x80808080u) >> 7;          // 1 in lanes with x = -128
+    s = __dp4a((int)x, (int)pos, s);
+    s -= __dp4a((int)x, (int)neg, 0) + 256 * __dp4a((int)m, (int)neg, 0);
+}
+
+// logical word w (two char2 samples) of a stream starting at sample 2 w0 + odd
+// of a 4-byte aligned array; the second load of an odd stream covers its next
+// sample, which lies inside the array
+__device__ __forceinline__ uint32_t word_at(const uint32_t *b32, size_t w0, int odd, int w)
+{
+    const uint32_t a = __ldg(b32 + w0 + w);
+    return odd ? __funnelshift_r(a, __ldg(b32 + w0 + w + 1), 16) : a;
+}
+
+// the main part (main_len samples, a multiple of 16) of one half-dot with a
+// real code: x at sample xoff of xb, code at sample yoff of yb
+__device__ __forceinline__ void half_main_vec(const uint32_t *xb, size_t xoff,
+                                              const uint32_t *yb, size_t yoff, int main_len,
+                                              int &sr, int &si)
+{
+    const size_t xw0 = xoff >> 1, yw0 = yoff >> 1;
+    const int xo = (int)(xoff & 1), yo = (int)(yoff & 1);
+    const int H = main_len >> 2;                 // pairs of words p, p + H
+    for (int p = threadIdx.x; p < H; p += blockDim.x) {
+        const uint32_t x0 = word_at(xb, xw0, xo, p), x1 = word_at(xb, xw0, xo, p + H);
+        const uint32_t y0 = word_at(yb, yw0, yo, p), y1 = word_at(yb, yw0, yo, p + H);
+        sgn_dot4(sr, __byte_perm(x0, x1, 0x6420), __byte_perm(y0, y1, 0x6420));   // I lanes
+        sgn_dot4(si, __byte_perm(x0, x1, 0x7531), __byte_perm(y0, y1, 0x7531));   // Q lanes
+    }
+}
+
 // one block (128 threads) per tap: both half-dots of src/sdr_func.c:990-991
 __global__ void __launch_bounds__(128) tapb_kernel(const TapDev *__restrict__ taps,
                                                    const CorrJobDev *__restrict__ jobs,
@@ -327,7 +370,11 @@ __global__ void __launch_bounds__(128) tapb_kernel(const TapDev *__restrict__ ta
         const char2 *x = IQ + (h == 0 ? 0 : j);
         const char2 *y = bank + (h == 0 ? N - j : 0);
         int sr = 0, si = 0;
-        if (J.cpx) half_main<true>(x, y, (len / 16) * 16, sr, si);
+        if (J.vec)
+            half_main_vec((const uint32_t *)iq, J.iq_off + (h == 0 ? 0 : j),
+                          (const uint32_t *)J.code, (size_t)T.k * N + (h == 0 ? N - j : 0),
+                          (len / 16) * 16, sr, si);
+        else if (J.cpx) half_main<true>(x, y, (len / 16) * 16, sr, si);
         else half_main<false>(x, y, (len / 16) * 16, sr, si);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -453,6 +500,7 @@ extern "C" int sdrg_corr_batch(const sdrg_corr_job_t *jobs, int n_job, const uin
         d.cpx = J.cpx_code ? 1 : 0; d.tap0 = (int)tap; d.n = J.n;
         d.iq_off = iq_off;
         d.code = (const char2 *)J.code;
+        d.vec = !J.cpx_code && ((uintptr_t)J.code & 3) == 0;
         jh[i] = d;
         for (int t = 0; t < J.n; ++t) th[tap + t] = TapDev{i, jk[t].x, jk[t].y, 0};
         tap += J.n;

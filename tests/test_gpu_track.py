@@ -79,3 +79,54 @@ def test_corr_batch_l1ca_tracking_taps(orc):
         ref, refC = orc.corr_std(IQ, bank, s["coff"], pos, False)
         assert np.array_equal(corr[j, :len(pos)].view(np.uint32), ref.view(np.uint32)), j
         assert np.array_equal(Cb[j].view(np.uint32), refC.view(np.uint32)), j
+
+
+def test_corr_batch_arbitrary_code_bytes_and_alignment(orc):
+    """Real-code banks holding any int8 value (-128, 0, independent I and Q
+    bytes), half of them at a 2-byte offset (no 4-byte alignment: the
+    byte-wise path), odd lengths and tap offsets: bit-exact. The packed path's
+    one special case, a mixed sample of -128 against a negative code byte,
+    is checked to occur."""
+    torch = pytest.importorskip("torch")
+    from pocketsdr_b200 import track
+    rng = np.random.default_rng(71)
+    buf = rng.integers(0, 256, 90001, dtype=np.uint8)
+    specs, banks, keep = [], [], []
+    n_special = 0
+    for j in range(10):
+        N = int(rng.integers(1000, 20000)) | (j & 1)          # odd and even lengths
+        bank = rng.integers(-128, 128, (10 * N, 2), dtype=np.int8)
+        bank[rng.random(10 * N) < 0.1] = 0
+        bank[rng.random(10 * N) < 0.05, 0] = -128
+        n = int(rng.integers(3, 40))
+        pos = np.concatenate([[0.0, -1.5, 2.5], rng.uniform(-N, N, n - 3)])
+        spec = dict(buf=0, ix=int(rng.integers(0, len(buf))), N=N, fs=12e6,
+                    fc=float(rng.uniform(-5e6, 5e6)), phi=float(rng.uniform(-1, 1)),
+                    coff=float(rng.uniform(0, N)), cpx_code=False, pos=pos)
+        # device copy, at a 2-byte offset for odd j
+        off = j & 1
+        dev = torch.zeros((10 * N + 1) * 2, dtype=torch.int8, device="cuda")
+        dev[2 * off:2 * off + 20 * N] = torch.from_numpy(bank.reshape(-1)).cuda()
+        keep.append(dev)
+        spec["code_ptr"] = dev.data_ptr() + 2 * off
+        specs.append(spec)
+        banks.append(bank)
+        IQ = orc.mix_carr(buf, spec["ix"], N, spec["fs"], spec["fc"], spec["phi"])
+        n_special += int(np.sum((IQ.view(np.int8).reshape(-1, 2) == -128).any(1)))
+    assert n_special > 0
+    d_buf = torch.from_numpy(buf).cuda()
+    jobs = track.make_jobs(specs)
+    n = len(specs)
+    corr = torch.zeros(n * track.SDR_MAX_CORR * 2, dtype=torch.float32, device="cuda")
+    Cb = torch.zeros(n * 4, dtype=torch.float32, device="cuda")
+    track.corr_batch(jobs, [d_buf.data_ptr()], [len(buf)], corr.data_ptr(), Cb.data_ptr(),
+                     torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    corr = corr.cpu().numpy().view(np.complex64).reshape(n, track.SDR_MAX_CORR)
+    Cb = Cb.cpu().numpy().view(np.complex64).reshape(n, 2)
+    for j, (s, bank) in enumerate(zip(specs, banks)):
+        IQ = orc.mix_carr(buf, s["ix"], s["N"], s["fs"], s["fc"], s["phi"])
+        ref, refC = orc.corr_std(IQ, bank, s["coff"], s["pos"], False)
+        k = len(s["pos"])
+        assert np.array_equal(corr[j, :k].view(np.uint32), ref.view(np.uint32)), j
+        assert np.array_equal(Cb[j].view(np.uint32), refC.view(np.uint32)), j
