@@ -258,6 +258,7 @@ struct CorrJobDev {
     size_t iq_off;              // first sample of this job in the IQ scratch
     const char2 *code;          // bank [SDR_N_CODES][N]
     int vec;                    // real code, 4-byte aligned bank: packed dot products
+    int has128;                 // set by mixb_kernel: the window holds a -128 byte
 };
 
 struct TapDev { int job, j, k, pad; };
@@ -275,7 +276,7 @@ __device__ __forceinline__ char2 mix_byte_b(uint8_t byte, uint32_t phase, const 
 
 // grid (chunks, jobs): carrier wipe-off of every job's window into the IQ
 // scratch, with the reference's phase restart at the buffer wrap
-__global__ void mixb_kernel(const CorrJobDev *__restrict__ jobs, const char2 *__restrict__ ctab_g,
+__global__ void mixb_kernel(CorrJobDev *__restrict__ jobs, const char2 *__restrict__ ctab_g,
                             char2 *__restrict__ iq)
 {
     __shared__ char2 ctab[256];
@@ -283,13 +284,17 @@ __global__ void mixb_kernel(const CorrJobDev *__restrict__ jobs, const char2 *__
     __syncthreads();
     const CorrJobDev J = jobs[blockIdx.y];
     char2 *out = iq + J.iq_off;
+    bool m128 = false;
     for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < J.N; n += gridDim.x * blockDim.x) {
         int pos = J.ix + n;
         if (pos >= J.len) pos -= J.len;
         const uint32_t ph = n < J.nsplit ? J.p0a + J.step * (uint32_t)n
                                          : J.p0b + J.step * (uint32_t)(n - J.nsplit);
-        out[n] = mix_byte_b(__ldg(J.buf + pos), ph, ctab);
+        const char2 o = mix_byte_b(__ldg(J.buf + pos), ph, ctab);
+        out[n] = o;
+        m128 |= (o.x == -128) | (o.y == -128);
     }
+    if (m128) atomicOr(&jobs[blockIdx.y].has128, 1);
 }
 
 // sign-product partial sums of one half-dot over [0, main_len) (integer)
@@ -311,43 +316,67 @@ __device__ __forceinline__ void half_main(const char2 *__restrict__ x, const cha
 
 // Packed form of half_main<false>, four samples per dp4a. sgn_mul8(x, c)
 // equals x * sgn(c) except for x = -128 with c < 0, where the reference's
-// byte negation wraps to -128 (x * sgn(c) = +128): those lanes are counted
-// and 256 taken off each, so the integer sums are identical.
+// byte negation wraps to -128 (x * sgn(c) = +128): with FIX those lanes are
+// counted and 256 taken off each, so the integer sums are identical. Windows
+// without a -128 sample (flagged by mixb_kernel) skip the count.
+template <bool FIX>
 __device__ __forceinline__ void sgn_dot4(int &s, uint32_t x, uint32_t c)
 {
     const uint32_t u = (c & 0x7f7f7f7fu) + 0x7f7f7f7fu;        // bit 7: c's low 7 bits != 0
     const uint32_t pos = ((u & ~c) & 0x80808080u) >> 7;        // 1 in lanes with c > 0
     const uint32_t neg = (c & 0x80808080u) >> 7;               // 1 in lanes with c < 0
-    const uint32_t t = x ^ 0x80808080u;                        // 0 in lanes with x = -128
-    const uint32_t v = (t & 0x7f7f7f7fu) + 0x7f7f7f7fu;
-    const uint32_t m = (~(v | t) & 0x80808080u) >> 7;          // 1 in lanes with x = -128
     s = __dp4a((int)x, (int)pos, s);
-    s -= __dp4a((int)x, (int)neg, 0) + 256 * __dp4a((int)m, (int)neg, 0);
+    s -= __dp4a((int)x, (int)neg, 0);
+    if (FIX) {
+        const uint32_t t = x ^ 0x80808080u;                    // 0 in lanes with x = -128
+        const uint32_t v = (t & 0x7f7f7f7fu) + 0x7f7f7f7fu;
+        const uint32_t m = (~(v | t) & 0x80808080u) >> 7;      // 1 in lanes with x = -128
+        s -= 256 * __dp4a((int)m, (int)neg, 0);
+    }
 }
 
-// logical word w (two char2 samples) of a stream starting at sample 2 w0 + odd
-// of a 4-byte aligned array; the second load of an odd stream covers its next
-// sample, which lies inside the array
-__device__ __forceinline__ uint32_t word_at(const uint32_t *b32, size_t w0, int odd, int w)
+// The main part of one half-dot with a real code: H pairs of 32-bit words
+// (p, p + H), each word two char2 samples. xp / yp point at the aligned word
+// holding a stream's first sample; XO / YO: the stream starts at its second
+// sample, so each word is joined from two loads (the second one's first
+// sample is in the stream, so the load stays inside the array).
+template <int XO, int YO, bool FIX>
+__device__ __forceinline__ void half_vec(const uint32_t *__restrict__ xp,
+                                         const uint32_t *__restrict__ yp, int H, int &sr, int &si)
 {
-    const uint32_t a = __ldg(b32 + w0 + w);
-    return odd ? __funnelshift_r(a, __ldg(b32 + w0 + w + 1), 16) : a;
+    for (int p = threadIdx.x; p < H; p += blockDim.x) {
+        uint32_t x0 = __ldg(xp + p), x1 = __ldg(xp + p + H);
+        uint32_t y0 = __ldg(yp + p), y1 = __ldg(yp + p + H);
+        if (XO) {
+            x0 = __funnelshift_r(x0, __ldg(xp + p + 1), 16);
+            x1 = __funnelshift_r(x1, __ldg(xp + p + H + 1), 16);
+        }
+        if (YO) {
+            y0 = __funnelshift_r(y0, __ldg(yp + p + 1), 16);
+            y1 = __funnelshift_r(y1, __ldg(yp + p + H + 1), 16);
+        }
+        sgn_dot4<FIX>(sr, __byte_perm(x0, x1, 0x6420), __byte_perm(y0, y1, 0x6420));   // I lanes
+        sgn_dot4<FIX>(si, __byte_perm(x0, x1, 0x7531), __byte_perm(y0, y1, 0x7531));   // Q lanes
+    }
 }
 
-// the main part (main_len samples, a multiple of 16) of one half-dot with a
-// real code: x at sample xoff of xb, code at sample yoff of yb
+// x at sample xoff of xb, code at sample yoff of yb (both 4-byte aligned
+// arrays); main_len a multiple of 16 samples
 __device__ __forceinline__ void half_main_vec(const uint32_t *xb, size_t xoff,
                                               const uint32_t *yb, size_t yoff, int main_len,
-                                              int &sr, int &si)
+                                              bool fix, int &sr, int &si)
 {
-    const size_t xw0 = xoff >> 1, yw0 = yoff >> 1;
-    const int xo = (int)(xoff & 1), yo = (int)(yoff & 1);
-    const int H = main_len >> 2;                 // pairs of words p, p + H
-    for (int p = threadIdx.x; p < H; p += blockDim.x) {
-        const uint32_t x0 = word_at(xb, xw0, xo, p), x1 = word_at(xb, xw0, xo, p + H);
-        const uint32_t y0 = word_at(yb, yw0, yo, p), y1 = word_at(yb, yw0, yo, p + H);
-        sgn_dot4(sr, __byte_perm(x0, x1, 0x6420), __byte_perm(y0, y1, 0x6420));   // I lanes
-        sgn_dot4(si, __byte_perm(x0, x1, 0x7531), __byte_perm(y0, y1, 0x7531));   // Q lanes
+    const uint32_t *xp = xb + (xoff >> 1), *yp = yb + (yoff >> 1);
+    const int H = main_len >> 2;
+    switch ((int)(xoff & 1) | ((int)(yoff & 1) << 1) | (fix ? 4 : 0)) {
+    case 0: half_vec<0, 0, false>(xp, yp, H, sr, si); break;
+    case 1: half_vec<1, 0, false>(xp, yp, H, sr, si); break;
+    case 2: half_vec<0, 1, false>(xp, yp, H, sr, si); break;
+    case 3: half_vec<1, 1, false>(xp, yp, H, sr, si); break;
+    case 4: half_vec<0, 0, true>(xp, yp, H, sr, si); break;
+    case 5: half_vec<1, 0, true>(xp, yp, H, sr, si); break;
+    case 6: half_vec<0, 1, true>(xp, yp, H, sr, si); break;
+    default: half_vec<1, 1, true>(xp, yp, H, sr, si); break;
     }
 }
 
@@ -373,7 +402,7 @@ __global__ void __launch_bounds__(128) tapb_kernel(const TapDev *__restrict__ ta
         if (J.vec)
             half_main_vec((const uint32_t *)iq, J.iq_off + (h == 0 ? 0 : j),
                           (const uint32_t *)J.code, (size_t)T.k * N + (h == 0 ? N - j : 0),
-                          (len / 16) * 16, sr, si);
+                          (len / 16) * 16, J.has128 != 0, sr, si);
         else if (J.cpx) half_main<true>(x, y, (len / 16) * 16, sr, si);
         else half_main<false>(x, y, (len / 16) * 16, sr, si);
 #pragma unroll
@@ -501,6 +530,7 @@ extern "C" int sdrg_corr_batch(const sdrg_corr_job_t *jobs, int n_job, const uin
         d.iq_off = iq_off;
         d.code = (const char2 *)J.code;
         d.vec = !J.cpx_code && ((uintptr_t)J.code & 3) == 0;
+        d.has128 = 0;
         jh[i] = d;
         for (int t = 0; t < J.n; ++t) th[tap + t] = TapDev{i, jk[t].x, jk[t].y, 0};
         tap += J.n;
