@@ -485,6 +485,16 @@ def run_ours(args):
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
                                 "sample": desc, "single_thread": var["single_thread"],
                                 "no_sleep": var["no_sleep"], "sleeps": var["sleeps"]}
+    if rank == 0 and world == 1:
+        cf = cufft_pipeline_rate(wl)
+        if cf:
+            line["cufft_comparison"] = {
+                "cells_per_s": cf[0], "ms_per_step": cf[1], "ours_over_cufft": value / cf[0],
+                "cufft_inverse_only_ms": cf[2],
+                "ours_consumer_span_ms": cons_ms / args.steps,
+                "what": "timing only: torch.fft (cuFFT) forward FFTs of the blocks, code "
+                        "product, inverse FFTs, |y|^2 summed over the sums, per-PRN max; "
+                        "random data of the same shapes, FP32"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     plan.close()
@@ -492,6 +502,72 @@ def run_ours(args):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def cufft_pipeline_rate(wl, reps: int = 3):
+    """Timing comparison only, never the product path: the same search shapes
+    through torch.fft (cuFFT) and torch elementwise kernels on random data -
+    forward FFT of every (bin, sum) block, code product, inverse FFT, |y|^2 of
+    the Nmax kept offsets summed over the sums, per-PRN maximum. Returns
+    (cells/s, ms per search, ms of the search's inverse transforms alone), or
+    None when the spectra would exceed 4 GB."""
+    import torch
+    dev = torch.device("cuda")
+    if sum(len(g.fds) * g.n_sum * g.L * 8 for g in wl.groups) > (4 << 30):
+        return None
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(11)
+    work = [(g, torch.randn((len(g.fds) * g.n_sum, g.L), dtype=torch.complex64, device=dev,
+                            generator=gen),
+             torch.randn((len(g.prns), g.L), dtype=torch.complex64, device=dev, generator=gen))
+            for g in wl.groups]
+
+    def search():
+        peaks = []
+        for g, x, c in work:
+            nb, ns, L, Nmax = len(g.fds), g.n_sum, g.L, g.Nmax
+            X = torch.fft.fft(x).view(nb, ns, L)
+            pc = max(1, (1 << 30) // (nb * L * 8))          # PRNs per batch: ~1 GB of products
+            for p0 in range(0, len(g.prns), pc):
+                cc = c[p0:p0 + pc]
+                P = None
+                for s_ in range(ns):
+                    Y = torch.fft.ifft(X[:, s_][None] * cc[:, None])
+                    pw = torch.view_as_real(Y[..., :Nmax]).square().sum(-1)
+                    P = pw if P is None else P.add_(pw)
+                peaks.append(P.flatten(1).max(1))
+        return peaks
+
+    search()
+    torch.cuda.synchronize()
+    a_, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a_.record()
+    for _ in range(reps):
+        search()
+    b_.record()
+    torch.cuda.synchronize()
+    ms = a_.elapsed_time(b_) / reps
+    cells = sum(len(g.prns) * len(g.fds) * g.Nmax for g in wl.groups)
+    # the inverse transforms alone: as many as the search makes, same lengths
+    inv_ms = 0.0
+    for g, x, c in work:
+        n_inv = len(g.prns) * len(g.fds) * g.n_sum
+        bt = max(1, min(n_inv, (1 << 30) // (g.L * 8)))
+        Z = torch.randn((bt, g.L), dtype=torch.complex64, device=dev, generator=gen)
+        torch.fft.ifft(Z)
+        a_.record()
+        done = 0
+        while done < n_inv:
+            k = min(bt, n_inv - done)
+            torch.fft.ifft(Z[:k])
+            done += k
+        b_.record()
+        torch.cuda.synchronize()
+        inv_ms += a_.elapsed_time(b_)
+        del Z
+    del work
+    torch.cuda.empty_cache()
+    return cells / (ms / 1e3), ms, inv_ms
 
 
 def _measured_hbm():
