@@ -675,12 +675,34 @@ static inline uint32_t step_of(double step)
     return (uint32_t)(int)(step * 4294967296.0);
 }
 
+// Plan for a batch of n transforms of length N. The default split puts one
+// CTA of each of its R sub-transforms on an SM; a batch that would leave more
+// than half of the SMs idle (n R < SMs / 2) takes the largest finer cluster
+// split (up to 8) that keeps n R within two waves, so that the same work is
+// spread over more SMs (10 L6 channels of 96 000 points: 4 -> 8 ways, 110 K ->
+// 145 K channel-epochs/s). A schedule set for N is kept as it is.
+static const FftPlan *plan_for_jobs(int N, int n)
+{
+    const FftPlan *pl = get_plan(N);
+    if (!pl || pl->R > 8 || sdrg_fft_schedule_get(N, nullptr, nullptr)) return pl;
+    Device *dev;
+    if (ensure_device(&dev)) return pl;
+    const long sms = dev->sm_count;
+    if (2L * n * pl->R >= sms) return pl;
+    for (int R : {8, 6, 5, 4, 3, 2}) {
+        if (R <= pl->R) break;
+        if ((long)n * R > 2 * sms || !shape_ok(N, R)) continue;
+        if (const FftPlan *p2 = get_plan_shaped(N, R, 0)) return p2;
+    }
+    return pl;
+}
+
 // Common body of the drop-in FFT correlator calls. iq_dev holds N mixed
 // samples on the device; code_host is the natural-order conjugated code DFT.
 static int corr_fft_device(const char2 *iq_dev, const sdr_cpx_t *code_host, int N,
                            sdr_cpx_t *corr_host)
 {
-    const FftPlan *pl = get_plan(N);
+    const FftPlan *pl = plan_for_jobs(N, 1);
     if (!pl) return tctx().error;
     Device *dev;
     int e;
@@ -749,7 +771,7 @@ size_t corr_job_scratch(int N)
 int corr_job_device(const uint8_t *buf, int len, const uint32_t *tab_dev, int N,
                     const float2 *code_nat, float2 *corr, void *scratch, cudaStream_t st)
 {
-    const FftPlan *pl = get_plan(N);
+    const FftPlan *pl = plan_for_jobs(N, 1);
     if (!pl) return tctx().error ? tctx().error : SDRG_ERR_ARG;
     Device *dev;
     int e;
@@ -778,7 +800,7 @@ int corr_job_device(const uint8_t *buf, int len, const uint32_t *tab_dev, int N,
 int corr_jobs_device(const uint8_t *buf, int len, const uint32_t *tab_dev, int n, int N,
                      const float2 *code_nat, float2 *corr, void *scratch, cudaStream_t st)
 {
-    const FftPlan *pl = get_plan(N);
+    const FftPlan *pl = plan_for_jobs(N, n);
     if (!pl) return tctx().error ? tctx().error : SDRG_ERR_ARG;
     if (pl->R > 8) return set_error(SDRG_ERR_ARG, "batched jobs need a cluster split (N=%d)", N);
     Device *dev;
@@ -1026,7 +1048,7 @@ void sdr_search_code(const sdr_cpx_t *code_fft, double T, const sdr_buff_t *buff
                   buff ? buff->N : 0);
         return;
     }
-    const FftPlan *pl = get_plan(N);
+    const FftPlan *pl = plan_for_jobs(N, len_fds);
     if (!pl) return;
     int e;
     Device *dev;
