@@ -319,9 +319,11 @@ __global__ void __launch_bounds__(512, 1) cons_kernel(ConsArgs a)
 
 // ---------------------------------------------------------------------------
 // staged consumer for splits R > 8 (L up to 20 * M, e.g. 480 000 = 20 x 24 000):
-// the combine writes the R sub-spectra w_c of a chunk of tasks to an
-// L2-resident scratch W, then R independent CTAs per task run the length-M
-// inverse transforms. Same arithmetic as cons_kernel's cluster exchange.
+// the combine writes the R sub-spectra w_c of a chunk of tasks to a scratch W
+// in global memory (about 256 MB per chunk: it passes through HBM, the L2
+// holding what is in flight), then R independent CTAs per task run the
+// length-M inverse transforms. Same arithmetic as cons_kernel's cluster
+// exchange.
 // ---------------------------------------------------------------------------
 struct StageArgs {
     const float2 *split, *X, *code;
@@ -645,7 +647,7 @@ static size_t staged_bytes(const FftPlan *pl, int w_tasks, int mode)
     return (size_t)w_tasks * pl->L * (sizeof(float2) + (mode == 0 ? sizeof(float) : 0));
 }
 
-// scratch tasks for a staged split: about 256 MB of L2/HBM-resident sub-spectra
+// scratch tasks for a staged split: about 256 MB of sub-spectra per chunk
 static int staged_chunk(const FftPlan *pl, int n_tasks)
 {
     if (pl->R <= 8) return 0;
