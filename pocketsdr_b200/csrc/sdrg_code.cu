@@ -192,14 +192,15 @@ int res_code_device(const int8_t *ci, const int8_t *cq, int len_code, int n_code
 
 int code_fft_device(const int8_t *ci, const int8_t *cq, int len_code, int n_code, double T,
                     double coff, double fs, int N, int L, int natural, float2 *out,
-                    cudaStream_t st)
+                    cudaStream_t st, const FftPlan *pl_in)
 {
     if (!ci || !out || len_code <= 0 || n_code <= 0 || N <= 0 || L < N || !(T > 0) ||
         !(fs > 0))
         return set_error(SDRG_ERR_ARG, "gen_code_fft: bad arguments (len_code=%d n_code=%d "
                          "N=%d L=%d)", len_code, n_code, N, L);
-    const FftPlan *pl = get_plan(L);
+    const FftPlan *pl = pl_in ? pl_in : get_plan(L);
     if (!pl) return tctx().error ? tctx().error : SDRG_ERR_ARG;
+    if (pl->L != L) return set_error(SDRG_ERR_ARG, "gen_code_fft: plan length %d != L=%d", pl->L, L);
     const double dx = (double)len_code / T / fs;
     const double cf = coff * fs;
     int e;

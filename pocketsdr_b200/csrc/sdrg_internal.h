@@ -116,9 +116,11 @@ int mix_cpx_device(const sdr_cpx_t *buff, int len_buff, int ix, int N, double fs
 int res_code_device(const int8_t *ci, const int8_t *cq, int len_code, int n_code, double T,
                     double coff, double fs, int N, int Nz, int n_bank, char2 *out,
                     cudaStream_t st);
+// natural = 0 writes the permuted layout of plan pl (null: the length's
+// default plan), the one a consumer using pl reads
 int code_fft_device(const int8_t *ci, const int8_t *cq, int len_code, int n_code, double T,
                     double coff, double fs, int N, int L, int natural, float2 *out,
-                    cudaStream_t st);
+                    cudaStream_t st, const FftPlan *pl = nullptr);
 
 // One correlation job on device data (sdrg_search.cu): sdr_mix_carr of the
 // window [ix, ix + N) of circular buffer buf (len samples) at (fs, fc, phi)

@@ -1161,7 +1161,7 @@ sdrg_acq_plan_t *sdrg_acq_plan_new(const sdrg_acq_sig_t *sigs, int n_sig)
             sdrg_acq_plan_free(plan);
             return nullptr;
         }
-        G.pl = get_plan(s.L);
+        G.pl = plan_for_jobs(s.L, s.n_prn * s.len_fds);
         if (!G.pl) { sdrg_acq_plan_free(plan); return nullptr; }
         G.fds.assign(s.fds, s.fds + s.len_fds);
         G.sig.fds = nullptr;
@@ -1295,7 +1295,7 @@ int sdrg_acq_set_codes(sdrg_acq_plan_t *plan, int g, const int8_t *code_I_dev,
     cudaStream_t st = (cudaStream_t)stream;
     if (!st && (e = thread_stream(&st))) return e;
     return code_fft_device(code_I_dev, code_Q_dev, len_code, G.sig.n_prn, T, coff, G.sig.fs, N,
-                           G.sig.L, 0, G.code, st);
+                           G.sig.L, 0, G.code, st, G.pl);
 }
 
 // Times the consumer (code product + inverse FFT + power accumulation) of a

@@ -9,10 +9,13 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def test_search_op_vs_reference(gpu, ref):
+@pytest.mark.parametrize("n_prn", [4, 1])
+def test_search_op_vs_reference(gpu, ref, n_prn):
+    """n_prn = 1: 21 (PRN, bin) tasks, few enough for the plan to take a finer
+    split of its 48 000-point transforms (8 ways), codes laid out for it."""
     torch = pytest.importorskip("torch")
     from pocketsdr_b200 import codes, ops, synth  # noqa: F401
-    wl = synth.acq_multi_24mhz(seed=3, prn_limit=4, t_sum=2e-3, sigs=(("L1CA", 0),))
+    wl = synth.acq_multi_24mhz(seed=3, prn_limit=n_prn, t_sum=2e-3, sigs=(("L1CA", 0),))
     g = wl.groups[0]
     buf = wl.bufs[g.buf]
     chips = np.stack([codes.gen_code(g.sig, p) for p in g.prns])
