@@ -51,6 +51,25 @@ UNIT = "cells/s"
 FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12   # 148 SM x 128 FP32 lanes x FMA at 1965 MHz
 
 
+def _cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
+def emit(line: dict) -> None:
+    """Prints the one JSON result line; a CPU baseline names the host's CPU."""
+    if isinstance(line.get("cpu_baseline"), dict):
+        line["cpu_baseline"].setdefault("cpu_model", _cpu_model())
+    print(json.dumps(line), flush=True)
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -319,7 +338,7 @@ def run_reference(args):
         line = _reference_other(args)
         if line is None:
             raise SystemExit(f"unknown workload {args.workload}")
-        print(json.dumps(line), flush=True)
+        emit(line)
         return 0
     wl = make_workload(args.workload, 2)
     vals = []
@@ -337,7 +356,7 @@ def run_reference(args):
             "impl": "reference",
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": desc},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
+    emit(line)
     return 0
 
 
@@ -494,7 +513,7 @@ def run_ours(args):
                         "product, inverse FFTs, |y|^2 summed over the sums, per-PRN max; "
                         "random data of the same shapes, FP32"}
     if rank == 0:
-        print(json.dumps(line), flush=True)
+        emit(line)
     plan.close()
     if dist:
         dist.barrier()
@@ -771,7 +790,7 @@ def run_track(args):
         line["cpu_baseline"] = {"value": rate, "unit": "channel-epochs/s", "cores": cores,
                                 "kind": kind, "sample": desc}
     if rank == 0:
-        print(json.dumps(line), flush=True)
+        emit(line)
     return 0
 
 
@@ -956,7 +975,7 @@ def run_refine(args):
                             + 1 + 2 * len(models)) * args.steps
     acq.profile(False)
     if rank == 0:
-        print(json.dumps(line), flush=True)
+        emit(line)
     plan.close()
     acq.close()
     return 0
@@ -1112,7 +1131,7 @@ def run_ingest(args):
         line["cpu_baseline"] = {"value": rate, "unit": "samples/s", "cores": cores, "kind": kind,
                                 "sample": desc}
     if rank == 0:
-        print(json.dumps(line), flush=True)
+        emit(line)
     ing.close()
     return 0
 
@@ -1181,7 +1200,7 @@ def run_search_batch(args):
         line["cpu_baseline"] = {"value": rate / cells_per_search, "unit": "searches/s",
                                 "cores": cores, "kind": kind, "sample": desc}
     if rank == 0:
-        print(json.dumps(line), flush=True)
+        emit(line)
     return 0
 
 
@@ -1299,7 +1318,7 @@ def run_l6(args):
         line["cpu_baseline"] = {"value": rate, "unit": "channel-epochs/s", "cores": cores,
                                 "kind": kind, "sample": desc}
     if rank == 0:
-        print(json.dumps(line), flush=True)
+        emit(line)
     return 0
 
 
