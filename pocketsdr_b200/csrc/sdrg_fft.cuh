@@ -510,10 +510,9 @@ __device__ __forceinline__ void s_inner_warp(float2 *sm, const float2 *twp)
             float2 v[R];
 #pragma unroll
             for (int j = 0; j < R; ++j) v[j] = p[j * S];
-            if (S > 1) {
-#pragma unroll
-                for (int j = 1; j < R; ++j) v[j] = cmul(v[j], cconj(twp[(j - 1) * S + i]));
-            }
+            // powers of the first twiddle by repeated products: one table
+            // load instead of R - 1
+            if (S > 1) apply_tw<R>(v, cconj(twp[i]));
             Dft<R, 1>::run(v);
 #pragma unroll
             for (int j = 0; j < R; ++j) p[j * S] = v[j];
