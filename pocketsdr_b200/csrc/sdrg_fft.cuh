@@ -495,27 +495,48 @@ __device__ __forceinline__ void s_pass0_store(const float2 *sm, const float2 *tw
 // M / W consecutive elements (W warps): the passes after the first DIF pass
 // (the last DIT passes) never reach outside a block of Ls_1 = M / R0 points,
 // so when R0 equals the warp count each warp owns one such block.
+// one butterfly of an inner inverse pass at p (stride S, index i in its block)
+template <int R, int S>
+__device__ __forceinline__ void s_bfly_inv(float2 *p, const float2 *twp, int i)
+{
+    float2 v[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) v[j] = p[j * S];
+    // powers of the first twiddle by repeated products: one table load
+    // instead of R - 1
+    if (S > 1) apply_tw<R>(v, cconj(twp[i]));
+    Dft<R, 1>::run(v);
+#pragma unroll
+    for (int j = 0; j < R; ++j) p[j * S] = v[j];
+}
+
 template <int R, int S, int REG>
 __device__ __forceinline__ void s_inner_warp(float2 *sm, const float2 *twp)
 {
     constexpr int NB = REG / R, LS = R * S, IT = (NB + 31) / 32;
+    static_assert(REG % LS == 0, "a warp's region holds whole blocks");
     const int lane = threadIdx.x & 31;
     float2 *base = sm + (threadIdx.x >> 5) * REG;
+    if constexpr (S > 1 && S <= 16) {
+        // one block per half-warp, lane i < S: the half-warp's R accesses
+        // are S consecutive elements, in distinct banks (lanes taken in order
+        // put two blocks LS apart into one half-warp, whose elements collided
+        // in the banks: 1.9x the wavefronts at R = 10, S = 15)
+        constexpr int NBLK = REG / LS, IH = (NBLK + 1) / 2;
+        const int i = lane & 15;
 #pragma unroll
-    for (int it = 0; it < IT; ++it) {
-        const int b = lane + it * 32;
-        if (b < NB) {
-            const int blk = b / S, i = b - blk * S;
-            float2 *p = base + blk * LS + i;
-            float2 v[R];
+        for (int it = 0; it < IH; ++it) {
+            const int blk = 2 * it + (lane >> 4);
+            if (blk < NBLK && i < S) s_bfly_inv<R, S>(base + blk * LS + i, twp, i);
+        }
+    } else {
 #pragma unroll
-            for (int j = 0; j < R; ++j) v[j] = p[j * S];
-            // powers of the first twiddle by repeated products: one table
-            // load instead of R - 1
-            if (S > 1) apply_tw<R>(v, cconj(twp[i]));
-            Dft<R, 1>::run(v);
-#pragma unroll
-            for (int j = 0; j < R; ++j) p[j * S] = v[j];
+        for (int it = 0; it < IT; ++it) {
+            const int b = lane + it * 32;
+            if (b < NB) {
+                const int blk = b / S, i = b - blk * S;
+                s_bfly_inv<R, S>(base + blk * LS + i, twp, i);
+            }
         }
     }
 }
