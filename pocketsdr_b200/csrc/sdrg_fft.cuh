@@ -517,11 +517,12 @@ __device__ __forceinline__ void s_inner_warp(float2 *sm, const float2 *twp)
     static_assert(REG % LS == 0, "a warp's region holds whole blocks");
     const int lane = threadIdx.x & 31;
     float2 *base = sm + (threadIdx.x >> 5) * REG;
-    if constexpr (S > 1 && S <= 16) {
+    if constexpr (S >= 8 && S <= 16) {
         // one block per half-warp, lane i < S: the half-warp's R accesses
         // are S consecutive elements, in distinct banks (lanes taken in order
         // put two blocks LS apart into one half-warp, whose elements collided
-        // in the banks: 1.9x the wavefronts at R = 10, S = 15)
+        // in the banks: 1.9x the wavefronts at R = 10, S = 15). Strides of 8
+        // to 16 keep at least half of the lanes busy.
         constexpr int NBLK = REG / LS, IH = (NBLK + 1) / 2;
         const int i = lane & 15;
 #pragma unroll
