@@ -406,20 +406,58 @@ struct StoreComplexRt {
     __device__ __forceinline__ void operator()(int m, float2 y, int) const { row[R * m + c] = y; }
 };
 
-// grid (R, chunk tasks): CTA c of a task inverts w_c
-template <int MODE, int SP>
-__global__ void __launch_bounds__(512, 1) stage_ifft_kernel(ConsArgs ca, StageArgs a)
+// ---- bulk copies through the TMA engine (cp.async.bulk, mbarrier) ----------
+// Set when a CTA gave up waiting for a bulk copy (a bound, never reached in
+// normal operation); the synchronous entry points report and clear it.
+__device__ int g_stage_wait_err = 0;
+constexpr long long kBulkWaitCycles = 4000000000LL;     // about 2 s at 1.97 GHz
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
 {
-    extern __shared__ float2 smem[];
-    float2 *sm = smem;
-    float2 *tw = smem + ca.pl.M;
-    const int M = SP ? Plan24000::M : ca.pl.M;
-    const int c = blockIdx.x, tl = blockIdx.y, task = a.task0 + tl;
-    const int prn = task % a.n_prn, b = task / a.n_prn;
-    load_twiddles(tw, ca.tw, ca.pl.twtot);
-    const float2 *src = a.W + ((size_t)tl * a.R + c) * M;
-    // W exceeds L2: UL loads per thread in flight before the shared-memory
-    // stores, so the copy runs at HBM bandwidth rather than latency
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;"
+                 ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// bytes (a multiple of 16) from global src to shared dst, both 16-byte
+// aligned, completing on bar
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32_t bytes,
+                                              uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
+                 "[%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+// waits for phase `parity` of bar to complete, at most kBulkWaitCycles
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+{
+    const long long t0 = clock64();
+    for (;;) {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred p;\n\t"
+                     "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+        if (done) return true;
+        if (clock64() - t0 > kBulkWaitCycles) return false;
+    }
+}
+
+// W exceeds L2: UL loads per thread in flight before the shared-memory stores,
+// so the copy runs at HBM bandwidth rather than latency
+__device__ __forceinline__ void load_plain(float2 *sm, const float2 *src, int M)
+{
     constexpr int UL = 8;
     if ((M & 1) == 0) {
         const float4 *s4 = (const float4 *)src;
@@ -441,7 +479,55 @@ __global__ void __launch_bounds__(512, 1) stage_ifft_kernel(ConsArgs ca, StageAr
     } else {
         for (int i = threadIdx.x; i < M; i += blockDim.x) sm[i] = __ldg(src + i);
     }
-    __syncthreads();
+}
+
+// grid (R, chunk tasks): CTA c of a task inverts w_c
+template <int MODE, int SP>
+__global__ void __launch_bounds__(512, 1) stage_ifft_kernel(ConsArgs ca, StageArgs a)
+{
+    extern __shared__ float2 smem[];
+    float2 *sm = smem;
+    float2 *tw = smem + ca.pl.M;
+    const int M = SP ? Plan24000::M : ca.pl.M;
+    const int c = blockIdx.x, tl = blockIdx.y, task = a.task0 + tl;
+    const int prn = task % a.n_prn, b = task / a.n_prn;
+    const float2 *src = a.W + ((size_t)tl * a.R + c) * M;
+    bool copied = false;
+    if constexpr (SP == 1) {
+        // compile-time plan: passes 3..1 run warp by warp on REG points each,
+        // so each warp's region is brought in by its own bulk copy and the warp
+        // starts as soon as that region has landed (the twiddles load meanwhile)
+        constexpr int NW = Plan24000::R0, REG = Plan24000::M / NW;
+        constexpr uint32_t RB = REG * sizeof(float2);
+        static_assert(RB % 16 == 0, "bulk copies move multiples of 16 bytes");
+        __shared__ __align__(8) uint64_t bar[NW];
+        if (((smem_u32(sm) | (uint32_t)(uintptr_t)src) & 15u) == 0) {
+            const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+            if (threadIdx.x == 0) {
+                for (int k = 0; k < NW; ++k) mbar_init(&bar[k], 1);
+                mbar_init_fence();
+            }
+            __syncthreads();
+            if (lane == 0) {
+                mbar_expect_tx(&bar[w], RB);
+                bulk_copy_g2s(sm + w * REG, src + w * REG, RB, &bar[w]);
+            }
+            load_twiddles(tw, ca.tw, ca.pl.twtot);
+            __syncthreads();
+            if (!mbar_wait(&bar[w], 0)) {
+                // give up on the bound: record it, wait (bounded) for the copy in
+                // flight before the region is touched, and keep every barrier
+                if (lane == 0) atomicOr(&g_stage_wait_err, 1);
+                mbar_wait(&bar[w], 0);
+            }
+            copied = true;
+        }
+    }
+    if (!copied) {
+        load_twiddles(tw, ca.tw, ca.pl.twtot);
+        load_plain(sm, src, M);
+        __syncthreads();
+    }
     if (MODE == 0) {
         const float *row = ca.P + (size_t)prn * ca.prn_stride + (size_t)b * ca.bin_stride;
         StorePowerQ st{a.Q + ((size_t)tl * a.R + c) * M, row, c, a.R, ca.Nmax,
@@ -575,9 +661,13 @@ static int set_stage_attr()
 {
     static bool done = false;
     if (!done) {
+        // the per-block limit covers the kernel's static shared memory too
+        // (its bulk-copy barriers)
+        cudaFuncAttributes fa;
+        SDRG_CUDA(cudaFuncGetAttributes(&fa, stage_ifft_kernel<MODE, SP>));
         SDRG_CUDA(cudaFuncSetAttribute(stage_ifft_kernel<MODE, SP>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)(g_smem_limit())));
+                                       (int)(g_smem_limit() - fa.sharedSizeBytes)));
         done = true;
     }
     return SDRG_OK;
@@ -677,6 +767,21 @@ static inline uint32_t step_of(double step)
     return (uint32_t)(int)(step * 4294967296.0);
 }
 
+// After a synchronous call that ran a staged split: reports (and clears) a
+// bulk-copy wait that reached its bound in stage_ifft_kernel.
+static int stage_wait_check(const FftPlan *pl)
+{
+    if (!pl || pl->R <= 8) return SDRG_OK;
+    int v = 0;
+    cudaError_t ce = cudaMemcpyFromSymbol(&v, g_stage_wait_err, sizeof(int));
+    if (ce != cudaSuccess) return cuda_error(ce, "staged FFT status");
+    if (!v) return SDRG_OK;
+    const int z = 0;
+    cudaMemcpyToSymbol(g_stage_wait_err, &z, sizeof(int));
+    return set_error(SDRG_ERR_CUDA, "staged FFT: a bulk copy into shared memory did not "
+                     "complete within its bound; results of that call are not valid");
+}
+
 // Plan for a batch of n transforms of length N. The default split puts one
 // CTA of each of its R sub-transforms on an SM; a batch that would leave more
 // than half of the SMs idle (n R < SMs / 2) takes the largest finer cluster
@@ -741,6 +846,7 @@ static int corr_fft_device(const char2 *iq_dev, const sdr_cpx_t *code_host, int 
         return e;
     SDRG_CUDA(cudaMemcpyAsync(c.host[0].ptr, Y, cb, cudaMemcpyDeviceToHost, st));
     SDRG_CUDA(cudaStreamSynchronize(st));
+    if ((e = stage_wait_check(pl))) return e;
     memcpy(corr_host, c.host[0].ptr, cb);
     return SDRG_OK;
 }
@@ -1122,6 +1228,7 @@ void sdr_search_code(const sdr_cpx_t *code_fft, double T, const sdr_buff_t *buff
         cuda_error(cudaGetLastError(), "sdr_search_code D2H");
         return;
     }
+    if (stage_wait_check(pl)) return;           // P unchanged, error recorded
     memcpy(P, c.host[2].ptr, pb);
 }
 
@@ -1601,6 +1708,7 @@ int sdrg_acq_run_host(sdrg_acq_plan_t *plan, const uint8_t *const *if_host, cons
                 cudaStreamSynchronize(st) != cudaSuccess))
         e = cuda_error(cudaGetLastError(), "sdrg_acq_run_host D2H");
     cudaStreamSynchronize(st);
+    for (size_t gi = 0; gi < plan->g.size() && !e; ++gi) e = stage_wait_check(plan->g[gi].pl);
     for (auto p : bufs) if (p) cudaFree(p);
     if (res_dev) cudaFree(res_dev);
     return e;
