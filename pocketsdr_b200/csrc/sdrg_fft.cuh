@@ -495,22 +495,29 @@ __device__ __forceinline__ void s_pass0_store(const float2 *sm, const float2 *tw
 // M / W consecutive elements (W warps): the passes after the first DIF pass
 // (the last DIT passes) never reach outside a block of Ls_1 = M / R0 points,
 // so when R0 equals the warp count each warp owns one such block.
-// one butterfly of an inner inverse pass at p (stride S, index i in its block)
-template <int R, int S>
-__device__ __forceinline__ void s_bfly_inv(float2 *p, const float2 *twp, int i)
+// one butterfly of an inner pass at p (stride S, index i in its block):
+// forward DIF (DFT, then twiddles) or inverse DIT (conjugate twiddles, then
+// backward DFT)
+template <int R, int S, bool FWD>
+__device__ __forceinline__ void s_bfly(float2 *p, const float2 *twp, int i)
 {
     float2 v[R];
 #pragma unroll
     for (int j = 0; j < R; ++j) v[j] = p[j * S];
     // powers of the first twiddle by repeated products: one table load
     // instead of R - 1
-    if (S > 1) apply_tw<R>(v, cconj(twp[i]));
-    Dft<R, 1>::run(v);
+    if (FWD) {
+        Dft<R, -1>::run(v);
+        if (S > 1) apply_tw<R>(v, twp[i]);
+    } else {
+        if (S > 1) apply_tw<R>(v, cconj(twp[i]));
+        Dft<R, 1>::run(v);
+    }
 #pragma unroll
     for (int j = 0; j < R; ++j) p[j * S] = v[j];
 }
 
-template <int R, int S, int REG>
+template <int R, int S, int REG, bool FWD = false>
 __device__ __forceinline__ void s_inner_warp(float2 *sm, const float2 *twp)
 {
     constexpr int NB = REG / R, LS = R * S, IT = (NB + 31) / 32;
@@ -528,7 +535,7 @@ __device__ __forceinline__ void s_inner_warp(float2 *sm, const float2 *twp)
 #pragma unroll
         for (int it = 0; it < IH; ++it) {
             const int blk = 2 * it + (lane >> 4);
-            if (blk < NBLK && i < S) s_bfly_inv<R, S>(base + blk * LS + i, twp, i);
+            if (blk < NBLK && i < S) s_bfly<R, S, FWD>(base + blk * LS + i, twp, i);
         }
     } else {
 #pragma unroll
@@ -536,10 +543,29 @@ __device__ __forceinline__ void s_inner_warp(float2 *sm, const float2 *twp)
             const int b = lane + it * 32;
             if (b < NB) {
                 const int blk = b / S, i = b - blk * S;
-                s_bfly_inv<R, S>(base + blk * LS + i, twp, i);
+                s_bfly<R, S, FWD>(base + blk * LS + i, twp, i);
             }
         }
     }
+}
+
+// Forward transform with a compile-time plan (same contract as fft_forward):
+// pass 0 over the CTA fused with load(), then, with R0 = warps per CTA, passes
+// 1..3 warp by warp on the independent blocks of M / R0 points. Ends with a
+// barrier.
+template <class P, class Load>
+__device__ __forceinline__ void fft_forward_static(float2 *sm, const float2 *tw, Load &load)
+{
+    static_assert(P::R0 * 32 == P::NT, "one warp per block after the first pass");
+    constexpr int REG = P::M / P::R0;
+    dif_pass0_load<P::R0>(sm, P::M, tw + P::O0, load, threadIdx.x, P::NT);
+    __syncthreads();
+    s_inner_warp<P::R1, P::S1, REG, true>(sm, tw + P::O1);
+    __syncwarp();
+    s_inner_warp<P::R2, P::S2, REG, true>(sm, tw + P::O2);
+    __syncwarp();
+    s_inner_warp<P::R3, P::S3, REG, true>(sm, tw + P::O3);
+    __syncthreads();
 }
 
 // Inverse transform with a compile-time plan (same contract as fft_inverse).

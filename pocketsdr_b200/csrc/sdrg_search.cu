@@ -98,7 +98,7 @@ struct LoadIQ {
     }
 };
 
-template <int MODE>
+template <int MODE, int SP>
 __global__ void __launch_bounds__(512, 1) fwd_kernel(FwdArgs a)
 {
     extern __shared__ float2 smem[];
@@ -121,10 +121,12 @@ __global__ void __launch_bounds__(512, 1) fwd_kernel(FwdArgs a)
         const int w = a.ix_per_bin ? b : s;
         LoadIF ld{a.buf, a.buf_len, a.ix[w], a.nsplit[w], a.R, r, a.phstep[b],
                   a.ph0a[b], a.ph0b[bs], ctab, a.cscale};
-        fft_forward(sm, tw, a.pl, ld);
+        if constexpr (SP == 1) fft_forward_static<Plan24000>(sm, tw, ld);
+        else fft_forward(sm, tw, a.pl, ld);
     } else {
         LoadIQ ld{a.iq, a.R, r, a.cscale};
-        fft_forward(sm, tw, a.pl, ld);
+        if constexpr (SP == 1) fft_forward_static<Plan24000>(sm, tw, ld);
+        else fft_forward(sm, tw, a.pl, ld);
     }
     // store F_r (digit-reversed order) contiguously
     float2 *dst = a.X + ((size_t)bs * a.R + r) * a.pl.M;
@@ -587,14 +589,17 @@ __global__ void perm_code_kernel(const float2 *code_nat, const int *kperm, int M
 template <int MODE>
 static int launch_fwd(const FftPlan *pl, const FwdArgs &a, int n_blocks, cudaStream_t st)
 {
-    static bool attr_set[2] = {false, false};
-    if (!attr_set[MODE]) {
-        SDRG_CUDA(cudaFuncSetAttribute(fwd_kernel<MODE>,
+    static bool attr_set[2][2] = {{false, false}, {false, false}};
+    // the compile-time 24 000-point plan where it applies
+    const int sp = Plan24000::matches(pl->k, pl->threads) ? 1 : 0;
+    if (!attr_set[MODE][sp]) {
+        SDRG_CUDA(cudaFuncSetAttribute(sp ? fwd_kernel<MODE, 1> : fwd_kernel<MODE, 0>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)(g_smem_limit())));
-        attr_set[MODE] = true;
+        attr_set[MODE][sp] = true;
     }
-    fwd_kernel<MODE><<<n_blocks, pl->threads, pl->smem, st>>>(a);
+    if (sp) fwd_kernel<MODE, 1><<<n_blocks, pl->threads, pl->smem, st>>>(a);
+    else fwd_kernel<MODE, 0><<<n_blocks, pl->threads, pl->smem, st>>>(a);
     SDRG_CUDA(cudaGetLastError());
     return SDRG_OK;
 }
