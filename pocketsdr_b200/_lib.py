@@ -176,3 +176,16 @@ def check(what: str = "") -> None:
 
 def ptr(a) -> C.c_void_p:
     return C.c_void_p(a.ctypes.data)
+
+
+CUDA_STREAM_LEGACY = 1      # cudaStreamLegacy
+
+
+def torch_stream() -> int:
+    """Handle of torch's current CUDA stream for the C ABI. Torch's default
+    stream is the legacy default stream, handle 0, but several entry points
+    read a NULL stream as the calling thread's own non-blocking stream, which
+    is not ordered with torch's work; the legacy stream is therefore named
+    explicitly (cudaStreamLegacy), which every entry point reads the same way."""
+    import torch
+    return torch.cuda.current_stream().cuda_stream or CUDA_STREAM_LEGACY

@@ -12,7 +12,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import IngestCfg, check, lib
+from ._lib import IngestCfg, check, lib, torch_stream
 
 FMT_INT8, FMT_INT8X2, FMT_RAW8, FMT_RAW16, FMT_RAW16I, FMT_RAW32, FMT_CS8, FMT_CS16 = range(1, 9)
 BYTES_PER_SAMPLE = {FMT_INT8: 1, FMT_INT8X2: 2, FMT_RAW8: 1, FMT_RAW16: 2, FMT_RAW16I: 2,
@@ -62,7 +62,6 @@ class Ingest:
     def run(self, raw, ix: int, bufs, base: int = 0, stream=None) -> None:
         """raw: CUDA uint8 tensor (N * bytes-per-sample); bufs: n_rf + narch CUDA
         uint8 tensors (IF buffers); asynchronous on torch's current stream."""
-        import torch
         if len(bufs) != self.n_rf + self.narch:
             raise ValueError(f"{self.n_rf + self.narch} buffers expected")
         for b in bufs:
@@ -71,7 +70,7 @@ class Ingest:
         if raw.numel() < self.N * BYTES_PER_SAMPLE[self.fmt]:
             raise ValueError("raw block shorter than N samples")
         ptrs = (C.c_void_p * len(bufs))(*[b.data_ptr() for b in bufs])
-        st = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        st = stream if stream is not None else torch_stream()
         if lib.sdrg_ingest_run(self.handle, C.c_void_p(raw.data_ptr()), int(ix), ptrs, int(base),
                                C.c_void_p(st)):
             check("sdrg_ingest_run")

@@ -24,6 +24,7 @@ import numpy as np
 import torch
 
 from . import acquire, track
+from ._lib import torch_stream
 
 _plans: dict = {}
 _plans_lock = threading.Lock()
@@ -74,7 +75,7 @@ def search(buf: torch.Tensor, ix: int, chips: torch.Tensor, fds: List[float], fs
     pl.set_codes(0, chips, T)
     res = torch.empty(n_prn * acquire.RESULT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
     pl.run_device([buf.data_ptr()], [buf.numel()], [ix], res.data_ptr(),
-                  torch.cuda.current_stream().cuda_stream)
+                  torch_stream())
     grid = _device_view(pl.grid_ptr(0), (n_prn, len(fds), N), "<f4").clone()
     r32 = res.view(torch.int32).view(n_prn, 8)
     rf = res.view(torch.float32).view(n_prn, 8)
@@ -116,7 +117,7 @@ def corr_batch(buf: torch.Tensor, ix: List[int], fc: List[float], phi: List[floa
     jobs = track.make_jobs(specs)
     out = torch.empty((n, track.SDR_MAX_CORR), dtype=torch.complex64, device="cuda")
     track.corr_batch(jobs, [buf.data_ptr()], [buf.numel()], out.data_ptr(), 0,
-                     torch.cuda.current_stream().cuda_stream)
+                     torch_stream())
     return out[:, :len(pos)].clone()
 
 

@@ -29,7 +29,7 @@ from dataclasses import dataclass
 import numpy as np
 import torch
 
-from ._lib import GpuError, RefineSig, check, lib
+from ._lib import GpuError, RefineSig, check, lib, torch_stream
 
 W = 12                      # sums per (signal, block)
 MODEL_POWER, MODEL_COHERENT, MODEL_BLOCKS = 0, 1, 2
@@ -44,9 +44,7 @@ class RefineSpec:
 
 
 def _stream() -> C.c_void_p:
-    # torch's current stream; handle 0 is the legacy default stream, which is
-    # also what the library takes NULL to mean
-    return C.c_void_p(torch.cuda.current_stream().cuda_stream or None)
+    return C.c_void_p(torch_stream())
 
 
 def _dptr(t: torch.Tensor) -> C.c_void_p:

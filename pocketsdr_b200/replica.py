@@ -20,7 +20,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import check, lib
+from ._lib import check, lib, torch_stream
 
 SDR_N_CODES = 10
 
@@ -44,7 +44,7 @@ def device_chips(chips):
 
 
 def _stream() -> C.c_void_p:
-    return C.c_void_p(_torch().cuda.current_stream().cuda_stream)
+    return C.c_void_p(torch_stream())
 
 
 def res_code(chips, T: float, coff: float, fs: float, N: int, Nz: int = 0,

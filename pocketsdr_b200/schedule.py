@@ -14,7 +14,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._lib import SrchReq, SrchRes, SrchSetup, check, lib
+from ._lib import SrchReq, SrchRes, SrchSetup, check, lib, torch_stream
 
 RESULT_DTYPE = np.dtype([("found", np.int32), ("bin", np.int32), ("offset", np.int32),
                          ("cn0", np.float32), ("fd", np.float64), ("coff", np.float64),
@@ -74,12 +74,11 @@ def groups(setups, reqs, t_acq):
 def search(setups, reqs, bufs, ix: int, t_acq: float, thres_cn0: float) -> np.ndarray:
     """Runs every request's search; bufs: CUDA uint8 tensors (IF buffers).
     Returns RESULT_DTYPE[len(reqs)]."""
-    import torch
     su, rq, keep = _arrays(setups, reqs)
     ptrs = (C.c_void_p * len(bufs))(*[b.data_ptr() for b in bufs])
     lens = (C.c_int * len(bufs))(*[b.numel() for b in bufs])
     res = (SrchRes * len(reqs))()
-    st = torch.cuda.current_stream().cuda_stream
+    st = torch_stream()
     if lib.sdrg_search_batch(su, len(su), rq, len(rq), ptrs, lens, int(ix), t_acq, thres_cn0,
                              res, C.c_void_p(st)):
         check("sdrg_search_batch")

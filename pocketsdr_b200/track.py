@@ -13,7 +13,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import check, lib
+from ._lib import check, lib, torch_stream
 
 SDR_N_CODES = 10
 SDR_MAX_CORR = 107
@@ -110,8 +110,7 @@ class L6Batch:
     def run(self, stream: int = 0):
         """Asynchronous on `stream` (0: torch's current stream)."""
         if not stream:
-            import torch
-            stream = torch.cuda.current_stream().cuda_stream
+            stream = torch_stream()
         ptrs, ls, sym, taps, corr = self._args
         if lib.sdrg_l6_csk_batch(self.arr, self.n, ptrs, ls, sym, taps, corr, C.c_void_p(stream)):
             check("sdrg_l6_csk_batch")

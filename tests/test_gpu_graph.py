@@ -12,9 +12,10 @@ pytestmark = pytest.mark.gpu
 
 
 def _device_run(plan, d_bufs, ix, graph, torch):
+    from pocketsdr_b200._lib import torch_stream
     from pocketsdr_b200.acquire import RESULT_DTYPE
     res = torch.zeros(plan.n_res * RESULT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
-    st = torch.cuda.current_stream().cuda_stream
+    st = torch_stream()
     plan.run_device([b.data_ptr() for b in d_bufs], [b.numel() for b in d_bufs], ix,
                     res.data_ptr(), st, graph=graph)
     torch.cuda.synchronize()

@@ -65,3 +65,26 @@ def test_corr_batch_op_bit_exact(gpu, orc):
         IQ = orc.mix_carr(buf, ix[j], N, fs, fc[j], phi[j])
         want, _ = orc.corr_std(IQ, banks[j], coff[j], np.asarray(pos), False)
         assert np.array_equal(out[j].view(np.uint32), want.view(np.uint32)), j
+
+
+def test_ops_ordered_after_torch_default_stream(gpu):
+    """The operators run on torch's current stream, the legacy default stream
+    here: an IF buffer whose fill is still queued behind a 0.1 s spin on that
+    stream is searched only once it is filled, and the grid's copy waits for
+    the search."""
+    torch = pytest.importorskip("torch")
+    from pocketsdr_b200 import codes, ops, synth  # noqa: F401
+    wl = synth.acq_multi_24mhz(seed=3, prn_limit=1, t_sum=2e-3, sigs=(("L1CA", 0),))
+    g = wl.groups[0]
+    chips = torch.from_numpy(np.stack([codes.gen_code(g.sig, p) for p in g.prns])).cuda()
+    src = torch.from_numpy(wl.bufs[g.buf]).cuda()
+    args = (chips, [float(f) for f in g.fds], g.fs, g.fi, g.T, g.N, g.L - g.N, g.n_sum)
+    want = torch.ops.pocketsdr.search(src, 0, *args)[0].cpu().numpy()
+    torch.cuda.synchronize()
+    for _ in range(2):
+        d = torch.zeros_like(src)
+        torch.cuda._sleep(200_000_000)          # about 0.1 s of device time
+        d.copy_(src)
+        got = torch.ops.pocketsdr.search(d, 0, *args)[0].cpu().numpy()
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    ops.release_plans()

@@ -9,6 +9,7 @@ pytestmark = pytest.mark.gpu
 
 def _run_batch(torch, bufs, specs, banks):
     from pocketsdr_b200 import track
+    from pocketsdr_b200._lib import torch_stream
     d_bufs = [torch.from_numpy(b).cuda() for b in bufs]
     d_banks = [torch.from_numpy(np.ascontiguousarray(bk)).cuda() for bk in banks]
     for s, db in zip(specs, d_banks):
@@ -18,7 +19,7 @@ def _run_batch(torch, bufs, specs, banks):
     corr = torch.zeros(n * track.SDR_MAX_CORR * 2, dtype=torch.float32, device="cuda")
     Cb = torch.zeros(n * 4, dtype=torch.float32, device="cuda")
     track.corr_batch(jobs, [b.data_ptr() for b in d_bufs], [len(b) for b in bufs],
-                     corr.data_ptr(), Cb.data_ptr(), torch.cuda.current_stream().cuda_stream)
+                     corr.data_ptr(), Cb.data_ptr(), torch_stream())
     torch.cuda.synchronize()
     corr = corr.cpu().numpy().view(np.complex64).reshape(n, track.SDR_MAX_CORR)
     Cb = Cb.cpu().numpy().view(np.complex64).reshape(n, 2)
@@ -89,6 +90,7 @@ def test_corr_batch_arbitrary_code_bytes_and_alignment(orc):
     is checked to occur."""
     torch = pytest.importorskip("torch")
     from pocketsdr_b200 import track
+    from pocketsdr_b200._lib import torch_stream
     rng = np.random.default_rng(71)
     buf = rng.integers(0, 256, 90001, dtype=np.uint8)
     specs, banks, keep = [], [], []
@@ -120,7 +122,7 @@ def test_corr_batch_arbitrary_code_bytes_and_alignment(orc):
     corr = torch.zeros(n * track.SDR_MAX_CORR * 2, dtype=torch.float32, device="cuda")
     Cb = torch.zeros(n * 4, dtype=torch.float32, device="cuda")
     track.corr_batch(jobs, [d_buf.data_ptr()], [len(buf)], corr.data_ptr(), Cb.data_ptr(),
-                     torch.cuda.current_stream().cuda_stream)
+                     torch_stream())
     torch.cuda.synchronize()
     corr = corr.cpu().numpy().view(np.complex64).reshape(n, track.SDR_MAX_CORR)
     Cb = Cb.cpu().numpy().view(np.complex64).reshape(n, 2)

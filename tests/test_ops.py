@@ -19,3 +19,15 @@ def test_ops_registered_with_shapes():
         c = torch.ops.pocketsdr.corr_batch(buf, [0, 7], [4e6, 4e6], [0.0, 0.1], [0.0, 3.5], banks,
                                            [0.0, -11.7, 11.7, -120.0], 24e6, 24000)
         assert c.shape == (2, 4) and c.dtype == torch.complex64
+
+
+def test_torch_stream_names_the_legacy_stream(monkeypatch):
+    """Torch's default stream (handle 0) goes to the C ABI as cudaStreamLegacy,
+    since a NULL stream means the calling thread's own stream to some entry
+    points; any other stream handle passes through."""
+    from types import SimpleNamespace
+    from pocketsdr_b200._lib import CUDA_STREAM_LEGACY, torch_stream
+    for handle, want in ((0, CUDA_STREAM_LEGACY), (0x7F3A10, 0x7F3A10)):
+        monkeypatch.setattr(torch.cuda, "current_stream",
+                            lambda h=handle: SimpleNamespace(cuda_stream=h))
+        assert torch_stream() == want

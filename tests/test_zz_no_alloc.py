@@ -39,9 +39,9 @@ def _noalloc(lib, torch, IQ, cf, stream):
 def test_corr_fft_noalloc_matches_allocating_entry():
     torch = pytest.importorskip("torch")
     from pocketsdr_b200 import sdr_func
-    from pocketsdr_b200._lib import lib
+    from pocketsdr_b200._lib import lib, torch_stream
     sdr_func.init()
-    stream = torch.cuda.current_stream().cuda_stream
+    stream = torch_stream()
     rng = np.random.default_rng(2024)
     # two calls in a row: a new length (tables uploaded), then the same length
     # with new data (array contents of the previous call left behind)
