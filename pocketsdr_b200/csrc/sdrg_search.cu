@@ -207,6 +207,20 @@ struct StoreComplex {
     __device__ __forceinline__ void operator()(int m, float2 y, int) const { row[R * m + c] = y; }
 };
 
+// Hint to bring [p, p + n) into L2 (cp.async.bulk.prefetch.L2): only the
+// 16-byte-aligned interior of the range is named, so nothing outside it is
+// touched; there is no completion to wait for.
+__device__ __forceinline__ void prefetch_l2(const float2 *p, int n)
+{
+    uintptr_t a0 = ((uintptr_t)p + 15) & ~(uintptr_t)15;
+    const uintptr_t e = ((uintptr_t)(p + n)) & ~(uintptr_t)15;
+    while (a0 < e) {
+        const uint32_t sz = (uint32_t)min((uintptr_t)32768, e - a0);
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a0), "r"(sz) : "memory");
+        a0 += sz;
+    }
+}
+
 template <int R, int MODE, int SP>
 __global__ void __launch_bounds__(512, 1) cons_kernel(ConsArgs a)
 {
@@ -222,6 +236,15 @@ __global__ void __launch_bounds__(512, 1) cons_kernel(ConsArgs a)
     const int prn = a.prn0 + task % n_prn_l;
     const int b = task / n_prn_l;
     if (b >= a.n_bin) return;     // uniform across the cluster
+    const int Mc = (M + R - 1) / R;
+    const int q0 = c * Mc, q1 = min(M, q0 + Mc);
+    const float2 *code = a.code + (size_t)(a.code_per_bin ? b : prn) * R * M;
+    // this CTA's ranges of the first sum's spectra and of the code head for
+    // L2 while the twiddles load
+    if (threadIdx.x < R && q1 > q0 && a.n_sum > 0) {
+        prefetch_l2(a.X + (size_t)b * a.n_sum * R * M + (size_t)threadIdx.x * M + q0, q1 - q0);
+        prefetch_l2(code + (size_t)threadIdx.x * M + q0, q1 - q0);
+    }
 
     load_twiddles(tw, a.tw, a.pl.twtot);
 
@@ -233,9 +256,6 @@ __global__ void __launch_bounds__(512, 1) cons_kernel(ConsArgs a)
     } else {
         dst[0] = sm;
     }
-    const int Mc = (M + R - 1) / R;
-    const int q0 = c * Mc, q1 = min(M, q0 + Mc);
-    const float2 *code = a.code + (size_t)(a.code_per_bin ? b : prn) * R * M;
 
     for (int s = 0; s < a.n_sum; ++s) {
         // all CTAs of the cluster are done with their shared memory
@@ -297,6 +317,9 @@ __global__ void __launch_bounds__(512, 1) cons_kernel(ConsArgs a)
             }
         }
         if constexpr (R > 1) cg::this_cluster().sync(); else __syncthreads();
+        // the next sum's spectra head for L2 during this sum's transform
+        if (s + 1 < a.n_sum && threadIdx.x < R && q1 > q0)
+            prefetch_l2(Xs + (size_t)R * M + (size_t)threadIdx.x * M + q0, q1 - q0);
 
         if (MODE == 0) {
             float *row = a.P + (size_t)(prn) * a.prn_stride + (size_t)b * a.bin_stride;
