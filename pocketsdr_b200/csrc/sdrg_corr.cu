@@ -160,12 +160,12 @@ static void corr_std_host(const sdr_cpx16_t *IQ, const sdr_cpx16_t *code, int N,
 {
     if (N <= 0 || n <= 0) return;
     cudaStream_t st;
-    int e;
     ThreadCtx &c = tctx();
     const size_t iqb = (size_t)N * 2, cb = (size_t)N * 2 * SDR_N_CODES;
     c.host[0].pinned = true;
-    if ((e = ensure_device(nullptr)) || (e = thread_stream(&st)) ||
-        (e = c.host[0].reserve(iqb + cb + 16)) || (e = c.dev[0].reserve(iqb + cb + 16)))
+    // a failing step has recorded its error in the thread's last-error state
+    if (ensure_device(nullptr) || thread_stream(&st) ||
+        c.host[0].reserve(iqb + cb + 16) || c.dev[0].reserve(iqb + cb + 16))
         goto fail;
     {
         uint8_t *h = (uint8_t *)c.host[0].ptr;
@@ -210,12 +210,11 @@ void sdr_corr_std_cpx(const sdr_cpx_t *buff, int len_buff, int ix, int N, double
 {
     if (N <= 0 || n <= 0) return;
     cudaStream_t st;
-    int e;
     ThreadCtx &c = tctx();
     c.host[0].pinned = true;
-    if ((e = ensure_device(nullptr)) || (e = thread_stream(&st)) ||
-        (e = c.dev[0].reserve((size_t)N * 4 + (size_t)N * 4 + 64)) ||
-        (e = c.host[0].reserve((size_t)N * 4 + 16))) {
+    if (ensure_device(nullptr) || thread_stream(&st) ||
+        c.dev[0].reserve((size_t)N * 4 + (size_t)N * 4 + 64) ||
+        c.host[0].reserve((size_t)N * 4 + 16)) {
         memset(corr, 0, sizeof(sdr_cpx_t) * n);
         return;
     }

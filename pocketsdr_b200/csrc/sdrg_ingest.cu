@@ -499,12 +499,11 @@ void sdr_lpf_apply(sdr_lpf_t *lpf, sdr_cpx8_t *data, int N)
     if (!lpf || !data || N <= 0) return;
     Device *dev;
     cudaStream_t st;
-    int e;
     ThreadCtx &c = tctx();
     c.host[0].pinned = true;
     const size_t nb = ((size_t)N + 255) / 256 * 256;
-    if ((e = ensure_device(&dev)) || (e = thread_stream(&st)) || (e = c.host[0].reserve(2 * nb)) ||
-        (e = c.dev[0].reserve(2 * nb + 2 * kMaxRf * 8)))
+    if (ensure_device(&dev) || thread_stream(&st) || c.host[0].reserve(2 * nb) ||
+        c.dev[0].reserve(2 * nb + 2 * kMaxRf * 8))
         return;   // error recorded; data left unfiltered
     uint8_t *h_in = (uint8_t *)c.host[0].ptr, *h_out = h_in + nb;
     uint8_t *d_in = (uint8_t *)c.dev[0].ptr, *d_out = d_in + nb;

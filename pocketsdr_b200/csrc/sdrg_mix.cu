@@ -147,11 +147,11 @@ void sdr_mix_carr(const sdr_buff_t *buff, int ix, int N, double fs, double fc, d
     }
     Device *dev;
     cudaStream_t st;
-    int e;
     ThreadCtx &c = tctx();
     c.host[0].pinned = true;
-    if ((e = ensure_device(&dev)) || (e = thread_stream(&st)) ||
-        (e = c.host[0].reserve((size_t)N * 3 + 16)) || (e = c.dev[0].reserve((size_t)N * 3 + 64))) {
+    // a failing step has recorded its error in the thread's last-error state
+    if (ensure_device(&dev) || thread_stream(&st) ||
+        c.host[0].reserve((size_t)N * 3 + 16) || c.dev[0].reserve((size_t)N * 3 + 64)) {
         memset(IQ, 0, (size_t)N * 2);
         return;
     }

@@ -182,13 +182,12 @@ float sdr_corr_max(const float *P, int N, int Nmax, int M, double T, int *ix)
 {
     if (M <= 0 || Nmax <= 0 || N < Nmax) return 0.0f;
     cudaStream_t st;
-    int e;
     ThreadCtx &c = tctx();
     const size_t pb = (size_t)M * N * sizeof(float);
     c.host[2].pinned = true;
-    if ((e = ensure_device(nullptr)) || (e = thread_stream(&st)) ||
-        (e = c.dev[3].reserve(pb + 256 + peak_scratch_bytes(1))) ||
-        (e = c.host[2].reserve(pb + 256)))
+    // a failing step has recorded its error in the thread's last-error state
+    if (ensure_device(nullptr) || thread_stream(&st) ||
+        c.dev[3].reserve(pb + 256 + peak_scratch_bytes(1)) || c.host[2].reserve(pb + 256))
         return 0.0f;
     memcpy(c.host[2].ptr, P, pb);
     float *P_d = (float *)c.dev[3].ptr;

@@ -207,7 +207,6 @@ void sdr_psd_cpx(const sdr_cpx_t *buff, int len_buff, int N, double fs, int IQ, 
     const int n_out = IQ == 1 ? N / 2 : N;
     Device *dev;
     cudaStream_t st;
-    int e;
     ThreadCtx &c = tctx();
     c.host[0].pinned = true;
     const size_t nin = (size_t)(len_buff > 0 ? len_buff : 0) * sizeof(float2);
@@ -217,8 +216,8 @@ void sdr_psd_cpx(const sdr_cpx_t *buff, int len_buff, int N, double fs, int IQ, 
         memset(psd, 0, nout);
         return;
     }
-    if ((e = ensure_device(&dev)) || (e = thread_stream(&st)) ||
-        (e = c.host[0].reserve(nin > nout ? nin : nout)) || (e = c.dev[0].reserve(nin + nout + 256))) {
+    if (ensure_device(&dev) || thread_stream(&st) ||
+        c.host[0].reserve(nin > nout ? nin : nout) || c.dev[0].reserve(nin + nout + 256)) {
         memset(psd, 0, nout);
         return;
     }

@@ -1139,13 +1139,12 @@ void sdr_corr_fft(const sdr_cpx16_t *IQ, const sdr_cpx_t *code_fft, int N,
                   sdr_cpx_t *corr)
 {
     if (N <= 0) return;
-    int e;
     Device *dev;
-    if ((e = ensure_device(&dev))) { memset(corr, 0, sizeof(sdr_cpx_t) * N); return; }
+    if (ensure_device(&dev)) { memset(corr, 0, sizeof(sdr_cpx_t) * N); return; }
     cudaStream_t st;
     ThreadCtx &c = tctx();
-    if ((e = thread_stream(&st)) || (e = c.dev[0].reserve((size_t)N * 2)) ||
-        ((c.host[1].pinned = true), (e = c.host[1].reserve((size_t)N * 2)))) {
+    if (thread_stream(&st) || c.dev[0].reserve((size_t)N * 2) ||
+        ((c.host[1].pinned = true), c.host[1].reserve((size_t)N * 2))) {
         memset(corr, 0, sizeof(sdr_cpx_t) * N);
         return;
     }
@@ -1161,14 +1160,12 @@ void sdr_corr_fft_cpx(const sdr_cpx_t *buff, int len_buff, int ix, int N, double
                       double fc, double phi, const sdr_cpx_t *code_fft, sdr_cpx_t *corr)
 {
     if (N <= 0) return;
-    int e;
     cudaStream_t st;
     ThreadCtx &c = tctx();
-    if ((e = ensure_device(nullptr)) || (e = thread_stream(&st)) ||
-        (e = c.dev[0].reserve((size_t)N * 2)) ||
-        (e = mix_cpx_device(buff, len_buff, ix, N, fs, fc, phi,
-                                 (char2 *)c.dev[0].ptr, st)) ||
-        (e = corr_fft_device((const char2 *)c.dev[0].ptr, code_fft, N, corr))) {
+    if (ensure_device(nullptr) || thread_stream(&st) ||
+        c.dev[0].reserve((size_t)N * 2) ||
+        mix_cpx_device(buff, len_buff, ix, N, fs, fc, phi, (char2 *)c.dev[0].ptr, st) ||
+        corr_fft_device((const char2 *)c.dev[0].ptr, code_fft, N, corr)) {
         memset(corr, 0, sizeof(sdr_cpx_t) * N);
     }
 }
@@ -1186,20 +1183,19 @@ void sdr_search_code(const sdr_cpx_t *code_fft, double T, const sdr_buff_t *buff
     }
     const FftPlan *pl = plan_for_jobs(N, len_fds);
     if (!pl) return;
-    int e;
     Device *dev;
     cudaStream_t st;
-    if ((e = ensure_device(&dev)) || (e = thread_stream(&st))) return;
+    if (ensure_device(&dev) || thread_stream(&st)) return;
     ThreadCtx &c = tctx();
     const size_t cb = (size_t)N * sizeof(float2);
     const size_t pb = (size_t)len_fds * N * sizeof(float);
     const size_t xb = (size_t)len_fds * cb;
     const size_t tabw = 3 * (size_t)len_fds + 2;
     for (int i = 0; i < 3; ++i) c.host[i].pinned = true;
-    if ((e = c.dev[0].reserve((size_t)N + 64)) || (e = c.dev[1].reserve(2 * cb)) ||
-        (e = c.dev[2].reserve(xb)) || (e = c.dev[3].reserve(pb)) ||
-        (e = c.dev[4].reserve(tabw * 4)) || (e = c.host[0].reserve(cb)) ||
-        (e = c.host[1].reserve((size_t)N + 16 + tabw * 4)) || (e = c.host[2].reserve(pb)))
+    if (c.dev[0].reserve((size_t)N + 64) || c.dev[1].reserve(2 * cb) ||
+        c.dev[2].reserve(xb) || c.dev[3].reserve(pb) ||
+        c.dev[4].reserve(tabw * 4) || c.host[0].reserve(cb) ||
+        c.host[1].reserve((size_t)N + 16 + tabw * 4) || c.host[2].reserve(pb))
         return;
     uint8_t *win_h = (uint8_t *)c.host[1].ptr;
     uint32_t *tab_h = (uint32_t *)(win_h + ((N + 15) / 16) * 16);
@@ -1232,7 +1228,7 @@ void sdr_search_code(const sdr_cpx_t *code_fft, double T, const sdr_buff_t *buff
         cuda_error(cudaGetLastError(), "sdr_search_code H2D");
         return;
     }
-    if ((e = perm_code(pl, code_nat, 1, code_perm, st))) return;
+    if (perm_code(pl, code_nat, 1, code_perm, st)) return;
     FwdArgs fa = {};
     fa.pl = pl->k; fa.tw = pl->tw_dev; fa.ctab = dev->ctab_dev; fa.R = pl->R;
     fa.n_bin = len_fds; fa.n_sum = 1; fa.cscale = kCScale;
@@ -1241,15 +1237,15 @@ void sdr_search_code(const sdr_cpx_t *code_fft, double T, const sdr_buff_t *buff
     fa.ix = (const int *)(tab_d + 3 * len_fds);
     fa.nsplit = fa.ix + 1;
     fa.X = X;
-    if ((e = launch_fwd<0>(pl, fa, len_fds * pl->R, st))) return;
+    if (launch_fwd<0>(pl, fa, len_fds * pl->R, st)) return;
     ConsArgs ca = {};
     ca.pl = pl->k; ca.tw = pl->tw_dev; ca.split = pl->split_dev; ca.X = X; ca.code = code_perm;
     ca.n_prn = 1; ca.n_bin = len_fds; ca.n_sum = 1; ca.prn0 = 0;
     ca.scale = 1.0f / N / N; ca.Nmax = N; ca.prn_stride = 0; ca.bin_stride = N;
     ca.accumulate = 1; ca.P = P_d;
     const int wt = staged_chunk(pl, len_fds);
-    if (wt && (e = c.dev[5].reserve(staged_bytes(pl, wt, 0)))) return;
-    if ((e = launch_consumer<0>(pl, ca, len_fds, st, wt ? (float2 *)c.dev[5].ptr : nullptr, wt)))
+    if (wt && c.dev[5].reserve(staged_bytes(pl, wt, 0))) return;
+    if (launch_consumer<0>(pl, ca, len_fds, st, wt ? (float2 *)c.dev[5].ptr : nullptr, wt))
         return;
     if (cudaMemcpyAsync(c.host[2].ptr, P_d, pb, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess) {
