@@ -179,7 +179,7 @@ int sdrg_init(int device);
 
 /* 1 when an FFT of length N has a GPU plan (N = R*M with R in
  * {1,2,3,4,5,6,8} (one thread-block cluster) or {10,12,15,16,20} (staged
- * through an L2-resident scratch), M 2-3-5-smooth and small enough for one
+ * through a scratch buffer in device memory), M 2-3-5-smooth and small enough for one
  * CTA's shared memory (<= ~27 000)), else 0. */
 int sdrg_fft_supported(int N);
 

@@ -263,7 +263,8 @@ bool shape_ok(int L, int R)
 }
 
 // R <= 8: one thread-block cluster per transform; R in 10..20: staged
-// through an L2-resident scratch (a cluster cannot exceed 8 portably)
+// through a scratch buffer in global memory (a cluster cannot exceed 8
+// portably)
 static const int kSplits[] = {1, 2, 3, 4, 5, 6, 8, 10, 12, 15, 16, 20};
 
 static bool split_allowed(int R)
