@@ -1209,7 +1209,7 @@ L6_METRIC = ("L6 CSK channel-epochs/s (QZSS L6D, 24 MHz: mix + 96 000-point FFT 
 
 
 def _l6_workload(seed, n_ch=10):
-    """10 QZSS L6D channels (PRN 193-202, stand-in codes) in a 24 MHz complex
+    """10 QZSS L6D channels (PRN 193-202) in a 24 MHz complex
     IF of 0.2 s, each keyed by its own code shift; per channel its code bank
     DFT (bank i % 10) and tap set (P, E, L, noise + 9 taps of 0.25 chip)."""
     from pocketsdr_b200 import codes, synth

@@ -341,6 +341,21 @@ typedef struct {
 int sdrg_corr_batch(const sdrg_corr_job_t *jobs, int n_job, const uint8_t *const *if_dev,
     const int *len_if, sdr_cpx_t *corr_dev, sdr_cpx_t *C_dev, void *stream);
 
+/* ---- spreading-code chips (host) -------------------------------------------
+ * The reference's sdr_gen_code / sdr_sec_code (src/sdr_code.c:2173-2182,
+ * :2274-2283; src/pocket_sdr.h:454-455) for the signals of the search and
+ * tracking paths: "L1CA" (PRN 1-210), "L5I" / "L5Q" (1-210), "L6D" (193-202),
+ * "L6E" (203-212), "E1B" (1-50, BOC(1,1) sub-carrier applied: 8184 values)
+ * and "B1I" (1-63); case-insensitive. Same chips as the reference: +1 / -1,
+ * 0 in the off slots of time-multiplexed codes (L6D / L6E). Secondary codes:
+ * NH10 (L5I), NH20 (L5Q, B1I PRN 6-58), the Manchester overlay of SBAS L5
+ * (PRN 120-158), otherwise the one-chip code {1}. Host only, no device work.
+ * Returns the code length and, if `chips` is not NULL, writes the chips there
+ * (`cap` values available; fewer than the length is SDRG_ERR_ARG). An
+ * unknown signal or PRN returns SDRG_ERR_ARG (the reference returns NULL). */
+int sdrg_gen_code(const char *sig, int prn, int8_t *chips, int cap);
+int sdrg_sec_code(const char *sig, int prn, int8_t *chips, int cap);
+
 /* ---- replicas on the device ------------------------------------------------
  * Batched forms of sdr_res_code / sdr_gen_code_fft (src/sdr_code.c:2556-2608)
  * for n_code codes of len_code chips each, stored back to back

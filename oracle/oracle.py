@@ -298,6 +298,8 @@ class Reference:
         L.sdr_dop_bins.restype = C.POINTER(_f)
         L.sdr_gen_code.argtypes = [C.c_char_p, _i, C.POINTER(_i)]
         L.sdr_gen_code.restype = C.POINTER(C.c_int8)
+        L.sdr_sec_code.argtypes = [C.c_char_p, _i, C.POINTER(_i)]
+        L.sdr_sec_code.restype = C.POINTER(C.c_int8)
         L.sdr_code_cyc.argtypes = [C.c_char_p]
         L.sdr_code_cyc.restype = _d
         L.sdr_res_code.argtypes = [_p, _p, _i, _d, _d, _d, _i, _i, _p]
@@ -409,6 +411,13 @@ class Reference:
         p = self.lib.sdr_gen_code(sig.encode(), prn, C.byref(n))
         if not p:
             raise ValueError(f"no code for {sig} {prn}")
+        return np.ctypeslib.as_array(p, shape=(n.value,)).copy()
+
+    def sec_code(self, sig: str, prn: int) -> np.ndarray:
+        n = _i(0)
+        p = self.lib.sdr_sec_code(sig.encode(), prn, C.byref(n))
+        if not p:
+            raise ValueError(f"no secondary code for {sig} {prn}")
         return np.ctypeslib.as_array(p, shape=(n.value,)).copy()
 
     def code_cyc(self, sig: str) -> float:

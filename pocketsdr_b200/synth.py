@@ -108,16 +108,20 @@ def gen_if(n: int, fs: float, fi_of: dict, sats: list, *, iq: bool, bits: int,
         n0 = 2.0 / fs
     for s in sats:
         chips = codes.gen_code(s.sig, s.prn).astype(np.float64)
+        sec = codes.sec_code(s.sig, s.prn).astype(np.float64)
         L, T = codes.SIGNALS[s.sig]
         rate = L / T * (1.0 + s.doppler / CARRIER[s.sig])
-        idx = np.floor(s.code_phase + rate * t).astype(np.int64) % L
+        u = np.floor(s.code_phase + rate * t).astype(np.int64)
+        # secondary code: the first whole primary period (the one after the
+        # partial period at sample 0) carries its first chip
+        c = chips[u % L] * sec[(u // L - 1) % len(sec)]
         ph = 2 * np.pi * ((fi_of[s.sig] + s.doppler) * t + s.phase)
         if iq:
             amp = np.sqrt(10 ** (s.cn0 / 10) * n0)
-            x += amp * chips[idx] * np.exp(1j * ph)
+            x += amp * c * np.exp(1j * ph)
         else:
             amp = np.sqrt(2 * 10 ** (s.cn0 / 10) * n0)
-            x += amp * chips[idx] * np.cos(ph)
+            x += amp * c * np.cos(ph)
     I = _quant(x.real, bits)
     Q = _quant(x.imag, bits) if iq else None
     return pack(I, Q)
@@ -179,31 +183,37 @@ def acq_multi_24mhz(seed: int = 2, prn_limit: int | None = None, t_sum: float = 
 
 def long_replica_fft(sig: str, prn: int, fs: float, t_coh: float, L: int) -> np.ndarray:
     """Conjugated DFT of a t_coh-second replica for long coherent integration:
-    the primary code repeated over t_coh with a seeded +-1 overlay per primary
-    period (standing in for a secondary code such as L5's NH sequences) and,
-    for codes longer than t_coh allows to repeat whole, simply truncated."""
+    the primary code repeated over t_coh with the signal's secondary code
+    overlaid, one secondary chip per primary period from its first chip (L5-Q:
+    NH20), and, for codes longer than t_coh allows to repeat whole (L6D, 4 ms
+    in 10 ms), truncated."""
     chips = codes.gen_code(sig, prn).astype(np.float64)
+    sec = codes.sec_code(sig, prn).astype(np.float64)
     Lc, T = codes.SIGNALS[sig]
     n = int(round(fs * t_coh))
     t = np.arange(n, dtype=np.float64)
     per = np.floor(t * (1.0 / (T * fs))).astype(np.int64)            # primary period index
     idx = (np.floor(t * (Lc / (T * fs))).astype(np.int64)) % Lc
-    ov = np.random.default_rng(sum(map(ord, sig)) * 7 + prn).choice([-1.0, 1.0], per.max() + 1)
     x = np.zeros(L, np.complex128)
-    x[:n] = chips[idx] * ov[per]
+    x[:n] = chips[idx] * sec[per % len(sec)]
     return np.conj(np.fft.fft(x)).astype(np.complex64)
 
 
 def acq_long_48mhz(seed: int = 6, prn_limit: int | None = None, n_sum: int = 20,
                    bins: np.ndarray | None = None) -> Workload:
     """Weak-signal long coherent search: 48 MHz complex IQ, 3-bit, GPS L5-Q
-    (stand-in codes, 1 ms primary with a per-ms overlay) and QZSS L6D (stand-in
-    TDM code, 4 ms) at C/N0 25-32 dB-Hz; 10 ms coherent (480 000-sample FFTs)
-    x n_sum non-coherent sums over +-10 kHz in 50 Hz bins."""
-    fs, bits, t_coh = 48e6, 3, 10e-3
+    (1 ms primary code with the NH20 secondary code) and QZSS L6D (4 ms code,
+    time-multiplexed) at C/N0 25-32 dB-Hz; 10 ms coherent (480 000-sample
+    FFTs) x n_sum non-coherent sums over +-10 kHz in 50 Hz bins. The coherent
+    windows start 20 ms apart - one NH20 period, five L6D periods - so that
+    every sum meets the replica's secondary-code and code phase (with 10 ms
+    steps, every other window would carry the other half of NH20 and start
+    half an L6D period later)."""
+    fs, bits, t_coh, t_step = 48e6, 3, 10e-3, 20e-3
     fi_of = {"L5Q": 0.0, "L6D": 5.0e6}
     rng = np.random.default_rng(seed)
     L = int(round(fs * t_coh))
+    step = int(round(fs * t_step))
     fds = np.arange(-10000, 10001, 50, dtype=np.float32) if bins is None else np.asarray(bins, np.float32)
     sats, groups = [], []
     for sig in ("L5Q", "L6D"):
@@ -215,8 +225,8 @@ def acq_long_48mhz(seed: int = 6, prn_limit: int | None = None, n_sum: int = 20,
             sats.append(Sat(sig, int(p), float(rng.uniform(0, codes.SIGNALS[sig][0])),
                             float(rng.uniform(-9000, 9000)), float(rng.uniform(0, 1)),
                             float(rng.uniform(25, 32)), 0))
-        groups.append(Group(sig, prns, fs, fi_of[sig], t_coh, L, L, L, n_sum, fds, 0))
-    buf = gen_if(L * (n_sum + 1), fs, fi_of, sats, iq=True, bits=bits, seed=seed * 10)
+        groups.append(Group(sig, prns, fs, fi_of[sig], t_coh, step, L, L, n_sum, fds, 0))
+    buf = gen_if(step * n_sum + L, fs, fi_of, sats, iq=True, bits=bits, seed=seed * 10)
     return Workload("acq_long_48mhz", fs, True, [buf], groups, sats, [0])
 
 
@@ -274,8 +284,8 @@ def refine_signal(sig: str, prn: int, fs: float, fi: float, n: int, tau: float, 
 
 def refine_12mhz(seed: int = 4, n_l1ca: int = 32, n_e1b: int = 32,
                  cn0=(30.0, 45.0)) -> RefineWorkload:
-    """12 MHz real IF at 3 MHz, 2-bit, GPS L1 C/A and Galileo E1-B (stand-in
-    codes, BOC(1,1)) satellites at C/N0 U[30, 45] dB-Hz with off-grid delay
+    """12 MHz real IF at 3 MHz, 2-bit, GPS L1 C/A and Galileo E1-B (BOC(1,1))
+    satellites at C/N0 U[30, 45] dB-Hz with off-grid delay
     and Doppler (U[-4500, 4500] Hz); refinement over 10 ms coherent x 4
     blocks. Starting grid: L1 C/A 10 ms coherent (N = 120 000, 2N FFT) x 4
     sums in 50 Hz bins, E1-B 8 ms (two code periods, N = 96 000) x 5 sums in

@@ -22,7 +22,7 @@ def ch():
 
 
 def _l6_setup(ref, seed=3):
-    """24 MHz complex IF with four L6D signals (stand-in codes), each keyed
+    """24 MHz complex IF with four L6D signals, each keyed
     by its own code shift, and the channels that track them."""
     from pocketsdr_b200 import codes, synth
     fs, fi, T = 24e6, 2.0e6, 4e-3
