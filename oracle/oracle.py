@@ -38,20 +38,21 @@ _d = C.c_double
 _f = C.c_float
 
 
-REF_ROOT = os.environ.get("POCKETSDR_REF", "/root/reference")
-
-
-def build(ref: bool = True) -> None:
-    """Compile the restatement, and the reference library when its sources
-    are present on this machine."""
+def build(ref_root: str | None = None) -> None:
+    """Compile the restatement and, given the Pocket SDR source tree (argument
+    or the POCKETSDR_REF environment variable), the reference library."""
+    ref_root = ref_root or os.environ.get("POCKETSDR_REF")
     targets = ["oracle"]
-    if ref and os.path.isdir(REF_ROOT + "/src"):
+    if ref_root and os.path.isdir(os.path.join(ref_root, "src")):
         targets.append("ref")
         # the reference's unit test and pocket_acq relinked against the GPU
         # library (which the package build makes first)
         if os.path.exists(os.path.join(HERE, "..", "pocketsdr_b200", "lib", "libsdr_gpu.so")):
             targets.append("linktest")
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+    cmd = ["make", "-s", "-C", HERE] + targets
+    if ref_root:
+        cmd.append("REF=" + os.path.abspath(ref_root))
+    subprocess.run(cmd, check=True)
 
 
 def _ptr(a: np.ndarray):
@@ -70,7 +71,7 @@ class Restatement:
 
     def __init__(self, path: str = ORC_SO):
         if not os.path.exists(path):
-            build(ref=False)
+            build()
         L = self.lib = C.CDLL(path)
         L.orc_init.argtypes = []
         L.orc_mix_table.restype = C.POINTER(C.c_int8)

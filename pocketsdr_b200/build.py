@@ -37,7 +37,7 @@ def nvcc() -> str:
 
 def _headers_mtime() -> float:
     hs = glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) + \
-        glob.glob(os.path.join(INCLUDE, "*.h"))
+        glob.glob(os.path.join(CSRC, "*.inc")) + glob.glob(os.path.join(INCLUDE, "*.h"))
     return max((os.path.getmtime(h) for h in hs), default=0.0)
 
 

@@ -1,8 +1,9 @@
 """Generates the golden fixtures in this folder from the reference itself.
 
-Run where the reference's sources are present (it builds oracle/_ref first):
+Run with POCKETSDR_REF naming the reference source tree (it builds
+oracle/_ref first):
 
-    python tests/golden/make_golden.py
+    POCKETSDR_REF=<tree> python tests/golden/make_golden.py
 
 Every output is produced by the reference's own C functions
 (src/sdr_func.c, src/sdr_code.c), compiled from source by oracle/Makefile, on
@@ -39,7 +40,7 @@ def mix_cases(rng, nbuf):
 
 
 def main() -> int:
-    oracle.build(ref=True)
+    oracle.build()          # the reference tree from POCKETSDR_REF
     R = oracle.Reference()
     rng = np.random.default_rng(20240601)
 
