@@ -193,6 +193,17 @@ const char *sdrg_version(void);
  * the device. */
 void sdrg_inject_alloc_failure(int after);
 
+/* Error-path testing of the staged splits (lengths split more than 8 ways,
+ * e.g. 480 000 points): the next n staged inverse-FFT launches give up their
+ * first wait for each bulk copy into shared memory at once, as if its bound
+ * (about 2 s) had run out. Each copy is still issued in full, lands and is
+ * waited for with the full bound before its data is used; the launch records
+ * the failure in its error word, and the synchronous call that ran it
+ * (sdr_search_code, sdr_corr_fft, sdrg_acq_run_host) returns / records
+ * SDRG_ERR_CUDA and clears the word, so the next call runs normally. Nothing
+ * is faulted or left waiting on the device. 0 cancels. */
+int sdrg_inject_stage_timeout(int n);
+
 /* ---- FFT schedules --------------------------------------------------------
  * The reference keeps FFTW planning wisdom in a file (sdr_func_init(file),
  * src/sdr_func.c:118-121). Here a transform length's schedule - how it is
@@ -212,24 +223,28 @@ int sdrg_fft_schedule_load(const char *path);             /* entries loaded, or 
 
 /* ---- FFT correlator that allocates nothing --------------------------------
  * No counterpart in the reference (an addition of this library).
- * Same result as sdr_corr_fft (corr = IFFT(FFT(IQ * CSCALE) * code_fft / N^2))
- * but for callers that cannot allocate device memory when they call: code
- * running inside a CUDA stream capture, real-time receiver threads that must
- * not hit cudaMalloc's implicit device synchronisation, or hosts whose memory
- * comes from their own pool. Inputs and output are DEVICE pointers owned by
- * the caller (IQ_dev: N mixed samples, code_fft_dev: N conjugated code-DFT
- * values in natural order, corr_dev: N outputs); `stream` is a cudaStream_t
- * (NULL = the legacy default stream); the call is asynchronous on it.
+ * Same result as sdr_corr_fft (corr = IFFT(FFT(IQ * CSCALE) * code_fft / N^2),
+ * within FP32 rounding) for callers that cannot call cudaMalloc: a real-time
+ * receiver channel thread that must not stall on the device-wide
+ * synchronisation an allocation may bring, or a host application whose
+ * device memory all comes from its own pool or budget. Inputs and output
+ * are DEVICE pointers owned by the caller (IQ_dev: N mixed samples,
+ * code_fft_dev: N conjugated code-DFT values in natural order, corr_dev: N
+ * outputs); `stream` is a cudaStream_t (NULL = the legacy default stream);
+ * the call is asynchronous on it and allocates nothing.
  * All intermediate data (permuted code DFT, forward spectrum, FFT tables)
  * live in one fixed device array of about 1.8 MB that every GPU loading the
- * library holds until the process exits; N above SDRG_NOALLOC_MAX_N, or a
- * length whose FFT plan does not fit that array, is rejected with
- * SDRG_ERR_ARG. The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress); make that first call before any stream
- * capture. Every call shares the array and leaves its contents behind: calls
- * that overlap on the GPU (other streams, other threads) race and must be
- * serialised by the caller. Nothing needs clearing between calls (each call
- * overwrites all it reads). Returns SDRG_OK or a negative status. */
+ * library holds until the process exits; N above SDRG_NOALLOC_MAX_N (65536),
+ * or a length whose cluster split does not fit that array, is rejected with
+ * SDRG_ERR_ARG. FFT schedules (sdrg_fft_schedule_set, autotuning) do not
+ * apply: this entry always takes the default split of N. The first call on
+ * a device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current; make that first call before any stream capture.
+ * Every call shares the array and leaves its contents behind; each call
+ * first rewrites every table it reads, so no call depends on an earlier
+ * one, but calls that overlap on the GPU (other streams, other host threads)
+ * race on the array and must be serialised by the caller. Returns SDRG_OK or
+ * a negative status. */
 #define SDRG_NOALLOC_MAX_N 65536
 int sdrg_corr_fft_noalloc(const sdr_cpx16_t *IQ_dev, const sdr_cpx_t *code_fft_dev,
     int N, sdr_cpx_t *corr_dev, void *stream);

@@ -441,6 +441,67 @@ class Reference:
         return out
 
 
+def search_groups(groups, bufs, code_ffts, gpu_res=None, keep=None, max_threads=None) -> dict:
+    """The reference's search path over every PRN of every signal group, on
+    this host's cores: per (group, PRN), sdr_search_code over every
+    non-coherent sum (src/sdr_func.c:664-687, with its 1 ms CPU release every
+    22 bins) into one grid, then sdr_corr_max and sdr_fine_dop
+    (src/sdr_func.c:690-744), as search_sig does per channel
+    (src/sdr_ch.c:420-432); one PRN search per thread, the longest first.
+    Groups are objects with prns, fs, fi, T, N (sum advance), L (FFT length),
+    Nmax, n_sum, fds (float32) and buf (index into bufs); code_ffts[g] holds
+    the conjugated code DFTs [n_prn, L].
+
+    Returns wall_s, cores, kind, "res" (per PRN in group order: bin, offset,
+    cn0, fd, pmax = the grid maximum, pmean = the grid mean over the Nmax kept
+    columns and, with gpu_res - per-PRN results in the same order - at_gpu,
+    the reference grid at the cell the GPU reported) and "grids"
+    ({g: (prn index, grid[n_bin, Nmax])} for the rows named by keep =
+    {g: prn index})."""
+    import concurrent.futures as cf
+    import time
+    R = best()
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    threads = min(cores, max_threads or cores)
+    keep = keep or {}
+    offs = np.cumsum([0] + [len(g.prns) for g in groups])
+    tasks = [(gi, pi) for gi, g in enumerate(groups) for pi in range(len(g.prns))]
+    tasks.sort(key=lambda t: -len(groups[t[0]].fds) * groups[t[0]].n_sum * groups[t[0]].L)
+    out = np.zeros(int(offs[-1]), [("bin", np.int32), ("offset", np.int32),
+                                   ("cn0", np.float64), ("fd", np.float64),
+                                   ("at_gpu", np.float64), ("pmax", np.float64),
+                                   ("pmean", np.float64)])
+    grids = {}
+
+    def one(t):
+        gi, pi = t
+        g = groups[gi]
+        buf = bufs[g.buf]
+        fds = np.ascontiguousarray(g.fds, np.float32)
+        P = np.zeros((len(fds), g.L), np.float32)
+        for s in range(g.n_sum):
+            R.search_code(code_ffts[gi][pi], buf, (s * g.N) % len(buf), g.L, g.fs, g.fi, fds, P,
+                          g.T)
+        cn0, (b, o) = R.corr_max(P, g.L, g.Nmax, len(fds), g.T)
+        k = int(offs[gi]) + pi
+        out[k]["bin"], out[k]["offset"], out[k]["cn0"] = b, o, cn0
+        out[k]["fd"] = R.fine_dop(P, g.L, fds, (b, o))
+        out[k]["pmax"] = float(P[b, o])
+        out[k]["pmean"] = float(P[:, :g.Nmax].mean(dtype=np.float64))
+        if gpu_res is not None:
+            gb, go = int(gpu_res[k]["bin"]), int(gpu_res[k]["offset"])
+            ok = 0 <= gb < len(fds) and 0 <= go < g.Nmax
+            out[k]["at_gpu"] = float(P[gb, go]) if ok else np.nan
+        if keep.get(gi) == pi:
+            grids[gi] = (pi, P[:, :g.Nmax].copy())
+
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+        list(ex.map(one, tasks))
+    return {"wall_s": time.perf_counter() - t0, "cores": threads, "kind": R.kind, "res": out,
+            "grids": grids}
+
+
 def reference_available() -> bool:
     return os.path.exists(REF_SO)
 

@@ -97,6 +97,7 @@ SIGNATURES = {
     "sdrg_fft_supported": ([_i], _i),
     "sdrg_version": ([], C.c_char_p),
     "sdrg_inject_alloc_failure": ([_i], None),
+    "sdrg_inject_stage_timeout": ([_i], _i),
     "sdrg_fft_autotune": ([_i, _p, _p, _p], _i),
     "sdrg_fft_schedule_set": ([_i, _i, _i], _i),
     "sdrg_fft_schedule_get": ([_i, _p, _p], _i),

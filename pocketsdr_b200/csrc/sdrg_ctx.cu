@@ -184,26 +184,34 @@ static bool factor235(int n, Fact *f)
 }
 
 // Best radix sequence for 2^a 3^b 5^c: fewest passes, then the largest
-// smallest radix (balanced passes). Exhaustive over the small exponent space.
-static void best_radices(int n, std::vector<int> &cur, std::vector<int> &best)
+// smallest radix (balanced passes). Exhaustive over the small exponent space;
+// fixed arrays (no heap use: the no-allocation correlator shapes its plans
+// with this too).
+struct Radices {
+    int r[kMaxPass + 1];
+    int n = 0;
+    int min_r() const
+    {
+        int m = 1 << 30;
+        for (int i = 0; i < n; ++i) m = r[i] < m ? r[i] : m;
+        return m;
+    }
+};
+
+static void best_radices(int n, Radices &cur, Radices &best)
 {
     if (n == 1) {
-        if (best.empty() || cur.size() < best.size()) { best = cur; return; }
-        if (cur.size() == best.size()) {
-            int mc = 1 << 30, mb = 1 << 30;
-            for (int r : cur) mc = r < mc ? r : mc;
-            for (int r : best) mb = r < mb ? r : mb;
-            if (mc > mb) best = cur;
-        }
+        if (best.n == 0 || cur.n < best.n || (cur.n == best.n && cur.min_r() > best.min_r()))
+            best = cur;
         return;
     }
-    if (!best.empty() && cur.size() + 1 > best.size()) return;
-    int last = cur.empty() ? 1 << 30 : cur.back();
+    if ((best.n && cur.n + 1 > best.n) || cur.n >= kMaxPass + 1) return;
+    int last = cur.n == 0 ? 1 << 30 : cur.r[cur.n - 1];
     for (int r : kRadices) {
         if (r > last || n % r) continue;  // non-increasing order avoids repeats
-        cur.push_back(r);
+        cur.r[cur.n++] = r;
         best_radices(n / r, cur, best);
-        cur.pop_back();
+        cur.n--;
     }
 }
 
@@ -224,35 +232,55 @@ static bool shape_for_R(int L, int R, int *Mout, FftPlanK *kout)
     int M = L / R;
     Fact f;
     if (!factor235(M, &f)) return false;
-    std::vector<int> cur, best;
-    if (M == 1) best.push_back(1);
+    Radices cur, best;
+    if (M == 1) best.r[best.n++] = 1;
     else best_radices(M, cur, best);
-    if (best.empty() || (int)best.size() > kMaxPass) return false;
+    if (best.n == 0 || best.n > kMaxPass) return false;
     // Even radices first (largest first), odd radices last: the last
     // passes have the smallest strides, and an odd stride of 8-byte
-    // elements spreads a half-warp over all 16 bank pairs.
-    std::stable_sort(best.begin(), best.end(), [](int a, int b) {
+    // elements spreads a half-warp over all 16 bank pairs (stable insertion
+    // sort)
+    auto before = [](int a, int b) {
         if ((a & 1) != (b & 1)) return (a & 1) == 0;
         return a > b;
-    });
+    };
+    for (int i = 1; i < best.n; ++i)
+        for (int j = i; j > 0 && before(best.r[j], best.r[j - 1]); --j) {
+            const int t = best.r[j];
+            best.r[j] = best.r[j - 1];
+            best.r[j - 1] = t;
+        }
     FftPlanK k{};
     k.M = M;
-    k.npass = (int)best.size();
+    k.npass = best.n;
     int Ls = M, off = 0;
     for (int p = 0; p < k.npass; ++p) {
-        k.radix[p] = best[p];
+        k.radix[p] = best.r[p];
         k.Ls[p] = Ls;
         k.twoff[p] = off;
         // pass 0: S entries (powers formed in registers); later passes:
         // S * (r - 1) entries, every twiddle of the pass
-        off += (p == 0) ? Ls / best[p] : (Ls / best[p]) * (best[p] - 1);
-        Ls /= best[p];
+        off += (p == 0) ? Ls / best.r[p] : (Ls / best.r[p]) * (best.r[p] - 1);
+        Ls /= best.r[p];
     }
     k.twtot = off;   // M == 1: one radix-1 pass, one unit twiddle
     if (plan_smem(M, k) > smax) return false;
     *Mout = M;
     *kout = k;
     return true;
+}
+
+// The default rule restricted to cluster splits (R <= 8), schedules not
+// consulted; no heap use.
+bool cluster_shape(int L, int *Rout, int *Mout, FftPlanK *kout)
+{
+    for (int R : {1, 2, 3, 4, 5, 6, 8}) {
+        if (shape_for_R(L, R, Mout, kout)) {
+            *Rout = R;
+            return true;
+        }
+    }
+    return false;
 }
 
 bool shape_ok(int L, int R)

@@ -60,6 +60,7 @@ struct ThreadCtx {
     Scratch host[3];     // pinned host staging slots
     // batched correlators (asynchronous): their own slots and the event of
     // the last upload from cb_host
+    Scratch stage_err;   // device error word of staged FFT launches
     Scratch cb_dev, cb_host;
     cudaEvent_t cb_ev = nullptr, cb_done = nullptr;
     // batched L6 CSK tracking (asynchronous): the same scheme
@@ -94,6 +95,9 @@ const FftPlan *get_plan_shaped(int L, int R, int threads);
 int set_schedule(int L, int R, int threads, double ms);
 bool plan_shape(int L, int *R, int *M, FftPlanK *k);
 bool shape_ok(int L, int R);       // L splits R ways into a fitting length
+// The default split rule over cluster splits only (R <= 8), ignoring any
+// schedule; allocates nothing.
+bool cluster_shape(int L, int *R, int *M, FftPlanK *k);
 
 // ---- kernel launch helpers (defined in the .cu files) -----------------------
 // Packed IF source of one coherent block for the forward transform.

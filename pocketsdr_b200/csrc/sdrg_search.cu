@@ -18,6 +18,7 @@
 // The forward transform of a (bin, sum) block does not depend on the PRN: it
 // is computed once per signal group and reused by every PRN's consumer task.
 #include <cooperative_groups.h>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -164,6 +165,7 @@ struct ConsArgs {
     // where each CTA's accesses are consecutive; the last sum writes P
     float *Q;               // or null: every sum reads and writes P
     int Mq;
+    int *stage_err;         // staged splits: error word (a bulk-copy wait ran out)
 };
 
 // Power store of one sum. kDirect: P = (add ? P : 0) + |y|^2. With the
@@ -359,6 +361,7 @@ struct StageArgs {
     float scale;
     float2 *W;               // [chunk][R][M]
     float *Q;                // power grids: [chunk][R][M] |y|^2 summed over the sums
+    long long wait_cycles;   // bound of the first wait for each bulk copy
 };
 
 template <int R>
@@ -409,16 +412,17 @@ struct StorePowerQ {
     const float *p;      // grid row of the task (seed of the first sum)
     int c, R, Nmax;
     int mode;            // 0: store, 1: add to Q, 2: add to the grid value
+    const int *skip;     // shared flag: the CTA's input never arrived
     __device__ __forceinline__ float pre(int m) const
     {
         const int n = R * m + c;
-        if (n >= Nmax || mode == 0) return 0.0f;
+        if (n >= Nmax || mode == 0 || *skip) return 0.0f;
         return mode == 1 ? q[m] : p[n];
     }
     __device__ __forceinline__ void operator()(int m, float2 y, float old) const
     {
         const int n = R * m + c;
-        if (n < Nmax) {
+        if (n < Nmax && !*skip) {
             const float pw = y.x * y.x + y.y * y.y;
             q[m] = mode ? old + pw : pw;
         }
@@ -429,14 +433,18 @@ struct StoreComplexRt {
     typedef int Old;
     float2 *row;
     int c, R;
+    const int *skip;     // shared flag: the CTA's input never arrived
     __device__ __forceinline__ int pre(int) const { return 0; }
-    __device__ __forceinline__ void operator()(int m, float2 y, int) const { row[R * m + c] = y; }
+    __device__ __forceinline__ void operator()(int m, float2 y, int) const
+    {
+        if (!*skip) row[R * m + c] = y;
+    }
 };
 
 // ---- bulk copies through the TMA engine (cp.async.bulk, mbarrier) ----------
-// Set when a CTA gave up waiting for a bulk copy (a bound, never reached in
-// normal operation); the synchronous entry points report and clear it.
-__device__ int g_stage_wait_err = 0;
+// Bound of every wait for a bulk copy (never reached in normal operation).
+// Past it a CTA sets the launch's error word (ConsArgs::stage_err), which the
+// synchronous entry points report and clear.
 constexpr long long kBulkWaitCycles = 4000000000LL;     // about 2 s at 1.97 GHz
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
@@ -466,18 +474,19 @@ __device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32
                  "[%0], [%1], %2, [%3];"
                  ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
 }
-// waits for phase `parity` of bar to complete, at most kBulkWaitCycles
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+// waits for phase `parity` of bar to complete; false once `limit` clock
+// cycles have passed (checked before each try: a limit of 0 gives up at once)
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit)
 {
     const long long t0 = clock64();
     for (;;) {
+        if (clock64() - t0 >= limit) return false;
         uint32_t done;
         asm volatile("{\n\t.reg .pred p;\n\t"
                      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
                      "selp.u32 %0, 1, 0, p;\n\t}"
                      : "=r"(done) : "r"(smem_u32(bar)), "r"(parity) : "memory");
         if (done) return true;
-        if (clock64() - t0 > kBulkWaitCycles) return false;
     }
 }
 
@@ -520,6 +529,8 @@ __global__ void __launch_bounds__(512, 1) stage_ifft_kernel(ConsArgs ca, StageAr
     const int prn = task % a.n_prn, b = task / a.n_prn;
     const float2 *src = a.W + ((size_t)tl * a.R + c) * M;
     bool copied = false;
+    __shared__ int skip;     // set when a region's copy never completed
+    if (threadIdx.x == 0) skip = 0;
     if constexpr (SP == 1) {
         // compile-time plan: passes 3..1 run warp by warp on REG points each,
         // so each warp's region is brought in by its own bulk copy and the warp
@@ -541,11 +552,13 @@ __global__ void __launch_bounds__(512, 1) stage_ifft_kernel(ConsArgs ca, StageAr
             }
             load_twiddles(tw, ca.tw, ca.pl.twtot);
             __syncthreads();
-            if (!mbar_wait(&bar[w], 0)) {
-                // give up on the bound: record it, wait (bounded) for the copy in
-                // flight before the region is touched, and keep every barrier
-                if (lane == 0) atomicOr(&g_stage_wait_err, 1);
-                mbar_wait(&bar[w], 0);
+            if (!mbar_wait(&bar[w], 0, a.wait_cycles)) {
+                // give up on the bound: record it and wait (bounded) for the
+                // copy in flight before the region is touched; if even that
+                // runs out, the CTA stores nothing (the flag is read after
+                // the barrier before the last pass)
+                if (lane == 0) atomicOr(ca.stage_err, 1);
+                if (!mbar_wait(&bar[w], 0, kBulkWaitCycles) && lane == 0) skip = 1;
             }
             copied = true;
         }
@@ -558,11 +571,11 @@ __global__ void __launch_bounds__(512, 1) stage_ifft_kernel(ConsArgs ca, StageAr
     if (MODE == 0) {
         const float *row = ca.P + (size_t)prn * ca.prn_stride + (size_t)b * ca.bin_stride;
         StorePowerQ st{a.Q + ((size_t)tl * a.R + c) * M, row, c, a.R, ca.Nmax,
-                       a.s > 0 ? 1 : (ca.accumulate ? 2 : 0)};
+                       a.s > 0 ? 1 : (ca.accumulate ? 2 : 0), &skip};
         if constexpr (SP == 1) fft_inverse_static<Plan24000>(sm, tw, st);
         else fft_inverse(sm, tw, ca.pl, st);
     } else {
-        StoreComplexRt st{ca.Y + (size_t)b * a.R * M, c, a.R};
+        StoreComplexRt st{ca.Y + (size_t)b * a.R * M, c, a.R, &skip};
         if constexpr (SP == 1) fft_inverse_static<Plan24000>(sm, tw, st);
         else fft_inverse(sm, tw, ca.pl, st);
     }
@@ -705,11 +718,25 @@ static int set_stage_attr()
 
 // Tasks of a staged split (R > 8) in chunks of w_tasks, each chunk through
 // the scratch W (w_tasks * L complex), sum by sum.
+// Staged inverse launches still to run with a first bulk-copy wait bound of 0
+// (sdrg_inject_stage_timeout): their waits give up at once and report, the
+// copies themselves land and are waited for with the full bound.
+static std::atomic<int> g_stage_timeouts{0};
+
+static long long stage_wait_bound()
+{
+    int n = g_stage_timeouts.load();
+    while (n > 0 && !g_stage_timeouts.compare_exchange_weak(n, n - 1)) {
+    }
+    return n > 0 ? 0 : kBulkWaitCycles;
+}
+
 template <int MODE>
 static int launch_staged(const FftPlan *pl, const ConsArgs &ca, int n_tasks, cudaStream_t st,
                          float2 *W, int w_tasks)
 {
     if (!W || w_tasks <= 0) return set_error(SDRG_ERR_ARG, "staged FFT split without scratch");
+    if (!ca.stage_err) return set_error(SDRG_ERR_ARG, "staged FFT split without an error word");
     const bool sp = Plan24000::matches(pl->k, pl->threads);
     int e;
     if ((e = sp ? set_stage_attr<MODE, 1>() : set_stage_attr<MODE, 0>())) return e;
@@ -736,6 +763,7 @@ static int launch_staged(const FftPlan *pl, const ConsArgs &ca, int n_tasks, cud
             }
             SDRG_CUDA(cudaGetLastError());
             const dim3 gi((unsigned)pl->R, (unsigned)n);
+            sa.wait_cycles = stage_wait_bound();
             if (sp) stage_ifft_kernel<MODE, 1><<<gi, pl->threads, pl->smem, st>>>(ca, sa);
             else stage_ifft_kernel<MODE, 0><<<gi, pl->threads, pl->smem, st>>>(ca, sa);
             SDRG_CUDA(cudaGetLastError());
@@ -797,17 +825,31 @@ static inline uint32_t step_of(double step)
     return (uint32_t)(int)(step * 4294967296.0);
 }
 
-// After a synchronous call that ran a staged split: reports (and clears) a
-// bulk-copy wait that reached its bound in stage_ifft_kernel.
-static int stage_wait_check(const FftPlan *pl)
+// The calling thread's error word for staged launches (device, zeroed once).
+static int thread_stage_err(int **out, cudaStream_t st)
 {
-    if (!pl || pl->R <= 8) return SDRG_OK;
+    ThreadCtx &c = tctx();
+    if (!c.stage_err.ptr) {
+        int e;
+        if ((e = c.stage_err.reserve(sizeof(int)))) return e;
+        SDRG_CUDA(cudaMemsetAsync(c.stage_err.ptr, 0, sizeof(int), st));
+    }
+    *out = (int *)c.stage_err.ptr;
+    return SDRG_OK;
+}
+
+// After a synchronous call that ran a staged split (its work on st has
+// completed): reports, and clears, a bulk-copy wait of stage_ifft_kernel that
+// reached its bound, recorded in the error word err.
+static int stage_wait_check(const FftPlan *pl, int *err, cudaStream_t st)
+{
+    if (!pl || pl->R <= 8 || !err) return SDRG_OK;
     int v = 0;
-    cudaError_t ce = cudaMemcpyFromSymbol(&v, g_stage_wait_err, sizeof(int));
-    if (ce != cudaSuccess) return cuda_error(ce, "staged FFT status");
+    SDRG_CUDA(cudaMemcpyAsync(&v, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SDRG_CUDA(cudaStreamSynchronize(st));
     if (!v) return SDRG_OK;
-    const int z = 0;
-    cudaMemcpyToSymbol(g_stage_wait_err, &z, sizeof(int));
+    SDRG_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+    SDRG_CUDA(cudaStreamSynchronize(st));
     return set_error(SDRG_ERR_CUDA, "staged FFT: a bulk copy into shared memory did not "
                      "complete within its bound; results of that call are not valid");
 }
@@ -870,13 +912,14 @@ static int corr_fft_device(const char2 *iq_dev, const sdr_cpx_t *code_host, int 
     ca.pl = pl->k; ca.tw = pl->tw_dev; ca.split = pl->split_dev; ca.X = X;
     ca.code = code_perm; ca.n_prn = 1; ca.n_bin = 1; ca.n_sum = 1; ca.prn0 = 0;
     ca.scale = 1.0f / N / N; ca.Nmax = N; ca.Y = Y;
+    if ((e = thread_stage_err(&ca.stage_err, st))) return e;
     const int wt = staged_chunk(pl, 1);
     if (wt && (e = c.dev[5].reserve((size_t)wt * cb))) return e;
     if ((e = launch_consumer<1>(pl, ca, 1, st, wt ? (float2 *)c.dev[5].ptr : nullptr, wt)))
         return e;
     SDRG_CUDA(cudaMemcpyAsync(c.host[0].ptr, Y, cb, cudaMemcpyDeviceToHost, st));
     SDRG_CUDA(cudaStreamSynchronize(st));
-    if ((e = stage_wait_check(pl))) return e;
+    if ((e = stage_wait_check(pl, ca.stage_err, st))) return e;
     memcpy(corr_host, c.host[0].ptr, cb);
     return SDRG_OK;
 }
@@ -928,6 +971,7 @@ int corr_job_device(const uint8_t *buf, int len, const uint32_t *tab_dev, int N,
     ca.pl = pl->k; ca.tw = pl->tw_dev; ca.split = pl->split_dev; ca.X = X; ca.code = code_perm;
     ca.n_prn = 1; ca.n_bin = 1; ca.n_sum = 1; ca.prn0 = 0;
     ca.scale = 1.0f / N / N; ca.Nmax = N; ca.Y = corr;
+    if ((e = thread_stage_err(&ca.stage_err, st))) return e;
     const int wt = staged_chunk(pl, 1);
     return launch_consumer<1>(pl, ca, 1, st, wt ? W : nullptr, wt);
 }
@@ -991,6 +1035,7 @@ struct GroupState {
 struct sdrg_acq_plan {
     std::vector<sdrg::GroupState> g;
     int n_res = 0;
+    int *stage_err = nullptr;   // device error word of the staged launches
     int64_t cells = 0;
     // Signal groups run concurrently on internal streams forked from and
     // joined back to the caller's stream: a group whose clusters cannot use
@@ -1086,6 +1131,13 @@ static int prof_end(sdrg_acq_plan *plan, cudaStream_t st, cudaEvent_t *ev, int k
 using namespace sdrg;
 
 extern "C" {
+
+int sdrg_inject_stage_timeout(int n)
+{
+    if (n < 0) return set_error(SDRG_ERR_ARG, "sdrg_inject_stage_timeout: n=%d", n);
+    g_stage_timeouts.store(n);
+    return SDRG_OK;
+}
 
 int sdrg_acq_profile(sdrg_acq_plan_t *plan, int enable)
 {
@@ -1245,6 +1297,7 @@ void sdr_search_code(const sdr_cpx_t *code_fft, double T, const sdr_buff_t *buff
     ca.n_prn = 1; ca.n_bin = len_fds; ca.n_sum = 1; ca.prn0 = 0;
     ca.scale = 1.0f / N / N; ca.Nmax = N; ca.prn_stride = 0; ca.bin_stride = N;
     ca.accumulate = 1; ca.P = P_d;
+    if (thread_stage_err(&ca.stage_err, st)) return;
     const int wt = staged_chunk(pl, len_fds);
     if (wt && c.dev[5].reserve(staged_bytes(pl, wt, 0))) return;
     if (launch_consumer<0>(pl, ca, len_fds, st, wt ? (float2 *)c.dev[5].ptr : nullptr, wt))
@@ -1254,7 +1307,7 @@ void sdr_search_code(const sdr_cpx_t *code_fft, double T, const sdr_buff_t *buff
         cuda_error(cudaGetLastError(), "sdr_search_code D2H");
         return;
     }
-    if (stage_wait_check(pl)) return;           // P unchanged, error recorded
+    if (stage_wait_check(pl, ca.stage_err, st)) return;   // P unchanged, error recorded
     memcpy(P, c.host[2].ptr, pb);
 }
 
@@ -1278,6 +1331,8 @@ sdrg_acq_plan_t *sdrg_acq_plan_new(const sdrg_acq_sig_t *sigs, int n_sig)
         sok = cudaStreamCreateWithFlags(&plan->streams[i], cudaStreamNonBlocking) == cudaSuccess &&
               cudaEventCreateWithFlags(&plan->ev_join[i], cudaEventDisableTiming) == cudaSuccess;
     }
+    sok = sok && cudaMalloc(&plan->stage_err, sizeof(int)) == cudaSuccess &&
+          cudaMemsetAsync(plan->stage_err, 0, sizeof(int), st) == cudaSuccess;
     if (!sok) {
         cuda_error(cudaGetLastError(), "sdrg_acq_plan_new streams");
         sdrg_acq_plan_free(plan);
@@ -1371,6 +1426,7 @@ void sdrg_acq_plan_free(sdrg_acq_plan_t *plan)
         cudaStreamDestroy(s);
     }
     for (auto ev : plan->ev_join) if (ev) cudaEventDestroy(ev);
+    if (plan->stage_err) cudaFree(plan->stage_err);
     if (plan->ev_fork) cudaEventDestroy(plan->ev_fork);
     for (auto ev : plan->ev_pool) cudaEventDestroy(ev);
     for (auto &u : plan->ev_used) {
@@ -1487,6 +1543,7 @@ int sdrg_fft_autotune(int L, int *R_out, int *threads_out, double *ms_out)
         ca.n_prn = n_prn; ca.n_bin = n_bin; ca.n_sum = n_sum; ca.prn0 = 0;
         ca.scale = 1.0f / L / L; ca.Nmax = Nmax;
         ca.prn_stride = (size_t)n_bin * Nmax; ca.bin_stride = Nmax; ca.accumulate = 0; ca.P = P;
+        if ((e = thread_stage_err(&ca.stage_err, st))) break;
         if (pl->R > 1 && pl->R <= 8) {
             ca.Q = Q;
             ca.Mq = (Nmax + pl->R - 1) / pl->R;
@@ -1598,7 +1655,7 @@ static int launch_run(sdrg_acq_plan_t *plan, Device *dev, const uint8_t *const *
         ca.code = G.code; ca.n_prn = s.n_prn; ca.n_bin = nb; ca.n_sum = ns; ca.prn0 = 0;
         ca.scale = 1.0f / s.L / s.L; ca.Nmax = s.Nmax;
         ca.prn_stride = (size_t)nb * s.Nmax; ca.bin_stride = s.Nmax;
-        ca.accumulate = 0; ca.P = G.P; ca.Q = G.Q; ca.Mq = G.Mq;
+        ca.accumulate = 0; ca.P = G.P; ca.Q = G.Q; ca.Mq = G.Mq; ca.stage_err = plan->stage_err;
         if ((e = prof_begin(plan, st, ev))) return e;
         if ((e = launch_consumer<0>(G.pl, ca, s.n_prn * nb, st, G.W, G.w_tasks))) return e;
         // a staged split launches a combine and an inverse pass per chunk and sum
@@ -1734,7 +1791,8 @@ int sdrg_acq_run_host(sdrg_acq_plan_t *plan, const uint8_t *const *if_host, cons
                 cudaStreamSynchronize(st) != cudaSuccess))
         e = cuda_error(cudaGetLastError(), "sdrg_acq_run_host D2H");
     cudaStreamSynchronize(st);
-    for (size_t gi = 0; gi < plan->g.size() && !e; ++gi) e = stage_wait_check(plan->g[gi].pl);
+    for (size_t gi = 0; gi < plan->g.size() && !e; ++gi)
+        e = stage_wait_check(plan->g[gi].pl, plan->stage_err, st);
     for (auto p : bufs) if (p) cudaFree(p);
     if (res_dev) cudaFree(res_dev);
     return e;
@@ -1762,57 +1820,47 @@ constexpr size_t kNaBytes = kNaSplit + (size_t)kNaMaxM * sizeof(float2);
 // Every GPU that loads the library holds this array until the process exits.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
 
-struct NoallocDev {
-    unsigned char *base = nullptr;   // device address of g_noalloc_scratch
-    int N = 0;                       // length whose tables the array holds
-    FftPlan pl;                      // plan whose pointers point into it
-};
+// Device address of g_noalloc_scratch per device, looked up once with that
+// device current (the host-side symbol is not a device address).
 static std::mutex g_na_mtx;
-static NoallocDev g_na[64];
-// host staging for the tables (static, guarded by g_na_mtx: no heap use)
-static float2 g_na_tw_h[2 * kNaMaxM];
-static int g_na_kperm_h[kNaMaxM];
-static float2 g_na_split_h[kNaMaxM];
+static unsigned char *g_na_base[64];
 
-// Host-side tables of a length-N plan (same construction as get_plan's) into
-// the static staging arrays, without touching device memory.
-static int noalloc_tables(int N, FftPlan *pl)
+// The FFT tables of a length-N plan with pass structure k, written into the
+// fixed array by every call (so a call, or a CUDA-graph replay of one, never
+// meets another length's tables): the same values get_plan builds on the
+// host - per-pass twiddles exp(-2 pi i (i j mod Ls) / Ls), the digit-reversed
+// frequency index k(q) of each DIF output position and the split twiddles
+// exp(+2 pi i k(q) / N) - from double sincospi, rounded to float.
+__global__ void __launch_bounds__(256) na_tables_kernel(FftPlanK k, int N, float2 *tw,
+                                                        int *kperm, float2 *split)
 {
-    int R, M;
-    FftPlanK k;
-    if (!plan_shape(N, &R, &M, &k) || M > kNaMaxM || k.twtot > 2 * kNaMaxM)
-        return set_error(SDRG_ERR_ARG, "sdrg_corr_fft_noalloc: length %d has no plan "
-                         "within the fixed scratch", N);
-    pl->L = N; pl->R = R; pl->M = M; pl->k = k;
-    int t = 32;
-    while (t < 512 && t * 8 < M) t *= 2;
-    pl->threads = t;
-    pl->smem = (size_t)M * sizeof(float2) + (size_t)k.twtot * sizeof(float2) + 512;
-    float2 *tw = g_na_tw_h;
-    int *kperm = g_na_kperm_h;
-    float2 *split = g_na_split_h;
-    for (int p = 0; p < k.npass; ++p) {
-        const int Ls = k.Ls[p], r = k.radix[p], S = Ls / r, jmax = (p == 0) ? 1 : r - 1;
-        for (int j = 1; j <= jmax; ++j)
-            for (int i = 0; i < S; ++i) {
-                const double a = -2.0 * M_PI * (double)((long)i * j % Ls) / Ls;
-                tw[k.twoff[p] + (j - 1) * S + i] = make_float2((float)cos(a), (float)sin(a));
+    const int total = k.twtot + k.M;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        if (t < k.twtot) {
+            int p = 0;
+            while (p + 1 < k.npass && t >= k.twoff[p + 1]) ++p;
+            const int Ls = k.Ls[p], S = Ls / k.radix[p], loc = t - k.twoff[p];
+            const int j = loc / S + 1, i = loc - (j - 1) * S;
+            const long e = (long)i * j % Ls;
+            double sn, cs;
+            sincospi(-2.0 * (double)e / Ls, &sn, &cs);
+            tw[t] = make_float2((float)cs, (float)sn);
+        } else {
+            const int q = t - k.twtot;
+            int rem = q, blk = k.M, kk = 0, mul = 1;
+            for (int p = 0; p < k.npass; ++p) {
+                blk /= k.radix[p];
+                const int j = rem / blk;
+                rem -= j * blk;
+                kk += j * mul;
+                mul *= k.radix[p];
             }
-    }
-    for (int q = 0; q < M; ++q) {
-        int rem = q, blk = M, kk = 0, mul = 1;
-        for (int p = 0; p < k.npass; ++p) {
-            blk /= k.radix[p];
-            const int j = rem / blk;
-            rem %= blk;
-            kk += j * mul;
-            mul *= k.radix[p];
+            kperm[q] = kk;
+            double sn, cs;
+            sincospi(2.0 * (double)kk / N, &sn, &cs);
+            split[q] = make_float2((float)cs, (float)sn);
         }
-        kperm[q] = kk;
-        const double a = 2.0 * M_PI * (double)kk / N;
-        split[q] = make_float2((float)cos(a), (float)sin(a));
     }
-    return SDRG_OK;
 }
 
 } // namespace sdrg
@@ -1824,48 +1872,50 @@ extern "C" int sdrg_corr_fft_noalloc(const sdr_cpx16_t *IQ_dev, const sdr_cpx_t 
         return set_error(SDRG_ERR_ARG, "sdrg_corr_fft_noalloc: N=%d outside 1..%d", N, kNaMaxN);
     if (!IQ_dev || !code_fft_dev || !corr_dev)
         return set_error(SDRG_ERR_ARG, "sdrg_corr_fft_noalloc: null pointer");
+    // the default cluster split of N (schedules do not apply here)
+    FftPlan pl;
+    int R, M;
+    FftPlanK k;
+    if (!cluster_shape(N, &R, &M, &k) || M > kNaMaxM || k.twtot > 2 * kNaMaxM)
+        return set_error(SDRG_ERR_ARG, "sdrg_corr_fft_noalloc: length %d has no plan "
+                         "within the fixed scratch", N);
     cudaStream_t st = (cudaStream_t)stream;
     int dev = 0;
     SDRG_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) return set_error(SDRG_ERR_ARG, "device %d out of range", dev);
-    std::lock_guard<std::mutex> lk(g_na_mtx);
-    NoallocDev &S = g_na[dev];
-    if (!S.base) {
-        // set-up, once per device, with that device current
-        void *p = nullptr;
-        SDRG_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-        S.base = (unsigned char *)p;
+    unsigned char *base;
+    {
+        std::lock_guard<std::mutex> lk(g_na_mtx);
+        if (!g_na_base[dev]) {
+            // set-up, once per device, with that device current
+            void *p = nullptr;
+            SDRG_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+            g_na_base[dev] = (unsigned char *)p;
+        }
+        base = g_na_base[dev];
     }
-    if (S.N != N) {
-        int e;
-        S.N = 0;
-        if ((e = noalloc_tables(N, &S.pl))) return e;
-        S.pl.tw_dev = (float2 *)(S.base + kNaTw);
-        S.pl.kperm_dev = (int *)(S.base + kNaKperm);
-        S.pl.split_dev = (float2 *)(S.base + kNaSplit);
-        const int M = S.pl.M, ntw = S.pl.k.twtot > 0 ? S.pl.k.twtot : 1;
-        // stream-ordered uploads from pageable memory: each call returns once
-        // the host data is staged, so the staging arrays may be reused
-        SDRG_CUDA(cudaMemcpyAsync(S.pl.tw_dev, g_na_tw_h, ntw * sizeof(float2),
-                                  cudaMemcpyHostToDevice, st));
-        SDRG_CUDA(cudaMemcpyAsync(S.pl.kperm_dev, g_na_kperm_h, M * sizeof(int),
-                                  cudaMemcpyHostToDevice, st));
-        SDRG_CUDA(cudaMemcpyAsync(S.pl.split_dev, g_na_split_h, M * sizeof(float2),
-                                  cudaMemcpyHostToDevice, st));
-        S.N = N;
-    }
-    const FftPlan *pl = &S.pl;
-    float2 *code_perm = (float2 *)(S.base + kNaCode);
-    float2 *X = (float2 *)(S.base + kNaX);
+    pl.L = N; pl.R = R; pl.M = M; pl.k = k;
+    int t = 32;
+    while (t < 512 && t * 8 < M) t *= 2;
+    pl.threads = t;
+    pl.smem = (size_t)M * sizeof(float2) + (size_t)k.twtot * sizeof(float2) + 512;
+    pl.tw_dev = (float2 *)(base + kNaTw);
+    pl.kperm_dev = (int *)(base + kNaKperm);
+    pl.split_dev = (float2 *)(base + kNaSplit);
+    const int nt = k.twtot + M;
+    na_tables_kernel<<<(nt + 255) / 256, 256, 0, st>>>(k, N, pl.tw_dev, pl.kperm_dev, pl.split_dev);
+    SDRG_CUDA(cudaGetLastError());
+    float2 *code_perm = (float2 *)(base + kNaCode);
+    float2 *X = (float2 *)(base + kNaX);
     int e;
-    if ((e = perm_code(pl, (const float2 *)code_fft_dev, 1, code_perm, st))) return e;
+    if ((e = perm_code(&pl, (const float2 *)code_fft_dev, 1, code_perm, st))) return e;
     FwdArgs fa = {};
-    fa.pl = pl->k; fa.tw = pl->tw_dev; fa.ctab = nullptr; fa.R = pl->R;
+    fa.pl = pl.k; fa.tw = pl.tw_dev; fa.ctab = nullptr; fa.R = pl.R;
     fa.n_bin = 1; fa.n_sum = 1; fa.cscale = kCScale; fa.iq = (const char2 *)IQ_dev; fa.X = X;
-    if ((e = launch_fwd<1>(pl, fa, pl->R, st))) return e;
+    if ((e = launch_fwd<1>(&pl, fa, pl.R, st))) return e;
     ConsArgs ca = {};
-    ca.pl = pl->k; ca.tw = pl->tw_dev; ca.split = pl->split_dev; ca.X = X;
+    ca.pl = pl.k; ca.tw = pl.tw_dev; ca.split = pl.split_dev; ca.X = X;
     ca.code = code_perm; ca.n_prn = 1; ca.n_bin = 1; ca.n_sum = 1; ca.prn0 = 0;
     ca.scale = 1.0f / N / N; ca.Nmax = N; ca.Y = (float2 *)corr_dev;
-    return launch_cons<1>(pl, ca, 1, st);
+    return launch_cons<1>(&pl, ca, 1, st);
 }

@@ -93,3 +93,60 @@ def test_plan_alloc_failure_returns_null(gpu):
     plan = acquire.AcqPlan(wl.groups, cfs)        # and the next plan builds
     assert plan.cells > 0
     lib.sdrg_inject_alloc_failure(-1)
+
+
+CUDA_ERR = -2
+
+
+def test_staged_copy_wait_bound_reported_and_cleared(gpu, ref):
+    """The bounded waits for the bulk copies of a staged split (480 000
+    points = 20 x 24 000): with sdrg_inject_stage_timeout the first wait of
+    each copy gives up at once (the copies still land and are waited for in
+    full). The synchronous drop-ins then report SDRG_ERR_CUDA - sdr_corr_fft
+    zero-fills its output, sdr_search_code leaves P unchanged - and the next
+    call, with the normal bound, runs and matches the reference."""
+    import ctypes as C
+    from pocketsdr_b200 import codes
+    from pocketsdr_b200._lib import SdrBuff, last_error, lib, ptr
+    N = 480000
+    rng = np.random.default_rng(17)
+    IQ = rng.integers(-60, 61, (N, 2), dtype=np.int8)
+    cf = (rng.standard_normal(N) + 1j * rng.standard_normal(N)).astype(np.complex64)
+    corr = np.full(N, 3.0, np.complex64)
+
+    def corr_fft():
+        lib.sdr_corr_fft(ptr(IQ), ptr(cf), N, ptr(corr))
+        code, msg = last_error()
+        lib.sdr_gpu_clear_error()
+        return code, msg
+
+    assert lib.sdrg_inject_stage_timeout(1) == 0
+    code, msg = corr_fft()
+    assert code == CUDA_ERR and "bulk copy" in msg, (code, msg)
+    assert not corr.any()
+    code, _ = corr_fft()
+    assert code == 0
+    want = ref.corr_fft(IQ, cf)
+    rms = float(np.sqrt(np.mean(np.abs(want) ** 2)))
+    assert np.all(np.abs(corr - want) <= 1e-4 * np.maximum(np.abs(want), rms))
+
+    # sdr_search_code over a 480 000-sample window, 2 bins
+    fs, fi, T = 48e6, 0.0, 10e-3
+    buf = ((rng.integers(-7, 8, N) & 0x0F) | ((rng.integers(-7, 8, N) & 0x0F) << 4)).astype(np.uint8)
+    sb = SdrBuff(buf.ctypes.data_as(C.POINTER(C.c_uint8)), 2, len(buf))
+    code_fft = np.ascontiguousarray(cf)
+    fds = np.array([-50.0, 50.0], np.float32)
+    P = np.full((2, N), 5.0, np.float32)
+    assert lib.sdrg_inject_stage_timeout(1) == 0
+    lib.sdr_search_code(ptr(code_fft), T, C.byref(sb), 0, N, fs, fi, ptr(fds), 2, ptr(P))
+    code, msg = last_error()
+    lib.sdr_gpu_clear_error()
+    assert code == CUDA_ERR and "bulk copy" in msg
+    assert np.all(P == 5.0)
+    lib.sdr_search_code(ptr(code_fft), T, C.byref(sb), 0, N, fs, fi, ptr(fds), 2, ptr(P))
+    assert last_error()[0] == 0
+    Pr = np.full((2, N), 5.0, np.float32)
+    ref.search_code(code_fft, buf, 0, N, fs, fi, fds, Pr, T)
+    floor = float(Pr.mean())
+    assert np.all(np.abs(P - Pr) <= 1e-4 * np.maximum(np.abs(Pr), floor))
+    assert lib.sdrg_inject_stage_timeout(0) == 0

@@ -270,3 +270,30 @@ def test_csk_restatement_vs_reference(orc):
     # no power anywhere: symbol of shift 0
     z = np.zeros(24000, np.complex64)
     assert R.csk(z, Lc, [0.0])[0] == orc.csk(z, Lc, [0.0])[0] == 255
+
+
+@pytest.mark.skipif(not HAVE_REF, reason="reference build (oracle/_ref) not present")
+def test_fine_dop_closed_form_matches_reference_lsq():
+    """The library's sdr_fine_dop (host; the vertex of the parabola through
+    three points, in closed form) against the reference's RTKLIB least-squares
+    fit (src/sdr_func.c:709-744) on random grids, bins and spacings, at a
+    local maximum along Doppler - what sdr_corr_max hands it: within 1e-9
+    relative (the two FP64 evaluations differ by rounding only; far from a
+    maximum the parabola flattens, its vertex runs off, and both fits lose
+    digits to the conditioning)."""
+    import ctypes as C
+    from pocketsdr_b200 import _lib
+    R = oracle.Reference()
+    rng = np.random.default_rng(11)
+    for _ in range(3000):
+        step = float(rng.choice([50.0, 62.5, 125.0, 250.0, 500.0]))
+        M, N = 41, 7
+        fds = (np.arange(M) * step - 20 * step + float(rng.choice([0.0, 3.0]))).astype(np.float32)
+        P = (rng.random((M, N)) * 1e6).astype(np.float32)
+        b, o = int(rng.integers(0, M)), int(rng.integers(0, N))
+        P[b, o] = P[max(b - 1, 0):b + 2, o].max() * np.float32(1.0 + rng.random())
+        ix = np.array([b, o], np.int32)
+        want = R.fine_dop(P, N, fds, (b, o))
+        got = _lib.lib.sdr_fine_dop(C.c_void_p(P.ctypes.data), N, C.c_void_p(fds.ctypes.data), M,
+                                    C.c_void_p(ix.ctypes.data))
+        assert abs(got - want) <= 1e-9 * max(abs(want), 1.0), (b, o, got, want)

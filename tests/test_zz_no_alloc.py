@@ -1,12 +1,14 @@
-"""sdrg_corr_fft_noalloc: the FFT correlator for callers that cannot allocate
-device memory when they call (inside a stream capture, on a real-time receiver
-thread that must not stall on cudaMalloc's device synchronisation, or with
-device memory from their own pool). It keeps every intermediate in one fixed
+"""sdrg_corr_fft_noalloc: the FFT correlator for callers that cannot call
+cudaMalloc - a real-time receiver channel thread that must not stall on the
+device synchronisation an allocation may bring, or an application whose device
+memory all comes from its own pool. It keeps every intermediate in one fixed
 device array, so this test owns the input and output buffers (torch tensors)
-and checks the entry point through the C ABI against the allocating
-sdr_corr_fft on two calls in a row, within the FFT-correlator tolerance of the
-other parity tests. Collected last on purpose (file name), so a failure here
-comes after every other test has run.
+and checks the entry point through the C ABI against the oracle's corr_fft
+(the reference's sdr_corr_fft, src/sdr_func.c:1088-1102) and against the
+library's allocating sdr_corr_fft, on calls in a row whose lengths alternate
+(each call must rebuild the tables it reads in the shared array), within the
+FFT-correlator tolerance of the other parity tests. Collected last on purpose
+(file name), so a failure here comes after every other test has run.
 """
 import ctypes as C
 
@@ -36,22 +38,47 @@ def _noalloc(lib, torch, IQ, cf, stream):
     return rc, d_out.cpu().numpy().view(np.complex64)
 
 
-def test_corr_fft_noalloc_matches_allocating_entry():
+def test_corr_fft_noalloc_matches_oracle_and_allocating_entry():
     torch = pytest.importorskip("torch")
+    from oracle import oracle
     from pocketsdr_b200 import sdr_func
     from pocketsdr_b200._lib import lib, torch_stream
     sdr_func.init()
+    R = oracle.best()
     stream = torch_stream()
     rng = np.random.default_rng(2024)
-    # two calls in a row: a new length (tables uploaded), then the same length
-    # with new data (array contents of the previous call left behind)
-    for N in (48000, 48000, 4000):
+    # calls in a row: a length, the same length with new data, another
+    # length, back to the first (the shared array holds the previous call's
+    # tables and data each time)
+    for N in (48000, 48000, 4000, 48000, 65536, 6000):
         IQ = rng.integers(-100, 101, (N, 2), dtype=np.int8)
         cf = (rng.standard_normal(N) + 1j * rng.standard_normal(N)).astype(np.complex64)
-        expected = sdr_func.sdr_corr_fft(IQ, cf)
         rc, got = _noalloc(lib, torch, IQ, cf, stream)
-        assert rc == 0, rc
-        assert _close(got, expected), N
+        assert rc == 0, (N, rc)
+        assert _close(got, R.corr_fft(IQ, cf)), N
+        assert _close(got, sdr_func.sdr_corr_fft(IQ, cf)), N
+
+
+def test_corr_fft_noalloc_ignores_schedules():
+    """A schedule that sends a length to a staged split (R > 8) applies to
+    sdr_corr_fft, not to this entry, which keeps the default cluster split."""
+    torch = pytest.importorskip("torch")
+    from oracle import oracle
+    from pocketsdr_b200 import sdr_func
+    from pocketsdr_b200._lib import lib, torch_stream
+    sdr_func.init()
+    R = oracle.best()
+    N = 48000
+    assert lib.sdrg_fft_schedule_set(N, 10, 256) == 0
+    try:
+        rng = np.random.default_rng(7)
+        IQ = rng.integers(-100, 101, (N, 2), dtype=np.int8)
+        cf = (rng.standard_normal(N) + 1j * rng.standard_normal(N)).astype(np.complex64)
+        rc, got = _noalloc(lib, torch, IQ, cf, torch_stream())
+        assert rc == 0
+        assert _close(got, R.corr_fft(IQ, cf))
+    finally:
+        lib.sdrg_fft_schedule_set(N, 0, 0)
 
 
 def test_corr_fft_noalloc_rejects_oversize():
