@@ -630,6 +630,12 @@ def run_ours(args):
         keep = ("value", "unit", "ms_per_step", "steps", "config", "e2e", "gpu_launches",
                 "roofline", "clocks", "detected", "cpu_baseline", "parity")
         line["extra"] = {"acq_l1ca_12mhz": {k: sub[k] for k in keep if k in sub}}
+        # refinement after the grid (64 signals at 12 MHz): its cost against
+        # the plain grid search and its agreement with the FP64 oracle
+        rf = refine_measure(args, 10, 3, with_oracle=cpu_leg, with_cpu=False)
+        keep = ("value", "unit", "ms_per_step", "grid_ms", "refine_ms", "cost_vs_grid", "e2e",
+                "config", "vs_fp64_oracle", "vs_truth", "clocks", "roofline")
+        line["extra"]["refine_12mhz"] = {k: rf[k] for k in keep if k in rf}
     if rank == 0:
         emit(line)
     if dist:
@@ -938,13 +944,15 @@ def _fp64_refine(wl, th0, models):
     return out, time.perf_counter() - t0, cores
 
 
-def run_refine(args):
+def refine_measure(args, steps: int, warmup: int, with_oracle: bool = True,
+                   with_cpu: bool = True) -> dict:
     """Differentiable-refinement workload: 64 GPS L1 C/A + Galileo E1-B
     signals at 12 MHz (C/N0 30-45 dB-Hz, off-grid delay and Doppler). A step
     is the plain grid search (10 ms / 8 ms coherent, +-5 kHz) of all 64 PRNs
     followed by 5 Gauss-Newton steps from its peaks; the line reports both
     parts, their cost ratio and the refinement's agreement with the FP64
-    oracle and with the truth."""
+    oracle and with the truth (with_oracle) and, with with_cpu, the CPU
+    baseline (reference grid + FP64 oracle Gauss-Newton)."""
     import torch
     from pocketsdr_b200 import acquire, codes, synth
     from pocketsdr_b200.refine import RefinePlan, RefineSpec
@@ -972,14 +980,14 @@ def run_refine(args):
         plan.from_peaks(res_d, 0, wl.ix0, theta, rate)
         plan.gn(buf_d, wl.ix0, theta, rate, models, info=False)
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         grid()
         refine()
     torch.cuda.synchronize()
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(steps)]
     clk = ClockSampler(local)
     clk.start()
-    for k in range(args.steps):
+    for k in range(steps):
         flush.fill_(k & 0xFF)
         ev[k][0].record(st)
         grid()
@@ -988,8 +996,8 @@ def run_refine(args):
         ev[k][2].record(st)
     torch.cuda.synchronize()
     clocks = clk.stop()
-    grid_ms = sum(e[0].elapsed_time(e[1]) for e in ev) / args.steps
-    ref_ms = sum(e[1].elapsed_time(e[2]) for e in ev) / args.steps
+    grid_ms = sum(e[0].elapsed_time(e[1]) for e in ev) / steps
+    ref_ms = sum(e[1].elapsed_time(e[2]) for e in ev) / steps
     # the sums kernel alone (mode 1), for its roofline
     s_ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     flush.fill_(1)
@@ -1006,8 +1014,8 @@ def run_refine(args):
     buf_h = torch.from_numpy(wl.buf).pin_memory()
     th_h = torch.empty((n, 3), dtype=torch.float64).pin_memory()
     e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-              for _ in range(args.steps)]
-    for k in range(args.steps):
+              for _ in range(steps)]
+    for k in range(steps):
         flush.fill_((k + 1) & 0xFF)
         e2e_ev[k][0].record(st)
         buf_d.copy_(buf_h, non_blocking=True)
@@ -1016,7 +1024,7 @@ def run_refine(args):
         th_h.copy_(theta, non_blocking=True)
         e2e_ev[k][1].record(st)
     torch.cuda.synchronize()
-    e2e_ms = sum(a.elapsed_time(b) for a, b in e2e_ev) / args.steps
+    e2e_ms = sum(a.elapsed_time(b) for a, b in e2e_ev) / steps
 
     # parity with the FP64 oracle from the same starting peaks, and the truth
     res = np.frombuffer(res_d.cpu().numpy().tobytes(), dtype=acquire.RESULT_DTYPE)
@@ -1025,7 +1033,7 @@ def run_refine(args):
     plan.gn(buf_d, wl.ix0, theta, rate, models, info=False)
     th = theta.cpu().numpy()
     line_extra = {}
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and with_oracle:
         th_ref, cpu_gn_s, cores = _fp64_refine(wl, th0, models)
         div = np.array([2.0 if s.sig == "E1B" else 1.0 for s in wl.sats])
         rn = np.array([synth.code_rate(s.sig) for s in wl.sats])
@@ -1048,7 +1056,7 @@ def run_refine(args):
             "within_5hz": int(np.sum(np.abs(th[ok, 1] - fd_t[ok]) < 5.0)),
             "start_rms_dtau_chip": float(np.sqrt(np.mean(e0_tau[ok] ** 2))),
             "start_rms_dfd_hz": float(np.sqrt(np.mean((th0[ok, 1] - fd_t[ok]) ** 2)))}
-        if world == 1:
+        if world == 1 and with_cpu:
             class _W:   # the grid's groups / buffers in cpu_reference_rate's shape
                 groups, bufs = wl.groups, [wl.buf]
             rate_c, cores_c, kind, desc = cpu_reference_rate(_W, budget_prn=4)
@@ -1064,7 +1072,7 @@ def run_refine(args):
     samples = n * wl.K * wl.Nb
     achieved = REFINE_FLOPS_PER_SAMPLE * samples / (sums_ms / 1e3) / 1e12
     line = {"metric": REFINE_METRIC, "value": value, "unit": "signals/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+            "steps": steps, "warmup": warmup, "ms_per_step": step_ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
             "config": {"workload": "refine_12mhz", "signals": n, "coherent_ms": 10, "blocks": wl.K,
@@ -1089,12 +1097,19 @@ def run_refine(args):
     grid()
     torch.cuda.synchronize()
     line["gpu_launches"] = (sum(v[1] for k, v in acq.profile_get().items() if k[0] != "span")
-                            + 1 + 2 * len(models)) * args.steps
+                            + 1 + 2 * len(models)) * steps
     acq.profile(False)
-    if rank == 0:
-        emit(line)
     plan.close()
     acq.close()
+    return line
+
+
+def run_refine(args):
+    rank, _, _ = dist_info()
+    line = refine_measure(args, args.steps, args.warmup, with_oracle=not args.no_cpu_baseline,
+                          with_cpu=not args.no_cpu_baseline)
+    if rank == 0:
+        emit(line)
     return 0
 
 

@@ -25,14 +25,22 @@ __device__ __forceinline__ int sgn_mul8(int x, int c)
 }
 __device__ __forceinline__ int neg8(int c) { return c == -128 ? -128 : -c; }
 
-// one block per (tap, half); blockDim.x = 256
+// Shift and code bank of every tap, passed by value (at most SDR_MAX_CORR).
+struct TapArgs {
+    int n;
+    int2 jk[SDR_MAX_CORR];
+};
+
+// One block per (tap, half), blockDim.x = 256: the half-dot products of the
+// tap (c12[2 tap + h]); the last block to finish then applies the polarity
+// test and the scaling for every tap (corr[n], C[2]) and re-arms the ticket.
 template <int CPX>
-__global__ void __launch_bounds__(256) corr_half_kernel(
-    const char2 *__restrict__ IQ, const char2 *__restrict__ code, int N,
-    const int2 *__restrict__ jk, float cs, float2 *__restrict__ c12)
+__global__ void __launch_bounds__(256) corr_std_kernel(
+    const char2 *__restrict__ IQ, const char2 *__restrict__ code, int N, TapArgs ta, float cs,
+    float2 *c12, unsigned *ticket, float2 *corr, float2 *C)
 {
     const int tap = blockIdx.x, h = blockIdx.y;
-    const int j = jk[tap].x, k = jk[tap].y;
+    const int j = ta.jk[tap].x, k = ta.jk[tap].y;
     const int len = h == 0 ? j : N - j;
     const char2 *x = IQ + (h == 0 ? 0 : j);
     const char2 *y = code + (size_t)k * N + (h == 0 ? N - j : 0);
@@ -54,6 +62,7 @@ __global__ void __launch_bounds__(256) corr_half_kernel(
         si += __shfl_xor_sync(0xffffffffu, si, o);
     }
     __shared__ int red[2][8];
+    __shared__ bool last;
     const int w = threadIdx.x >> 5;
     if ((threadIdx.x & 31) == 0) { red[0][w] = sr; red[1][w] = si; }
     __syncthreads();
@@ -61,6 +70,7 @@ __global__ void __launch_bounds__(256) corr_half_kernel(
         int tr = 0, ti = 0;
         for (int i = 0; i < (int)(blockDim.x >> 5); ++i) { tr += red[0][i]; ti += red[1][i]; }
         float fr = (float)tr, fi = (float)ti;
+        // the tail in float, one product at a time, in the reference's order
         for (int i = main_len; i < len; ++i) {
             const char2 a = x[i], c = y[i];
             if (CPX) {
@@ -72,26 +82,29 @@ __global__ void __launch_bounds__(256) corr_half_kernel(
             }
         }
         c12[2 * tap + h] = make_float2(__fmul_rn(fr, cs), __fmul_rn(fi, cs));
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == gridDim.x * gridDim.y - 1;
     }
-}
-
-__global__ void corr_finish_kernel(const float2 *__restrict__ c12, int n, int N,
-                                   float2 *__restrict__ corr, float2 *__restrict__ C)
-{
+    __syncthreads();
+    if (!last) return;
+    // every block's c12 is visible (each fenced its store before its ticket)
+    __threadfence();
     __shared__ float sign;
+    const int n = ta.n;
     if (threadIdx.x == 0) {
         float dot = 0.0f;
         for (int i = 0; i < 3 && i < n; ++i) {
-            const float2 a = c12[2 * i], b = c12[2 * i + 1];
+            const float2 a = __ldcg(c12 + 2 * i), b = __ldcg(c12 + 2 * i + 1);
             dot = __fadd_rn(dot, __fmaf_rn(a.x, b.x, __fmul_rn(a.y, b.y)));
         }
         sign = dot < 0.0f ? -1.0f : 1.0f;
-        if (C && n > 0) { C[0] = c12[0]; C[1] = c12[1]; }
+        if (n > 0) { C[0] = __ldcg(c12); C[1] = __ldcg(c12 + 1); }
+        *ticket = 0u;
     }
     __syncthreads();
     const float fN = (float)N;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const float2 a = c12[2 * i], b = c12[2 * i + 1];
+        const float2 a = __ldcg(c12 + 2 * i), b = __ldcg(c12 + 2 * i + 1);
         corr[i] = make_float2(__fdiv_rn(__fadd_rn(a.x, __fmul_rn(sign, b.x)), fN),
                               __fdiv_rn(__fadd_rn(a.y, __fmul_rn(sign, b.y)), fN));
     }
@@ -122,62 +135,134 @@ static bool tap_params(int N, double coff, const double *pos, int n, int nbank, 
     return true;
 }
 
-// IQ_dev / code_dev already on the device; results to host corr / C.
-static int corr_std_device(const char2 *IQ_dev, const char2 *code_dev, int N, int nbank,
-                           double coff, const double *pos, int n, int cpx,
-                           sdr_cpx_t *corr, sdr_cpx_t *C, cudaStream_t st)
+// The thread's device scratch of the synchronous correlators: c12 partials
+// (2 SDR_MAX_CORR), outputs (SDR_MAX_CORR + 2) and the finishing ticket
+// (zeroed once; the finishing block leaves it 0).
+static int corr_scratch(float2 **c12, float2 **out, unsigned **ticket, cudaStream_t st)
 {
-    if (n <= 0) return SDRG_OK;
-    if (n > SDR_MAX_CORR) return set_error(SDRG_ERR_ARG, "corr_std: n=%d > %d", n, SDR_MAX_CORR);
     ThreadCtx &c = tctx();
+    const size_t bytes = sizeof(float2) * (3 * SDR_MAX_CORR + 2) + 16;
+    const bool fresh = c.corr_dev.size < bytes;
     int e;
-    c.host[2].pinned = true;
-    const size_t jkb = sizeof(int2) * n, outb = sizeof(float2) * (n + 2);
-    if ((e = c.host[2].reserve(jkb + outb + 64)) || (e = c.dev[5].reserve(jkb + sizeof(float2) * 2 * n + outb + 64)))
-        return e;
-    int2 *jk_h = (int2 *)c.host[2].ptr;
-    if (!tap_params(N, coff, pos, n, nbank, jk_h))
-        return set_error(SDRG_ERR_ARG, "corr_std: a tap shift leaves [-N, 2N) or the code bank");
-    int2 *jk_d = (int2 *)c.dev[5].ptr;
-    float2 *c12 = (float2 *)(jk_d + n);
-    float2 *out_d = c12 + 2 * n;     // corr[n], C[2]
-    float2 *out_h = (float2 *)(jk_h + n);
-    SDRG_CUDA(cudaMemcpyAsync(jk_d, jk_h, jkb, cudaMemcpyHostToDevice, st));
-    if (cpx) corr_half_kernel<1><<<dim3(n, 2), 256, 0, st>>>(IQ_dev, code_dev, N, jk_d, kCScale, c12);
-    else     corr_half_kernel<0><<<dim3(n, 2), 256, 0, st>>>(IQ_dev, code_dev, N, jk_d, kCScale, c12);
+    if ((e = c.corr_dev.reserve(bytes))) return e;
+    *c12 = (float2 *)c.corr_dev.ptr;
+    *out = *c12 + 2 * SDR_MAX_CORR;
+    *ticket = (unsigned *)(*out + SDR_MAX_CORR + 2);
+    if (fresh) SDRG_CUDA(cudaMemsetAsync(*ticket, 0, sizeof(unsigned), st));
+    return SDRG_OK;
+}
+
+// IQ_dev / code_dev on the device, tap shifts in ta; results to host corr / C
+// through the pinned staging `out_h` (n + 2 values). One launch.
+static int corr_std_run(const char2 *IQ_dev, const char2 *code_dev, int N, const TapArgs &ta,
+                        int cpx, float2 *out_h, sdr_cpx_t *corr, sdr_cpx_t *C, cudaStream_t st)
+{
+    const int n = ta.n;
+    float2 *c12, *out_d;
+    unsigned *ticket;
+    int e;
+    if ((e = corr_scratch(&c12, &out_d, &ticket, st))) return e;
+    if (cpx) corr_std_kernel<1><<<dim3(n, 2), 256, 0, st>>>(IQ_dev, code_dev, N, ta, kCScale, c12,
+                                                           ticket, out_d, out_d + n);
+    else     corr_std_kernel<0><<<dim3(n, 2), 256, 0, st>>>(IQ_dev, code_dev, N, ta, kCScale, c12,
+                                                           ticket, out_d, out_d + n);
     SDRG_CUDA(cudaGetLastError());
-    corr_finish_kernel<<<1, 128, 0, st>>>(c12, n, N, out_d, out_d + n);
-    SDRG_CUDA(cudaGetLastError());
-    SDRG_CUDA(cudaMemcpyAsync(out_h, out_d, outb, cudaMemcpyDeviceToHost, st));
+    SDRG_CUDA(cudaMemcpyAsync(out_h, out_d, sizeof(float2) * (n + 2), cudaMemcpyDeviceToHost, st));
     SDRG_CUDA(cudaStreamSynchronize(st));
     memcpy(corr, out_h, sizeof(float2) * n);
     if (C) memcpy(C, out_h + n, sizeof(float2) * 2);
     return SDRG_OK;
 }
 
+constexpr int kBankCacheMax = 16;
+
+// The device copy of the caller's code bank (pointer, N): every bank a tap
+// selects (mask) is on the device and equal, byte for byte, to the caller's
+// bank once the uploads queued on st (staged through `stage`, SDR_N_CODES x
+// 2N bytes of pinned memory) have run.
+static int bank_on_device(const sdr_cpx16_t *code, int N, uint32_t mask, uint8_t *stage,
+                          cudaStream_t st, const char2 **dev_out)
+{
+    ThreadCtx &c = tctx();
+    const size_t bb = (size_t)N * 2;                 // bytes per bank
+    BankCache *bc = nullptr;
+    for (BankCache *b : c.banks)
+        if (b->key == code && b->N == N) { bc = b; break; }
+    if (!bc) {
+        if ((int)c.banks.size() >= kBankCacheMax) {   // evict the least recently used
+            size_t lru = 0;
+            for (size_t i = 1; i < c.banks.size(); ++i)
+                if (c.banks[i]->used < c.banks[lru]->used) lru = i;
+            SDRG_CUDA(cudaStreamSynchronize(st));
+            delete c.banks[lru];
+            c.banks.erase(c.banks.begin() + (long)lru);
+        }
+        int fe;
+        if ((fe = alloc_fault("cudaMalloc"))) return fe;
+        void *d = nullptr;
+        SDRG_CUDA(cudaMalloc(&d, bb * SDR_N_CODES));
+        bc = new BankCache();
+        bc->key = code;
+        bc->N = N;
+        bc->dev = d;
+        bc->host.resize(bb * SDR_N_CODES);
+        c.banks.push_back(bc);
+    }
+    bc->used = ++c.bank_clock;
+    const uint8_t *src = (const uint8_t *)code;
+    for (int k = 0; k < SDR_N_CODES; ++k) {
+        if (!((mask >> k) & 1u)) continue;
+        const size_t off = (size_t)k * bb;
+        if (((bc->valid >> k) & 1u) && memcmp(bc->host.data() + off, src + off, bb) == 0) continue;
+        memcpy(bc->host.data() + off, src + off, bb);
+        memcpy(stage + off, src + off, bb);
+        bc->valid |= 1u << k;
+        SDRG_CUDA(cudaMemcpyAsync((uint8_t *)bc->dev + off, stage + off, bb,
+                                  cudaMemcpyHostToDevice, st));
+    }
+    *dev_out = (const char2 *)bc->dev;
+    return SDRG_OK;
+}
+
+// sdr_corr_std / sdr_corr_std_cpx_code: IQ staged and uploaded, the selected
+// code banks resident on the device (uploaded when their bytes change), one
+// launch, results back.
 static void corr_std_host(const sdr_cpx16_t *IQ, const sdr_cpx16_t *code, int N, double coff,
                           const double *pos, int n, sdr_cpx_t *corr, sdr_cpx_t *C, int cpx)
 {
     if (N <= 0 || n <= 0) return;
     cudaStream_t st;
     ThreadCtx &c = tctx();
+    TapArgs ta;
+    uint32_t mask = 0;
     const size_t iqb = (size_t)N * 2, cb = (size_t)N * 2 * SDR_N_CODES;
     c.host[0].pinned = true;
+    c.host[2].pinned = true;
+    if (n > SDR_MAX_CORR) {
+        set_error(SDRG_ERR_ARG, "corr_std: n=%d > %d", n, SDR_MAX_CORR);
+        goto fail;
+    }
+    ta.n = n;
+    if (!tap_params(N, coff, pos, n, SDR_N_CODES, ta.jk)) {
+        set_error(SDRG_ERR_ARG, "corr_std: a tap shift leaves [-N, 2N) or the code bank");
+        goto fail;
+    }
+    for (int i = 0; i < n; ++i) mask |= 1u << ta.jk[i].y;
     // a failing step has recorded its error in the thread's last-error state
-    if (ensure_device(nullptr) || thread_stream(&st) ||
-        c.host[0].reserve(iqb + cb + 16) || c.dev[0].reserve(iqb + cb + 16))
+    if (ensure_device(nullptr) || thread_stream(&st) || c.host[0].reserve(iqb + cb + 16) ||
+        c.dev[0].reserve(iqb + 16) || c.host[2].reserve(sizeof(float2) * (SDR_MAX_CORR + 2)))
         goto fail;
     {
         uint8_t *h = (uint8_t *)c.host[0].ptr;
+        const char2 *code_d = nullptr;
+        if (bank_on_device(code, N, mask, h + iqb, st, &code_d)) goto fail;
         memcpy(h, IQ, iqb);
-        memcpy(h + iqb, code, cb);
-        uint8_t *d = (uint8_t *)c.dev[0].ptr;
-        if (cudaMemcpyAsync(d, h, iqb + cb, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+        if (cudaMemcpyAsync(c.dev[0].ptr, h, iqb, cudaMemcpyHostToDevice, st) != cudaSuccess) {
             cuda_error(cudaGetLastError(), "corr_std H2D");
             goto fail;
         }
-        if (corr_std_device((const char2 *)d, (const char2 *)(d + iqb), N, SDR_N_CODES, coff,
-                            pos, n, cpx, corr, C, st))
+        if (corr_std_run((const char2 *)c.dev[0].ptr, code_d, N, ta, cpx, (float2 *)c.host[2].ptr,
+                         corr, C, st))
             goto fail;
     }
     return;
@@ -237,7 +322,21 @@ void sdr_corr_std_cpx(const sdr_cpx_t *buff, int len_buff, int ix, int N, double
     // the reference passes a single bank (src/sdr_func.c:1070); a tap whose
     // fractional shift selects another bank reads past it there and is
     // rejected here
-    if (corr_std_device(iq_d, code_d, N, 1, 0.0, pos, n, 0, corr, Cb, st)) {
+    TapArgs ta;
+    ta.n = n;
+    c.host[2].pinned = true;
+    if (n > SDR_MAX_CORR) {
+        set_error(SDRG_ERR_ARG, "corr_std: n=%d > %d", n, SDR_MAX_CORR);
+        memset(corr, 0, sizeof(sdr_cpx_t) * n);
+        return;
+    }
+    if (!tap_params(N, 0.0, pos, n, 1, ta.jk)) {
+        set_error(SDRG_ERR_ARG, "corr_std: a tap shift leaves [-N, 2N) or the code bank");
+        memset(corr, 0, sizeof(sdr_cpx_t) * n);
+        return;
+    }
+    if (c.host[2].reserve(sizeof(float2) * (SDR_MAX_CORR + 2)) ||
+        corr_std_run(iq_d, code_d, N, ta, 0, (float2 *)c.host[2].ptr, corr, Cb, st)) {
         memset(corr, 0, sizeof(sdr_cpx_t) * n);
     }
 }

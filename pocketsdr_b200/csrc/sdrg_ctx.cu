@@ -140,6 +140,16 @@ int thread_stream(cudaStream_t *s)
     return SDRG_OK;
 }
 
+BankCache::~BankCache()
+{
+    if (dev) cudaFree(dev);      // at thread exit; errors ignored
+}
+
+ThreadCtx::~ThreadCtx()
+{
+    for (BankCache *b : banks) delete b;
+}
+
 Scratch::~Scratch()
 {
     // Released at thread exit; errors are ignored (the context may be gone).

@@ -54,13 +54,33 @@ struct Scratch {
     int reserve(size_t bytes);
 };
 
+// A tracking channel's code bank ([SDR_N_CODES][N] sdr_cpx16_t, host memory
+// of the caller) kept on the device by the synchronous correlators of one
+// host thread: `host` holds the bytes each uploaded bank had, so a later call
+// uploads a bank only when the caller's bytes differ.
+struct BankCache {
+    const void *key = nullptr;   // the caller's bank pointer
+    int N = 0;
+    void *dev = nullptr;         // [SDR_N_CODES][N] char2 on the device
+    std::vector<uint8_t> host;   // [SDR_N_CODES][N] char2: what dev holds
+    uint32_t valid = 0;          // bit k: bank k is on the device
+    uint64_t used = 0;           // last use (for eviction)
+    BankCache() = default;
+    BankCache(const BankCache &) = delete;
+    BankCache &operator=(const BankCache &) = delete;
+    ~BankCache();
+};
+
 struct ThreadCtx {
     cudaStream_t stream = nullptr;
+    std::vector<BankCache *> banks;   // sdr_corr_std* code banks (bounded, LRU)
+    uint64_t bank_clock = 0;
     Scratch dev[6];      // device scratch slots
     Scratch host[3];     // pinned host staging slots
     // batched correlators (asynchronous): their own slots and the event of
     // the last upload from cb_host
     Scratch stage_err;   // device error word of staged FFT launches
+    Scratch corr_dev;    // synchronous correlators: partials, outputs, ticket
     Scratch cb_dev, cb_host;
     cudaEvent_t cb_ev = nullptr, cb_done = nullptr;
     // batched L6 CSK tracking (asynchronous): the same scheme
@@ -68,6 +88,7 @@ struct ThreadCtx {
     cudaEvent_t l6_ev = nullptr, l6_done = nullptr;
     int error = 0;
     std::string msg;
+    ~ThreadCtx();
 };
 ThreadCtx &tctx();
 int thread_stream(cudaStream_t *s);  // creates the thread's stream lazily
