@@ -84,6 +84,8 @@ def parse():
                     help="weak: one IF block per rank; strong: PRNs dealt over ranks")
     ap.add_argument("--t-sum", type=float, default=20e-3,
                     help="non-coherent time per group (s)")
+    ap.add_argument("--worklist", type=int, choices=(-1, 0, 1), default=-1,
+                    help="consumer launches: 1 one work-list launch, 0 per group, -1 automatic")
     return ap.parse_args()
 
 
@@ -457,6 +459,7 @@ def acq_measure(args, name: str, steps: int, warmup: int, dist, rank: int, world
         wl.groups, shard_index = D.shard_groups(full_groups, rank, world)
     cfs = [workload_code_ffts(wl, g) for g in wl.groups]
     plan = acquire.AcqPlan(wl.groups, cfs)
+    worklist = plan.set_worklist(args.worklist)
     cells = plan.cells
     job_cells = sum(len(g.prns) * len(g.fds) * g.Nmax for g in full_groups) if strong \
         else cells * world
@@ -503,6 +506,25 @@ def acq_measure(args, name: str, steps: int, warmup: int, dist, rank: int, world
     plan.profile(False)
     total_ms = D.max_over_ranks(sum(step_ms), dist)
     value = job_cells * steps / (total_ms / 1e3)
+
+    # the other consumer launch mode on the same plan and buffers, for comparison
+    alt = None
+    if plan.set_worklist(0 if worklist else -1) != worklist:
+        for _ in range(2):
+            step()
+        torch.cuda.synchronize()
+        a_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                for _ in range(steps)]
+        for k in range(steps):
+            flush.fill_(k & 0xFF)
+            a_ev[k][0].record(st)
+            step()
+            a_ev[k][1].record(st)
+        torch.cuda.synchronize()
+        a_ms = D.max_over_ranks(sum(a.elapsed_time(b) for a, b in a_ev), dist)
+        alt = {"launch": "per-group streams" if worklist else "work list",
+               "value": job_cells * steps / (a_ms / 1e3), "ms_per_step": a_ms / steps}
+        plan.set_worklist(args.worklist)
 
     # ---- end to end through the public API: host IF -> device -> results -> host
     bufs_h = [torch.from_numpy(b).pin_memory() for b in wl.bufs]
@@ -568,10 +590,19 @@ def acq_measure(args, name: str, steps: int, warmup: int, dist, rank: int, world
                     "d2h_bytes_per_step": d2h, "launch": "CUDA graph replay (sdrg_acq_run_graph)",
                     "graph_captures": plan.graph_captures()},
             "gpu_launches": sum(n for _, n in prof.values()),
-            "kernel_ms_per_step": {f"{wl.groups[g].sig}.{k}": v[0] / steps
-                                   for (g, k), v in prof_g.items()},
+            "kernel_ms_per_step": {(("all" if worklist and k != "peak" else wl.groups[g].sig)
+                                    + f".{k}"): v[0] / steps
+                                   for (g, k), v in prof_g.items() if v[1] > 0},
+            "consumer_launch": ("work list: one forward launch for every group, one persistent "
+                                "consumer launch (clusters of 8 where they fit, else 2) over every "
+                                "group's (PRN, bin) tasks, a drain launch, each group's peaks"
+                                if worklist else
+                                "per group: forward, consumer and peak launches on concurrent "
+                                "streams"),
             "roofline": roofline, "clocks": clocks,
             "detected": int(sum(1 for r in res if r["cn0"] >= 38.0))}
+    if alt:
+        line["other_launch_mode"] = alt
     if cpu_leg:
         if name == "acq_long_48mhz":
             # 480 000-point searches: a sample of the bins (the whole workload

@@ -311,6 +311,21 @@ int sdrg_acq_run_graph(sdrg_acq_plan_t *plan, const uint8_t *const *if_dev,
 /* Number of graph captures sdrg_acq_run_graph has made for the plan. */
 int sdrg_acq_graph_captures(const sdrg_acq_plan_t *plan);
 
+/* How a run issues its consumer work (the per-PRN loop of
+ * app/pocket_acq/pocket_acq.c:152-192 and search_sig, src/sdr_ch.c:398-450,
+ * done as one work list). mode 1: every group's (PRN, Doppler bin) tasks are
+ * one work list consumed by a single persistent launch (clusters of 8 CTAs
+ * where they fit, of 2 elsewhere; tasks claimed dynamically, the 8-way
+ * splits first), after one forward-transform launch for all groups, all on
+ * the caller's stream; needs every group on the 24 000-point sub-transform
+ * with split 2 or 8 (48 000 / 192 000 points), else SDRG_ERR_ARG. mode 0:
+ * each group's forward / consumer / peak launches on concurrent internal
+ * streams. mode -1 (default): the work list where the plan allows it. Grids
+ * and results are bit-identical either way. Returns 1 when runs use the work
+ * list, 0 when not, or a negative status. A captured graph is re-captured
+ * on the next sdrg_acq_run_graph after a change. */
+int sdrg_acq_set_worklist(sdrg_acq_plan_t *plan, int mode);
+
 /* Device pointer to the accumulated grid of group g, laid out
  * [n_prn][len_fds][Nmax] (float), valid after sdrg_acq_run completes. */
 const float *sdrg_acq_grid(const sdrg_acq_plan_t *plan, int g);

@@ -110,6 +110,7 @@ SIGNATURES = {
     "sdrg_acq_run": ([_p, _p, _p, _p, _p, _p], _i),
     "sdrg_acq_run_graph": ([_p, _p, _p, _p, _p, _p], _i),
     "sdrg_acq_graph_captures": ([_p], _i),
+    "sdrg_acq_set_worklist": ([_p, _i], _i),
     "sdrg_acq_grid": ([_p, _i], _p),
     "sdrg_acq_grid_host": ([_p, _i, _p], _i),
     "sdrg_acq_profile": ([_p, _i], _i),

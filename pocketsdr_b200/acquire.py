@@ -97,6 +97,15 @@ class AcqPlan:
         if st:
             check("sdrg_acq_run_graph" if graph else "sdrg_acq_run")
 
+    def set_worklist(self, mode: int = -1) -> bool:
+        """Consumer issue mode (sdrg_acq_set_worklist): 1 the single
+        persistent work-list launch, 0 per-group launches on concurrent
+        streams, -1 automatic. Returns whether runs use the work list."""
+        r = lib.sdrg_acq_set_worklist(self.handle, int(mode))
+        if r < 0:
+            check("sdrg_acq_set_worklist")
+        return bool(r)
+
     def graph_captures(self) -> int:
         return int(lib.sdrg_acq_graph_captures(self.handle))
 

@@ -99,15 +99,13 @@ struct LoadIQ {
     }
 };
 
+// One forward block: (bin, sum, r) = blk of the group described by a; sm
+// (M points), tw (the plan's twiddles) and ctab (256 carrier values) in
+// shared memory. Ends after its spectrum is stored.
 template <int MODE, int SP>
-__global__ void __launch_bounds__(512, 1) fwd_kernel(FwdArgs a)
+__device__ __forceinline__ void fwd_block(const FwdArgs &a, int blk, float2 *sm, float2 *tw,
+                                          char2 *ctab)
 {
-    extern __shared__ float2 smem[];
-    float2 *sm = smem;
-    float2 *tw = smem + a.pl.M;
-    char2 *ctab = (char2 *)(tw + a.pl.twtot);
-
-    const int blk = blockIdx.x;
     const int r = blk % a.R;
     const int bs = blk / a.R;            // b * n_sum + s
     const int s = bs % a.n_sum, b = bs / a.n_sum;
@@ -139,6 +137,34 @@ __global__ void __launch_bounds__(512, 1) fwd_kernel(FwdArgs a)
     } else {
         for (int i = threadIdx.x; i < M; i += blockDim.x) dst[i] = sm[i];
     }
+}
+
+template <int MODE, int SP>
+__global__ void __launch_bounds__(512, 1) fwd_kernel(FwdArgs a)
+{
+    extern __shared__ float2 smem[];
+    float2 *tw = smem + a.pl.M;
+    fwd_block<MODE, SP>(a, blockIdx.x, smem, tw, (char2 *)(tw + a.pl.twtot));
+}
+
+// Forward blocks of every signal group of a plan in one launch (groups on the
+// compile-time 24 000-point plan): block i belongs to the group g with
+// blk0[g] <= i < blk0[g + 1].
+constexpr int kMaxWorkGroups = 8;
+struct FwdMulti {
+    int n_group;
+    int blk0[kMaxWorkGroups + 1];
+    FwdArgs g[kMaxWorkGroups];
+};
+
+__global__ void __launch_bounds__(512, 1) fwd_multi_kernel(FwdMulti m)
+{
+    extern __shared__ float2 smem[];
+    int g = 0;
+    while (g + 1 < m.n_group && (int)blockIdx.x >= m.blk0[g + 1]) ++g;
+    const FwdArgs &a = m.g[g];
+    float2 *tw = smem + Plan24000::M;
+    fwd_block<0, 1>(a, (int)blockIdx.x - m.blk0[g], smem, tw, (char2 *)(tw + Plan24000::TWTOT));
 }
 
 // ---------------------------------------------------------------------------
@@ -223,45 +249,25 @@ __device__ __forceinline__ void prefetch_l2(const float2 *p, int n)
     }
 }
 
-template <int R, int MODE, int SP>
-__global__ void __launch_bounds__(512, 1) cons_kernel(ConsArgs a)
+// The sums of one consumer task (PRN prn, bin b; this CTA's share c of its
+// R-way split): per sum, combine + code product into the split's shared
+// memory (dst[j]: CTA j of the task), barrier, inverse transform and power
+// (or complex) store. ns_run iterations, each with its two barriers (cluster
+// barriers with CL), so that CTAs whose tasks have fewer sums - or none
+// (active false) - keep step with the cluster; the twiddles are in tw.
+template <int R, int MODE, int SP, bool CL>
+__device__ __forceinline__ void cons_task(const ConsArgs &a, float2 *sm, const float2 *tw,
+                                          float2 *const *dst, int c, int task, int prn, int b,
+                                          int ns_run, bool active)
 {
-    extern __shared__ float2 smem[];
-    float2 *sm = smem;
-    float2 *tw = smem + a.pl.M;
     const int M = SP ? Plan24000::M : a.pl.M;   // SP: compile-time plan
-    const int c = (R > 1) ? (int)(blockIdx.x % R) : 0;
-    // bin-major tasks: the PRNs of one Doppler bin run side by side, so the
-    // bin's forward spectra are fetched from HBM once and then hit in L2
-    const int task = blockIdx.x / R;
-    const int n_prn_l = a.n_prn - a.prn0;
-    const int prn = a.prn0 + task % n_prn_l;
-    const int b = task / n_prn_l;
-    if (b >= a.n_bin) return;     // uniform across the cluster
     const int Mc = (M + R - 1) / R;
     const int q0 = c * Mc, q1 = min(M, q0 + Mc);
     const float2 *code = a.code + (size_t)(a.code_per_bin ? b : prn) * R * M;
-    // this CTA's ranges of the first sum's spectra and of the code head for
-    // L2 while the twiddles load
-    if (threadIdx.x < R && q1 > q0 && a.n_sum > 0) {
-        prefetch_l2(a.X + (size_t)b * a.n_sum * R * M + (size_t)threadIdx.x * M + q0, q1 - q0);
-        prefetch_l2(code + (size_t)threadIdx.x * M + q0, q1 - q0);
-    }
-
-    load_twiddles(tw, a.tw, a.pl.twtot);
-
-    float2 *dst[R];
-    if constexpr (R > 1) {
-        cg::cluster_group cl = cg::this_cluster();
-#pragma unroll
-        for (int j = 0; j < R; ++j) dst[j] = cl.map_shared_rank(sm, j);
-    } else {
-        dst[0] = sm;
-    }
-
-    for (int s = 0; s < a.n_sum; ++s) {
+    for (int s = 0; s < ns_run; ++s) {
         // all CTAs of the cluster are done with their shared memory
-        if constexpr (R > 1) cg::this_cluster().sync(); else __syncthreads();
+        if constexpr (CL) cg::this_cluster().sync(); else __syncthreads();
+        const bool run = active && s < a.n_sum;
         const float2 *Xs = a.X + ((size_t)b * a.n_sum + s) * R * M;
         // U positions per iteration: all their global loads are issued
         // before any arithmetic or (remote) shared-memory store (more loads
@@ -270,7 +276,7 @@ __global__ void __launch_bounds__(512, 1) cons_kernel(ConsArgs a)
         // a second one only fills the load queue (measured 2 % slower).
         constexpr int U = R <= 2 ? 4 : (R <= 6 ? 2 : 1);
         const int qstep = U * blockDim.x;
-        for (int q = q0 + threadIdx.x; q < q1; q += qstep) {
+        for (int q = q0 + threadIdx.x; run && q < q1; q += qstep) {
             float2 xs[U][R], cs[U][R], ts[U];
             bool ok[U];
 #pragma unroll
@@ -320,7 +326,8 @@ __global__ void __launch_bounds__(512, 1) cons_kernel(ConsArgs a)
                 }
             }
         }
-        if constexpr (R > 1) cg::this_cluster().sync(); else __syncthreads();
+        if constexpr (CL) cg::this_cluster().sync(); else __syncthreads();
+        if (!run) continue;
         // the next sum's spectra head for L2 during this sum's transform
         if (s + 1 < a.n_sum && threadIdx.x < R && q1 > q0)
             prefetch_l2(Xs + (size_t)R * M + (size_t)threadIdx.x * M + q0, q1 - q0);
@@ -342,8 +349,160 @@ __global__ void __launch_bounds__(512, 1) cons_kernel(ConsArgs a)
             else fft_inverse(sm, tw, a.pl, st);
         }
     }
+}
+
+template <int R, int MODE, int SP>
+__global__ void __launch_bounds__(512, 1) cons_kernel(ConsArgs a)
+{
+    extern __shared__ float2 smem[];
+    float2 *sm = smem;
+    float2 *tw = smem + a.pl.M;
+    const int M = SP ? Plan24000::M : a.pl.M;   // SP: compile-time plan
+    const int c = (R > 1) ? (int)(blockIdx.x % R) : 0;
+    // bin-major tasks: the PRNs of one Doppler bin run side by side, so the
+    // bin's forward spectra are fetched from HBM once and then hit in L2
+    const int task = blockIdx.x / R;
+    const int n_prn_l = a.n_prn - a.prn0;
+    const int prn = a.prn0 + task % n_prn_l;
+    const int b = task / n_prn_l;
+    if (b >= a.n_bin) return;     // uniform across the cluster
+    const int Mc = (M + R - 1) / R;
+    const int q0 = c * Mc, q1 = min(M, q0 + Mc);
+    const float2 *code = a.code + (size_t)(a.code_per_bin ? b : prn) * R * M;
+    // this CTA's ranges of the first sum's spectra and of the code head for
+    // L2 while the twiddles load
+    if (threadIdx.x < R && q1 > q0 && a.n_sum > 0) {
+        prefetch_l2(a.X + (size_t)b * a.n_sum * R * M + (size_t)threadIdx.x * M + q0, q1 - q0);
+        prefetch_l2(code + (size_t)threadIdx.x * M + q0, q1 - q0);
+    }
+
+    load_twiddles(tw, a.tw, a.pl.twtot);
+
+    float2 *dst[R];
+    if constexpr (R > 1) {
+        cg::cluster_group cl = cg::this_cluster();
+#pragma unroll
+        for (int j = 0; j < R; ++j) dst[j] = cl.map_shared_rank(sm, j);
+    } else {
+        dst[0] = sm;
+    }
+    cons_task<R, MODE, SP, (R > 1)>(a, sm, tw, dst, c, task, prn, b, a.n_sum, true);
     // keep remote shared memory alive until every CTA has finished reading
     if constexpr (R > 1) cg::this_cluster().sync();
+}
+
+// ---------------------------------------------------------------------------
+// work-list consumer: every (PRN, bin) task of every signal group of a plan
+// in one persistent launch. Groups on the compile-time 24 000-point plan with
+// split R = 8 (e.g. 192 000 points) form the wide queue, R = 2 (48 000) the
+// narrow one. The launch asks for clusters of 8 CTAs and accepts clusters of 2
+// where 8 do not fit (a preferred cluster dimension; 8-CTA clusters fit 120
+// of the 148 SMs): an 8-CTA cluster takes wide tasks while there are any,
+// then four narrow tasks at a time; a 2-CTA cluster takes one narrow task at
+// a time. Tasks are claimed with one atomic per unit, in bin-major order
+// within each group (the PRNs of a bin share its spectra in L2).
+// ---------------------------------------------------------------------------
+struct WorkGroup {
+    const float2 *split, *X, *code;
+    float *P, *Q;
+    int R, n_prn, n_bin, n_sum, Nmax, Mq;
+    size_t prn_stride, bin_stride;
+    float scale;
+    int task0;              // first task of the group in its queue
+};
+
+struct WorkArgs {
+    FftPlanK pl;            // the 24 000-point plan
+    const float2 *tw;       // its twiddles
+    int n_group;
+    int n_task[2];          // tasks of the wide (R = 8) and narrow (R = 2) queues
+    int *next;              // [2] next unclaimed task of each queue, 0 at launch
+    WorkGroup g[kMaxWorkGroups];
+};
+
+__device__ __forceinline__ int work_group_of(const WorkArgs &a, int q, int t)
+{
+    for (int g = 0; g < a.n_group; ++g) {
+        const WorkGroup &G = a.g[g];
+        if ((G.R == 8) == (q == 0) && t >= G.task0 && t < G.task0 + G.n_prn * G.n_bin) return g;
+    }
+    return -1;
+}
+
+__device__ __forceinline__ ConsArgs work_cons_args(const WorkArgs &a, const WorkGroup &G)
+{
+    ConsArgs ca = {};
+    ca.pl = a.pl; ca.tw = a.tw; ca.split = G.split; ca.X = G.X; ca.code = G.code;
+    ca.n_prn = G.n_prn; ca.n_bin = G.n_bin; ca.n_sum = G.n_sum; ca.prn0 = 0;
+    ca.scale = G.scale; ca.Nmax = G.Nmax; ca.prn_stride = G.prn_stride;
+    ca.bin_stride = G.bin_stride; ca.accumulate = 0; ca.P = G.P; ca.Q = G.Q; ca.Mq = G.Mq;
+    return ca;
+}
+
+__global__ void __launch_bounds__(512, 1) work_cons_kernel(WorkArgs a)
+{
+    extern __shared__ float2 smem[];
+    float2 *sm = smem;
+    float2 *tw = smem + Plan24000::M;
+    __shared__ int unit[3];           // queue (0 wide, 1 narrow, -1 none), first task, tasks
+    cg::cluster_group cl = cg::this_cluster();
+    const int csize = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+    load_twiddles(tw, a.tw, Plan24000::TWTOT);
+    for (;;) {
+        if (rank == 0 && threadIdx.x == 0) {
+            int q = -1, t = 0, n = 0;
+            if (csize >= 8) {
+                t = atomicAdd(&a.next[0], 1);
+                if (t < a.n_task[0]) { q = 0; n = 1; }
+            }
+            if (q < 0) {
+                const int per = csize / 2;
+                t = atomicAdd(&a.next[1], per);
+                if (t < a.n_task[1]) { q = 1; n = min(per, a.n_task[1] - t); }
+            }
+            unit[0] = q; unit[1] = t; unit[2] = n;
+        }
+        cl.sync();                    // the unit (and, at first, the twiddles) visible
+        const int *lu = cl.map_shared_rank(unit, 0);
+        const int q = lu[0], t0 = lu[1], n = lu[2];
+        if (q < 0) break;             // uniform across the cluster
+        const int R = q == 0 ? 8 : 2;
+        const int slot = rank / R, c = rank % R;
+        const bool active = slot < n;
+        int ns_run = 0;               // the unit's longest task, in sums
+        for (int k = 0; k < n; ++k) {
+            const int gk = work_group_of(a, q, t0 + k);
+            ns_run = max(ns_run, gk >= 0 ? a.g[gk].n_sum : 0);
+        }
+        const int gi = active ? work_group_of(a, q, t0 + slot) : -1;
+        const WorkGroup &G = a.g[gi >= 0 ? gi : 0];
+        const int local = t0 + slot - G.task0;
+        const int prn = local % G.n_prn, b = local / G.n_prn;
+        const ConsArgs ca = work_cons_args(a, G);
+        const bool run = gi >= 0;
+        if (run && threadIdx.x < R && G.n_sum > 0) {
+            const int Mc = (Plan24000::M + R - 1) / R, q0 = c * Mc;
+            const int q1 = min(Plan24000::M, q0 + Mc);
+            prefetch_l2(G.X + (size_t)b * G.n_sum * R * Plan24000::M +
+                        (size_t)threadIdx.x * Plan24000::M + q0, q1 - q0);
+            prefetch_l2(G.code + (size_t)prn * R * Plan24000::M +
+                        (size_t)threadIdx.x * Plan24000::M + q0, q1 - q0);
+        }
+        if (R == 8) {
+            float2 *dst[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) dst[j] = cl.map_shared_rank(sm, j);
+            cons_task<8, 0, 1, true>(ca, sm, tw, dst, c, local, prn, b, ns_run, run);
+        } else {
+            float2 *dst[2];
+#pragma unroll
+            for (int j = 0; j < 2; ++j) dst[j] = cl.map_shared_rank(sm, 2 * slot + j);
+            cons_task<2, 0, 1, true>(ca, sm, tw, dst, c, local, prn, b, ns_run, run);
+        }
+    }
+    // the leader's unit word and every CTA's shared memory stay alive until
+    // the whole cluster is done
+    cl.sync();
 }
 
 // ---------------------------------------------------------------------------
@@ -1056,6 +1215,11 @@ struct sdrg_acq_plan {
     cudaGraphExec_t graph_exec = nullptr;
     std::vector<intptr_t> graph_key;
     int graph_captures = 0;
+    // work-list consumer (sdrg_acq_set_worklist): eligible when every group
+    // is on the 24 000-point compile-time plan with split 2 or 8
+    bool wl_ok = false;
+    int wl_mode = -1;           // -1 automatic, 0 per-group launches, 1 work list
+    int *wl_next = nullptr;     // [2] device queue heads
 };
 
 static void drop_graph(sdrg_acq_plan_t *plan)
@@ -1409,6 +1573,17 @@ sdrg_acq_plan_t *sdrg_acq_plan_new(const sdrg_acq_sig_t *sigs, int n_sig)
         plan->cells += (int64_t)s.n_prn * s.len_fds * s.Nmax;
     }
     plan->n_res = res_off;
+    // the work-list consumer: all groups on the 24 000-point compile-time
+    // plan, splits 2 (narrow queue) or 8 (wide queue), at most kMaxWorkGroups
+    bool wl = n_sig <= kMaxWorkGroups;
+    for (auto &G : plan->g)
+        wl = wl && (G.pl->R == 2 || G.pl->R == 8) && Plan24000::matches(G.pl->k, G.pl->threads);
+    if (wl && cudaMalloc(&plan->wl_next, 2 * sizeof(int)) != cudaSuccess) {
+        cuda_error(cudaGetLastError(), "sdrg_acq_plan_new work list");
+        sdrg_acq_plan_free(plan);
+        return nullptr;
+    }
+    plan->wl_ok = wl;
     return plan;
 }
 
@@ -1427,6 +1602,7 @@ void sdrg_acq_plan_free(sdrg_acq_plan_t *plan)
     }
     for (auto ev : plan->ev_join) if (ev) cudaEventDestroy(ev);
     if (plan->stage_err) cudaFree(plan->stage_err);
+    if (plan->wl_next) cudaFree(plan->wl_next);
     if (plan->ev_fork) cudaEventDestroy(plan->ev_fork);
     for (auto ev : plan->ev_pool) cudaEventDestroy(ev);
     for (auto &u : plan->ev_used) {
@@ -1614,6 +1790,113 @@ static int check_run(const sdrg_acq_plan_t *plan, const int *len_if)
 // With `ix` the tables are uploaded on the group streams as needed; without
 // (graph capture) the caller has uploaded them and no profiling events are
 // recorded.
+static bool use_worklist(const sdrg_acq_plan_t *plan)
+{
+    return plan->wl_ok && plan->wl_mode != 0;
+}
+
+// The forward arguments of group G on IF buffer if_dev[G.sig.buf].
+static FwdArgs group_fwd_args(const GroupState &G, const Device *dev,
+                              const uint8_t *const *if_dev, const int *len_if)
+{
+    const sdrg_acq_sig_t &s = G.sig;
+    const int nb = s.len_fds, ns = s.n_sum;
+    FwdArgs fa = {};
+    fa.pl = G.pl->k; fa.tw = G.pl->tw_dev; fa.ctab = dev->ctab_dev; fa.R = G.pl->R;
+    fa.n_bin = nb; fa.n_sum = ns; fa.cscale = kCScale;
+    fa.buf = if_dev[s.buf]; fa.buf_len = len_if[s.buf];
+    fa.phstep = G.tab_dev; fa.ph0a = G.tab_dev + nb; fa.ph0b = G.tab_dev + 2 * nb;
+    fa.ix = (const int *)(G.tab_dev + 2 * nb + (size_t)nb * ns);
+    fa.nsplit = fa.ix + ns;
+    fa.X = G.X;
+    return fa;
+}
+
+// The run as a work list, on the caller's stream: one forward launch for
+// every group, the persistent consumer over every group's tasks (plus a
+// drain launch of regular 8-CTA clusters, which finds the queues empty
+// unless no 8-CTA cluster formed in the first), then each group's peaks.
+// Kernel timing (profiling) goes to group 0's forward and consumer entries.
+static int launch_run_worklist(sdrg_acq_plan_t *plan, Device *dev, const uint8_t *const *if_dev,
+                               const int *len_if, const int *ix, sdrg_acq_result_t *res_dev,
+                               cudaStream_t caller)
+{
+    int e;
+    const int ng = (int)plan->g.size();
+    const FftPlan *pl0 = plan->g[0].pl;
+    static bool attr_set = false;
+    if (!attr_set) {
+        SDRG_CUDA(cudaFuncSetAttribute(fwd_multi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)g_smem_limit()));
+        cudaFuncAttributes fa;
+        SDRG_CUDA(cudaFuncGetAttributes(&fa, work_cons_kernel));
+        SDRG_CUDA(cudaFuncSetAttribute(work_cons_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(g_smem_limit() - fa.sharedSizeBytes)));
+        attr_set = true;
+    }
+    FwdMulti fm = {};
+    fm.n_group = ng;
+    WorkArgs wa = {};
+    wa.pl = pl0->k; wa.tw = pl0->tw_dev; wa.n_group = ng; wa.next = plan->wl_next;
+    for (int gi = 0; gi < ng; ++gi) {
+        GroupState &G = plan->g[gi];
+        const sdrg_acq_sig_t &s = G.sig;
+        if (ix && (e = upload_tables(G, len_if, ix, caller))) return e;
+        fm.g[gi] = group_fwd_args(G, dev, if_dev, len_if);
+        fm.blk0[gi + 1] = fm.blk0[gi] + s.len_fds * s.n_sum * G.pl->R;
+        WorkGroup &W = wa.g[gi];
+        W.split = G.pl->split_dev; W.X = G.X; W.code = G.code; W.P = G.P; W.Q = G.Q;
+        W.R = G.pl->R; W.n_prn = s.n_prn; W.n_bin = s.len_fds; W.n_sum = s.n_sum;
+        W.Nmax = s.Nmax; W.Mq = G.Mq; W.prn_stride = (size_t)s.len_fds * s.Nmax;
+        W.bin_stride = s.Nmax; W.scale = 1.0f / s.L / s.L;
+        const int q = W.R == 8 ? 0 : 1;
+        W.task0 = wa.n_task[q];
+        wa.n_task[q] += s.n_prn * s.len_fds;
+    }
+    cudaEvent_t ev[2];
+    if ((e = prof_begin(plan, caller, ev))) return e;
+    fwd_multi_kernel<<<fm.blk0[ng], pl0->threads, pl0->smem, caller>>>(fm);
+    SDRG_CUDA(cudaGetLastError());
+    if ((e = prof_end(plan, caller, ev, 0))) return e;
+
+    if ((e = prof_begin(plan, caller, ev))) return e;
+    SDRG_CUDA(cudaMemsetAsync(plan->wl_next, 0, 2 * sizeof(int), caller));
+    cudaLaunchConfig_t cfg = {};
+    cfg.blockDim = dim3(pl0->threads);
+    cfg.dynamicSmemBytes = pl0->smem;
+    cfg.stream = caller;
+    cudaLaunchAttribute attr[2];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2; attr[0].val.clusterDim.y = 1; attr[0].val.clusterDim.z = 1;
+    attr[1].id = cudaLaunchAttributePreferredClusterDimension;
+    attr[1].val.preferredClusterDim.x = 8; attr[1].val.preferredClusterDim.y = 1;
+    attr[1].val.preferredClusterDim.z = 1;
+    cfg.attrs = attr;
+    // one CTA per SM (shared memory), a whole number of 8-CTA clusters
+    cfg.gridDim = dim3((unsigned)((dev->sm_count + 7) / 8 * 8));
+    cfg.numAttrs = 2;
+    SDRG_CUDA(cudaLaunchKernelEx(&cfg, work_cons_kernel, wa));
+    // drain: regular 8-CTA clusters take whatever is left (normally nothing)
+    attr[0].val.clusterDim.x = 8;
+    cfg.gridDim = dim3((unsigned)(dev->sm_count / 8 * 8 > 0 ? dev->sm_count / 8 * 8 : 8));
+    cfg.numAttrs = 1;
+    SDRG_CUDA(cudaLaunchKernelEx(&cfg, work_cons_kernel, wa));
+    if ((e = prof_end(plan, caller, ev, 1, 2))) return e;
+
+    for (int gi = 0; gi < ng; ++gi) {
+        GroupState &G = plan->g[gi];
+        const sdrg_acq_sig_t &s = G.sig;
+        const int nb = s.len_fds;
+        const float *fd_dev = (const float *)(G.tab_dev + G.tab_words - nb);
+        if ((e = prof_begin(plan, caller, ev))) return e;
+        if ((e = launch_peaks(G.P, s.n_prn, nb, s.Nmax, s.Nmax, (size_t)nb * s.Nmax, s.T,
+                              fd_dev, res_dev + G.res_off, G.peak_parts, caller)))
+            return e;
+        if ((e = prof_end(plan, caller, ev, 3 * gi + 2, 2))) return e;
+    }
+    return SDRG_OK;
+}
+
 static int launch_run(sdrg_acq_plan_t *plan, Device *dev, const uint8_t *const *if_dev,
                       const int *len_if, const int *ix, sdrg_acq_result_t *res_dev,
                       cudaStream_t caller)
@@ -1629,6 +1912,7 @@ static int launch_run(sdrg_acq_plan_t *plan, Device *dev, const uint8_t *const *
     const bool saved = plan->prof;
     plan->prof = prof;
     struct Restore { sdrg_acq_plan_t *p; bool v; ~Restore() { p->prof = v; } } restore{plan, saved};
+    if (use_worklist(plan)) return launch_run_worklist(plan, dev, if_dev, len_if, ix, res_dev, caller);
     // fork: every internal stream starts after the caller's prior work
     SDRG_CUDA(cudaEventRecord(plan->ev_fork, caller));
     for (cudaStream_t s2 : plan->streams) SDRG_CUDA(cudaStreamWaitEvent(s2, plan->ev_fork, 0));
@@ -1757,6 +2041,18 @@ int sdrg_acq_run_graph(sdrg_acq_plan_t *plan, const uint8_t *const *if_dev, cons
     SDRG_CUDA(cudaGraphLaunch(plan->graph_exec, caller));
     plan->run++;
     return SDRG_OK;
+}
+
+int sdrg_acq_set_worklist(sdrg_acq_plan_t *plan, int mode)
+{
+    if (!plan || mode < -1 || mode > 1)
+        return set_error(SDRG_ERR_ARG, "sdrg_acq_set_worklist: bad argument");
+    if (mode == 1 && !plan->wl_ok)
+        return set_error(SDRG_ERR_ARG, "sdrg_acq_set_worklist: the plan's groups are not all on "
+                         "the 24 000-point plan with split 2 or 8");
+    if (mode != plan->wl_mode) drop_graph(plan);
+    plan->wl_mode = mode;
+    return use_worklist(plan) ? 1 : 0;
 }
 
 int sdrg_acq_graph_captures(const sdrg_acq_plan_t *plan)
