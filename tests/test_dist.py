@@ -68,3 +68,68 @@ def test_two_gloo_ranks():
         assert out[r][3][1] == [1, 2, 3]
         assert out[r][4][0] == [i % 2 for i in range(32)]   # dealt round-robin
     assert out[0][2][0] == list(range(1, 33, 2)) and out[1][2][0] == list(range(2, 33, 2))
+
+
+def _search_worker(rank, world, port, q):
+    """One rank of the strong mode with real search results: the reference
+    search (the oracle's sdr_search_code + sdr_corr_max + sdr_fine_dop) over
+    this rank's PRN shard, gathered as per-PRN result records."""
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank),
+                      MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    try:
+        from oracle import oracle
+        from pocketsdr_b200 import dist as D
+        from pocketsdr_b200 import synth
+        dist = D.init(backend="gloo", timeout_s=60)
+        wl = _small_workload(synth)
+        mine, index = D.shard_groups(wl.groups, rank, world)
+        cfs = [synth.group_code_ffts(g) for g in mine]
+        ref = oracle.search_groups(mine, wl.bufs, cfs, max_threads=2)
+        full = D.gather_results(_records(ref["res"]), index, wl.groups, world, dist)
+        dist.barrier()
+        dist.destroy_process_group()
+        q.put((rank, np.concatenate(full).tobytes()))
+    except Exception as e:  # surfaced in the parent
+        q.put((rank, "error: " + repr(e)))
+
+
+def _small_workload(synth):
+    wl = synth.acq_multi_24mhz(seed=12, prn_limit=5, t_sum=2e-3)
+    for g in wl.groups:
+        g.fds = g.fds[::10].copy()
+    return wl
+
+
+def _records(r):
+    dt = np.dtype([("bin", np.int32), ("offset", np.int32), ("cn0", np.float32),
+                   ("pmax", np.float32), ("pave", np.float64), ("fd", np.float64)])
+    out = np.zeros(len(r), dt)
+    for f in ("bin", "offset", "cn0", "fd"):
+        out[f] = r[f]
+    out["pmax"] = r["pmax"]
+    out["pave"] = r["pmean"]
+    return out
+
+
+def test_two_gloo_ranks_gather_real_search_results():
+    """PRNs dealt over two ranks, each searching its share with the reference
+    path on CPU; the gathered per-PRN results equal one process searching
+    every PRN."""
+    import torch.multiprocessing as mp
+    from oracle import oracle
+    from pocketsdr_b200 import synth
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_search_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = dict(q.get(timeout=300) for _ in range(2))
+    for p in procs:
+        p.join(timeout=60)
+    for r in (0, 1):
+        assert not isinstance(out[r], str), out[r]
+    wl = _small_workload(synth)
+    single = oracle.search_groups(wl.groups, wl.bufs, [synth.group_code_ffts(g) for g in wl.groups])
+    want = _records(single["res"]).tobytes()
+    assert out[0] == want and out[1] == want
