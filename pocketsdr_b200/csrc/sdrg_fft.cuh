@@ -161,8 +161,15 @@ struct DftCT {
 #pragma unroll
             for (int k1 = 0; k1 < A; ++k1) {
                 const int e = (n2 * k1) % N;
+                // quarter turns are exact rotations (no multiplication)
                 if (e == 0) {
                     y[n2 * A + k1] = t[k1];
+                } else if (4 * e == N) {
+                    y[n2 * A + k1] = cmul_i<DIR>(t[k1]);
+                } else if (2 * e == N) {
+                    y[n2 * A + k1] = make_float2(-t[k1].x, -t[k1].y);
+                } else if (4 * e == 3 * N) {
+                    y[n2 * A + k1] = cmul_i<-DIR>(t[k1]);
                 } else {
                     y[n2 * A + k1] = cmul(t[k1], make_float2(tw.c[e], tw.s[e]));
                 }
@@ -517,6 +524,45 @@ __device__ __forceinline__ void s_bfly(float2 *p, const float2 *twp, int i)
     for (int j = 0; j < R; ++j) p[j * S] = v[j];
 }
 
+#ifndef SDRG_WARP_PAIR
+#define SDRG_WARP_PAIR 0
+#endif
+// two butterflies of a warp-private pass at once (p0 always, p1 when ok1):
+// both loads before either butterfly's arithmetic, both stores after
+template <int R, int S, bool FWD>
+__device__ __forceinline__ void s_bfly2(float2 *p0, int i0, float2 *p1, int i1, bool ok1,
+                                        const float2 *twp)
+{
+    float2 v0[R], v1[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) v0[j] = p0[j * S];
+    if (ok1) {
+#pragma unroll
+        for (int j = 0; j < R; ++j) v1[j] = p1[j * S];
+    }
+    if (FWD) {
+        Dft<R, -1>::run(v0);
+        if (S > 1) apply_tw<R>(v0, twp[i0]);
+        if (ok1) {
+            Dft<R, -1>::run(v1);
+            if (S > 1) apply_tw<R>(v1, twp[i1]);
+        }
+    } else {
+        if (S > 1) apply_tw<R>(v0, cconj(twp[i0]));
+        Dft<R, 1>::run(v0);
+        if (ok1) {
+            if (S > 1) apply_tw<R>(v1, cconj(twp[i1]));
+            Dft<R, 1>::run(v1);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < R; ++j) p0[j * S] = v0[j];
+    if (ok1) {
+#pragma unroll
+        for (int j = 0; j < R; ++j) p1[j * S] = v1[j];
+    }
+}
+
 template <int R, int S, int REG, bool FWD = false>
 __device__ __forceinline__ void s_inner_warp(float2 *sm, const float2 *twp)
 {
@@ -532,18 +578,40 @@ __device__ __forceinline__ void s_inner_warp(float2 *sm, const float2 *twp)
         // to 16 keep at least half of the lanes busy.
         constexpr int NBLK = REG / LS, IH = (NBLK + 1) / 2;
         const int i = lane & 15;
+        if constexpr (SDRG_WARP_PAIR && R <= 10) {
 #pragma unroll
-        for (int it = 0; it < IH; ++it) {
-            const int blk = 2 * it + (lane >> 4);
-            if (blk < NBLK && i < S) s_bfly<R, S, FWD>(base + blk * LS + i, twp, i);
+            for (int it = 0; it < IH; it += 2) {
+                const int b0 = 2 * it + (lane >> 4), b1 = b0 + 2;
+                if (b0 < NBLK && i < S)
+                    s_bfly2<R, S, FWD>(base + b0 * LS + i, i, base + b1 * LS + i, i,
+                                       it + 1 < IH && b1 < NBLK, twp);
+            }
+        } else {
+#pragma unroll
+            for (int it = 0; it < IH; ++it) {
+                const int blk = 2 * it + (lane >> 4);
+                if (blk < NBLK && i < S) s_bfly<R, S, FWD>(base + blk * LS + i, twp, i);
+            }
         }
     } else {
+        if constexpr (SDRG_WARP_PAIR && R <= 10) {
 #pragma unroll
-        for (int it = 0; it < IT; ++it) {
-            const int b = lane + it * 32;
-            if (b < NB) {
-                const int blk = b / S, i = b - blk * S;
-                s_bfly<R, S, FWD>(base + blk * LS + i, twp, i);
+            for (int it = 0; it < IT; it += 2) {
+                const int b0 = lane + it * 32, b1 = b0 + 32;
+                if (b0 < NB) {
+                    const int k0 = b0 / S, i0 = b0 - k0 * S, k1 = b1 / S, i1 = b1 - k1 * S;
+                    s_bfly2<R, S, FWD>(base + k0 * LS + i0, i0, base + k1 * LS + i1, i1,
+                                       it + 1 < IT && b1 < NB, twp);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int it = 0; it < IT; ++it) {
+                const int b = lane + it * 32;
+                if (b < NB) {
+                    const int blk = b / S, i = b - blk * S;
+                    s_bfly<R, S, FWD>(base + blk * LS + i, twp, i);
+                }
             }
         }
     }
