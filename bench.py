@@ -3,7 +3,8 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload acq_multi_24mhz|acq_l1ca_12mhz|acq_long_48mhz|track_24mhz|
-                                refine_12mhz]
+                                refine_12mhz|mix_24mhz|ingest_raw32_24mhz|
+                                search_batch_24mhz|l6_csk_24mhz] [--worklist -1|0|1]
 
 Besides the default acquisition workload: acq_l1ca_12mhz is the plain 12 MHz
 GPS L1 C/A search (32 PRNs x 41 bins x 5 x 4 ms), acq_long_48mhz the weak-signal
@@ -11,7 +12,8 @@ long coherent search (48 MHz, GPS L5-Q and QZSS L6D, 10 ms coherent =
 480 000-point FFTs x 20 sums, 401 bins of 50 Hz), track_24mhz times the batched
 tracking correlators (channel-epochs/s) and refine_12mhz the grid search plus
 Gauss-Newton refinement of 64 signals (signals/s, with the refinement's cost
-against the grid and its agreement with the FP64 oracle).
+against the grid and its agreement with the FP64 oracle), mix_24mhz the
+carrier wipe-off of a device-resident IF buffer (samples/s, HBM bound).
 
 A step is one full search of the workload: every PRN of every signal group x
 every Doppler bin x every code offset, accumulated over all non-coherent sums,
@@ -364,6 +366,12 @@ def _reference_other(args):
             rate, cores, kind, desc = cpu_l6_rate(fs, fi, N, Lc, sats, buf, pos, cfs, 20)
             metric, unit, cfg = L6_METRIC, "channel-epochs/s", {"workload": w, "channels": 10}
             per_step = 250 * len(sats)                                             # 1 s
+        elif w == "mix_24mhz":
+            buf = np.random.default_rng(8).integers(0, 256, MIX_N, dtype=np.uint8)
+            rate, cores, kind, desc = cpu_mix_rate(buf, 24e6, 2.0e6 + 1234.5, 0.3, 64_000_000)
+            metric, unit, cfg = MIX_METRIC, "samples/s", {"workload": w,
+                                                          "samples_per_step": MIX_N}
+            per_step = MIX_N
         elif w == "search_batch_24mhz":
             wl = make_workload("acq_multi_24mhz", 2)
             ref = cpu_reference_full(wl)
@@ -1144,6 +1152,116 @@ def run_refine(args):
     return 0
 
 
+MIX_METRIC = ("carrier wipe-off samples/s (sdr_mix_carr on a device-resident 24 MHz complex "
+              "IF buffer: 4 s = 96 M packed samples per step)")
+MIX_N = 96_000_000
+
+
+def cpu_mix_rate(buf, fs, fc, phi, n_samples):
+    """Reference CPU rate (samples/s): the reference's own sdr_mix_carr over
+    consecutive windows of the buffer, one window per host thread at a time,
+    n_samples in all."""
+    import concurrent.futures as cf
+    from oracle import oracle
+    R = oracle.best()
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    W = 1_000_000
+    n_win = max(cores, n_samples // W)
+
+    def one(k):
+        ix = (k * W) % (len(buf) - W)
+        return R.mix_carr(buf, ix, W, fs, fc, phi + 0.01 * k).shape[0]
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=cores) as ex:
+        done = sum(ex.map(one, range(n_win)))
+    wall = time.perf_counter() - t0
+    return done / wall, cores, R.kind, (f"{n_win} windows of {W} samples over {cores} threads "
+                                        f"({wall:.1f}s)")
+
+
+def run_mix(args):
+    """Carrier wipe-off (the mixing stage of every search and tracking
+    epoch): one step mixes a 4 s window (96 M samples) of a 24 MHz complex
+    3-bit IF buffer resident on the device (sdrg_mix_carr; bit-identical to
+    sdr_mix_carr). HBM bound: 1 byte read, 2 bytes written per sample."""
+    import ctypes as C
+    import torch
+    from pocketsdr_b200._lib import lib
+    rank, world, local = dist_info()
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(8 + rank)
+    buf = rng.integers(0, 256, MIX_N, dtype=np.uint8)
+    fs, fc, phi = 24e6, 2.0e6 + 1234.5, 0.3
+    st = torch.cuda.Stream()
+    torch.cuda.set_stream(st)
+    d_buf = torch.from_numpy(buf).cuda()
+    d_out = torch.empty(2 * MIX_N, dtype=torch.int8, device="cuda")
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+
+    def step():
+        if lib.sdrg_mix_carr(C.c_void_p(d_buf.data_ptr()), MIX_N, 0, MIX_N, fs, fc, phi,
+                             C.c_void_p(d_out.data_ptr()), C.c_void_p(st.cuda_stream)):
+            raise RuntimeError("sdrg_mix_carr failed")
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    clk = ClockSampler(local)
+    clk.start()
+    for k in range(args.steps):
+        flush.fill_(k & 0xFF)
+        ev[k][0].record(st)
+        step()
+        ev[k][1].record(st)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    from pocketsdr_b200 import dist as D
+    ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
+    value = MIX_N / (ms / 1e3) * world
+    # end to end: IF from pinned host memory, mixed samples back to the host
+    buf_h = torch.from_numpy(buf).pin_memory()
+    out_h = torch.empty(2 * MIX_N, dtype=torch.int8).pin_memory()
+    e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]
+    for k in range(args.steps):
+        e2e_ev[k][0].record(st)
+        d_buf.copy_(buf_h, non_blocking=True)
+        step()
+        out_h.copy_(d_out, non_blocking=True)
+        e2e_ev[k][1].record(st)
+    torch.cuda.synchronize()
+    e2e_ms = sum(a.elapsed_time(b) for a, b in e2e_ev) / args.steps
+    bytes_step = 3 * MIX_N
+    achieved = bytes_step / (ms / 1e3) / 1e9
+    peak = _measured_hbm()
+    line = {"metric": MIX_METRIC, "value": value, "unit": "samples/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/i8",
+            "data": "synthetic", "config": {"workload": "mix_24mhz", "samples_per_step": MIX_N,
+                                            "l2": "flushed between timed steps (512 MB write "
+                                                  "outside the events); the 288 MB of traffic "
+                                                  "per step exceeds L2 anyway"},
+            "e2e": {"value": MIX_N / (e2e_ms / 1e3) * world, "unit": "samples/s",
+                    "h2d_bytes_per_step": MIX_N, "d2h_bytes_per_step": 2 * MIX_N},
+            "gpu_launches": args.steps,
+            "roofline": {"kernel": "mix_kernel (carrier wipe-off, 16 samples per thread)",
+                         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak,
+                         "peak_source": ("MEASURED_PEAKS.json" if os.path.exists(
+                             os.path.join(ROOT, "MEASURED_PEAKS.json")) else "fallback 6650 GB/s"),
+                         "algorithmic_bytes_per_step": bytes_step, "traffic": None},
+            "clocks": clocks}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, cores, kind, desc = cpu_mix_rate(buf, fs, fc, phi, 64_000_000)
+        line["cpu_baseline"] = {"value": rate, "unit": "samples/s", "cores": cores, "kind": kind,
+                                "sample": desc}
+    if rank == 0:
+        emit(line)
+    return 0
+
+
 INGEST_METRIC = ("IF ingest samples/s (Pocket SDR FE 8CH RAW32 at 24 MHz -> 8 RF + 2 array "
                  "cpx8 buffers, fs/4 mixing, LPF, beam-forming)")
 
@@ -1495,6 +1613,8 @@ def main():
         return run_l6(args)
     if args.workload == "ingest_raw32_24mhz":
         return run_ingest(args)
+    if args.workload == "mix_24mhz":
+        return run_mix(args)
     if args.workload == "track_24mhz":
         return run_track(args)
     if args.workload == "refine_12mhz":

@@ -371,6 +371,16 @@ typedef struct {
 int sdrg_corr_batch(const sdrg_corr_job_t *jobs, int n_job, const uint8_t *const *if_dev,
     const int *len_if, sdr_cpx_t *corr_dev, sdr_cpx_t *C_dev, void *stream);
 
+/* ---- carrier wipe-off on the device -----------------------------------------
+ * sdr_mix_carr (src/sdr_func.c:824-836) on a device-resident circular IF
+ * buffer: IQ_dev[n] = the window sample (ix + n) mod len of buf_dev (len
+ * packed sdr_cpx8_t samples) mixed with the carrier of frequency fc and phase
+ * phi (cycles) at sample ix, the phase restarting at the buffer wrap as in the
+ * reference. Bit-identical to sdr_mix_carr. DEVICE pointers; asynchronous on
+ * `stream` (NULL = the legacy default stream). */
+int sdrg_mix_carr(const uint8_t *buf_dev, int len, int ix, int N, double fs,
+    double fc, double phi, sdr_cpx16_t *IQ_dev, void *stream);
+
 /* ---- spreading-code chips (host) -------------------------------------------
  * The reference's sdr_gen_code / sdr_sec_code (src/sdr_code.c:2173-2182,
  * :2274-2283; src/pocket_sdr.h:454-455) for the signals of the search and

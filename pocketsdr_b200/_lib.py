@@ -117,6 +117,7 @@ SIGNATURES = {
     "sdrg_acq_profile_get": ([_p, _p, _p], _i),
     "sdrg_acq_run_host": ([_p, _p, _p, _p, _p], _i),
     "sdrg_corr_batch": ([_p, _i, _p, _p, _p, _p, _p], _i),
+    "sdrg_mix_carr": ([_p, _i, _i, _i, _d, _d, _d, _p, _p], _i),
     "sdrg_gen_code": ([C.c_char_p, _i, _p, _i], _i),
     "sdrg_sec_code": ([C.c_char_p, _i, _p, _i], _i),
     "sdrg_res_code": ([_p, _p, _i, _i, _d, _d, _d, _i, _i, _i, _p, _p], _i),

@@ -26,37 +26,53 @@ __device__ __forceinline__ char2 mix_byte(uint8_t byte, uint32_t phase, const ch
     return o;
 }
 
-// 4 samples per thread; win is a linear copy of the window (N samples).
-__global__ void mix_kernel(const uint8_t *__restrict__ win, int N, int nsplit,
-                           uint32_t p0a, uint32_t p0b, uint32_t step,
-                           const char2 *__restrict__ ctab_g, char2 *__restrict__ out)
+// Window sample n is buf[(ix + n) mod len], its carrier phase
+// n < nsplit ? p0a + n step : p0b + (n - nsplit) step (the restart at the
+// buffer wrap). 16 samples per thread: where its 16 samples lie contiguous and
+// 16-byte aligned in the buffer and the output is 16-byte aligned, one
+// 16-byte load and two 16-byte stores; otherwise sample by sample. HBM bound:
+// 1 byte read and 2 bytes written per sample.
+constexpr int kMixPer = 16;
+
+__global__ void __launch_bounds__(256) mix_kernel(
+    const uint8_t *__restrict__ buf, int len, int ix, int N, int nsplit, uint32_t p0a,
+    uint32_t p0b, uint32_t step, const char2 *__restrict__ ctab_g, char2 *__restrict__ out)
 {
     __shared__ char2 ctab[256];
     for (int i = threadIdx.x; i < 256; i += blockDim.x) ctab[i] = ctab_g[i];
     __syncthreads();
-    const int n0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
-    if (n0 >= N) return;
-    if (n0 + 4 <= N) {
-        const uchar4 b = *(const uchar4 *)(win + n0);
-        const uint8_t bb[4] = {b.x, b.y, b.z, b.w};
-        char2 o[4];
+    const long long n0l = (long long)kMixPer * (blockIdx.x * (long long)blockDim.x + threadIdx.x);
+    if (n0l >= N) return;
+    const int n0 = (int)n0l;
+    int pos0 = ix + n0;
+    if (pos0 >= len) pos0 -= len;
+    const bool fast = n0 + kMixPer <= N && pos0 + kMixPer <= len &&
+                      (n0 + kMixPer <= nsplit || n0 >= nsplit) &&
+                      ((((uintptr_t)(buf + pos0)) | ((uintptr_t)(out + n0))) & 15u) == 0;
+    if (fast) {
+        const uint4 w = *(const uint4 *)(buf + pos0);
+        const uint32_t wd[4] = {w.x, w.y, w.z, w.w};
+        uint32_t ph = n0 < nsplit ? p0a + step * (uint32_t)n0 : p0b + step * (uint32_t)(n0 - nsplit);
+        uint32_t o[8];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int n = n0 + j;
-            const uint32_t ph = n < nsplit ? p0a + step * (uint32_t)n
-                                           : p0b + step * (uint32_t)(n - nsplit);
-            o[j] = mix_byte(bb[j], ph, ctab);
+        for (int k = 0; k < 8; ++k) {
+            const char2 a = mix_byte((uint8_t)(wd[k >> 1] >> (16 * (k & 1))), ph, ctab);
+            ph += step;
+            const char2 b = mix_byte((uint8_t)(wd[k >> 1] >> (16 * (k & 1) + 8)), ph, ctab);
+            ph += step;
+            o[k] = (uint32_t)(uint8_t)a.x | ((uint32_t)(uint8_t)a.y << 8) |
+                   ((uint32_t)(uint8_t)b.x << 16) | ((uint32_t)(uint8_t)b.y << 24);
         }
-        *(int2 *)(out + n0) = make_int2(
-            (int)((uint32_t)(uint8_t)o[0].x | ((uint32_t)(uint8_t)o[0].y << 8) |
-                  ((uint32_t)(uint8_t)o[1].x << 16) | ((uint32_t)(uint8_t)o[1].y << 24)),
-            (int)((uint32_t)(uint8_t)o[2].x | ((uint32_t)(uint8_t)o[2].y << 8) |
-                  ((uint32_t)(uint8_t)o[3].x << 16) | ((uint32_t)(uint8_t)o[3].y << 24)));
+        uint4 *d = (uint4 *)(out + n0);
+        d[0] = make_uint4(o[0], o[1], o[2], o[3]);
+        d[1] = make_uint4(o[4], o[5], o[6], o[7]);
     } else {
-        for (int n = n0; n < N; ++n) {
+        for (int n = n0; n < N && n < n0 + kMixPer; ++n) {
+            int pos = ix + n;
+            if (pos >= len) pos -= len;
             const uint32_t ph = n < nsplit ? p0a + step * (uint32_t)n
                                            : p0b + step * (uint32_t)(n - nsplit);
-            out[n] = mix_byte(win[n], ph, ctab);
+            out[n] = mix_byte(buf[pos], ph, ctab);
         }
     }
 }
@@ -82,12 +98,15 @@ static inline uint32_t step_of(double step)
     return (uint32_t)(int)(step * 4294967296.0);
 }
 
-int launch_mix(const uint8_t *win_dev, int N, int nsplit, uint32_t p0a, uint32_t p0b,
-               uint32_t step, const char2 *ctab_dev, char2 *out_dev, cudaStream_t st)
+int launch_mix(const uint8_t *buf_dev, int len, int ix, int N, int nsplit, uint32_t p0a,
+               uint32_t p0b, uint32_t step, const char2 *ctab_dev, char2 *out_dev,
+               cudaStream_t st)
 {
     const int threads = 256;
-    const int blocks = (N / 4 + threads) / threads + 1;
-    mix_kernel<<<blocks, threads, 0, st>>>(win_dev, N, nsplit, p0a, p0b, step, ctab_dev, out_dev);
+    const long long units = ((long long)N + kMixPer - 1) / kMixPer;
+    const unsigned blocks = (unsigned)((units + threads - 1) / threads);
+    mix_kernel<<<blocks, threads, 0, st>>>(buf_dev, len, ix, N, nsplit, p0a, p0b, step, ctab_dev,
+                                           out_dev);
     SDRG_CUDA(cudaGetLastError());
     return SDRG_OK;
 }
@@ -121,7 +140,7 @@ int mix_cpx_device(const sdr_cpx_t *buff, int len_buff, int ix, int N, double fs
     SDRG_CUDA(cudaMemcpyAsync(fin, h, (size_t)N * 8, cudaMemcpyHostToDevice, st));
     pack_cpx_kernel<<<(N + 255) / 256, 256, 0, st>>>(fin, N, packed);
     SDRG_CUDA(cudaGetLastError());
-    if ((e = launch_mix(packed, N, N, phase_of(phi), 0, step_of(fc / fs), dev->ctab_dev,
+    if ((e = launch_mix(packed, N, 0, N, N, phase_of(phi), 0, step_of(fc / fs), dev->ctab_dev,
                         iq_dev, st)))
         return e;
     // the staging buffer is reused by the next call: finish the copy first
@@ -167,7 +186,7 @@ void sdr_mix_carr(const sdr_buff_t *buff, int ix, int N, double fs, double fc, d
     char2 *out_d = (char2 *)(win_d + off);
     char2 *out_h = (char2 *)(h + off);
     if (cudaMemcpyAsync(win_d, h, (size_t)N, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-        launch_mix(win_d, N, n1, p0a, p0b, step_of(step), dev->ctab_dev, out_d, st) ||
+        launch_mix(win_d, N, 0, N, n1, p0a, p0b, step_of(step), dev->ctab_dev, out_d, st) ||
         cudaMemcpyAsync(out_h, out_d, (size_t)N * 2, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess) {
         cuda_error(cudaGetLastError(), "sdr_mix_carr");
@@ -175,6 +194,22 @@ void sdr_mix_carr(const sdr_buff_t *buff, int ix, int N, double fs, double fc, d
         return;
     }
     memcpy(IQ, out_h, (size_t)N * 2);
+}
+
+int sdrg_mix_carr(const uint8_t *buf_dev, int len, int ix, int N, double fs, double fc,
+                  double phi, sdr_cpx16_t *IQ_dev, void *stream)
+{
+    if (N <= 0) return SDRG_OK;
+    if (!buf_dev || !IQ_dev || len <= 0 || ix < 0 || ix >= len || N > len)
+        return set_error(SDRG_ERR_ARG, "sdrg_mix_carr: bad window ix=%d N=%d len=%d", ix, N, len);
+    Device *dev;
+    int e;
+    if ((e = ensure_device(&dev))) return e;
+    // the phases of sdr_mix_carr (src/sdr_func.c:824-836): restart at the wrap
+    const double step = fc / fs;
+    const int n1 = (ix + N <= len) ? N : len - ix;
+    return launch_mix(buf_dev, len, ix, N, n1, phase_of(phi), n1 < N ? phase_of(phi + step * n1) : 0,
+                      step_of(step), dev->ctab_dev, (char2 *)IQ_dev, (cudaStream_t)stream);
 }
 
 } // extern "C"
