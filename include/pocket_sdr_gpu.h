@@ -320,8 +320,9 @@ int sdrg_acq_graph_captures(const sdrg_acq_plan_t *plan);
  * the caller's stream; needs every group on the 24 000-point sub-transform
  * with split 2 or 8 (48 000 / 192 000 points), else SDRG_ERR_ARG. mode 0:
  * each group's forward / consumer / peak launches on concurrent internal
- * streams. mode -1 (default): the work list where the plan allows it. Grids
- * and results are bit-identical either way. Returns 1 when runs use the work
+ * streams. mode -1 (default): the work list where the plan allows it. The
+ * arithmetic is the same either way (grids agree within FP32 rounding, the
+ * kernels being compiled apart; same peaks). Returns 1 when runs use the work
  * list, 0 when not, or a negative status. A captured graph is re-captured
  * on the next sdrg_acq_run_graph after a change. */
 int sdrg_acq_set_worklist(sdrg_acq_plan_t *plan, int mode);

@@ -249,16 +249,72 @@ __device__ __forceinline__ void prefetch_l2(const float2 *p, int n)
     }
 }
 
+// Bound of every wait of a kernel on an mbarrier (bulk copies into shared
+// memory, partner CTAs; never reached in normal operation). Past it the CTA
+// sets the launch's error word, which the synchronous entry points report and
+// clear, and goes on.
+constexpr long long kBulkWaitCycles = 4000000000LL;     // about 2 s at 1.97 GHz
+
+// ---- synchronisation of the CTAs that share a task --------------------------
+struct CtaSync {
+    __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+struct ClusterSync {
+    __device__ __forceinline__ void operator()() const { cg::this_cluster().sync(); }
+};
+
+// The two CTAs of a 2-way task inside a larger cluster (the work list's
+// narrow tasks in 8-CTA clusters), without holding up the other pairs. Each
+// CTA has two mbarriers (one expected arrival each), used by alternate
+// barrier calls; a call arrives remotely on the partner's barrier of that
+// turn (release at cluster scope, after the CTA's own barrier, so the CTA's
+// writes into the partner's shared memory and its reads of its own come
+// before) and passes when its own barrier of that turn has completed the
+// phase (acquire). With two barriers in turn, a barrier cannot complete a
+// second phase before its owner has seen the first: the partner's next
+// arrival on it needs the owner's arrival of the turn in between. Thread 0
+// keeps the turn and the parities in shared memory (state[0]: turn,
+// state[1 + turn]: parity).
+struct PairSync {
+    uint32_t bar;        // this CTA's two mbarriers (shared::cta address of the first)
+    uint32_t remote;     // the partner's two mbarriers (shared::cluster address)
+    uint32_t *state;     // turn and parities (shared, thread 0)
+    int *err;            // error word: a wait reached kBulkWaitCycles
+    __device__ __forceinline__ void operator()() const
+    {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const uint32_t turn = state[0], par = state[1 + turn];
+            asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];"
+                         ::"r"(remote + 8u * turn) : "memory");
+            const long long t0 = clock64();
+            for (;;) {
+                if (clock64() - t0 >= kBulkWaitCycles) { atomicOr(err, 1); break; }
+                uint32_t done;
+                asm volatile("{\n\t.reg .pred p;\n\t"
+                             "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+                             "selp.u32 %0, 1, 0, p;\n\t}"
+                             : "=r"(done) : "r"(bar + 8u * turn), "r"(par) : "memory");
+                if (done) break;
+            }
+            state[1 + turn] = par ^ 1u;
+            state[0] = turn ^ 1u;
+        }
+        __syncthreads();
+    }
+};
+
 // The sums of one consumer task (PRN prn, bin b; this CTA's share c of its
 // R-way split): per sum, combine + code product into the split's shared
 // memory (dst[j]: CTA j of the task), barrier, inverse transform and power
-// (or complex) store. ns_run iterations, each with its two barriers (cluster
-// barriers with CL), so that CTAs whose tasks have fewer sums - or none
-// (active false) - keep step with the cluster; the twiddles are in tw.
-template <int R, int MODE, int SP, bool CL>
+// (or complex) store. ns_run iterations, each with its two barriers
+// (sync(): over the CTA, the cluster or the pair of CTAs that share the task),
+// so that CTAs whose tasks have fewer sums - or none (active false) - keep
+// step with the others; the twiddles are in tw.
+template <int R, int MODE, int SP, class Sync>
 __device__ __forceinline__ void cons_task(const ConsArgs &a, float2 *sm, const float2 *tw,
                                           float2 *const *dst, int c, int task, int prn, int b,
-                                          int ns_run, bool active)
+                                          int ns_run, bool active, const Sync &sync)
 {
     const int M = SP ? Plan24000::M : a.pl.M;   // SP: compile-time plan
     const int Mc = (M + R - 1) / R;
@@ -266,7 +322,7 @@ __device__ __forceinline__ void cons_task(const ConsArgs &a, float2 *sm, const f
     const float2 *code = a.code + (size_t)(a.code_per_bin ? b : prn) * R * M;
     for (int s = 0; s < ns_run; ++s) {
         // all CTAs of the cluster are done with their shared memory
-        if constexpr (CL) cg::this_cluster().sync(); else __syncthreads();
+        sync();
         const bool run = active && s < a.n_sum;
         const float2 *Xs = a.X + ((size_t)b * a.n_sum + s) * R * M;
         // U positions per iteration: all their global loads are issued
@@ -326,7 +382,7 @@ __device__ __forceinline__ void cons_task(const ConsArgs &a, float2 *sm, const f
                 }
             }
         }
-        if constexpr (CL) cg::this_cluster().sync(); else __syncthreads();
+        sync();
         if (!run) continue;
         // the next sum's spectra head for L2 during this sum's transform
         if (s + 1 < a.n_sum && threadIdx.x < R && q1 > q0)
@@ -386,7 +442,8 @@ __global__ void __launch_bounds__(512, 1) cons_kernel(ConsArgs a)
     } else {
         dst[0] = sm;
     }
-    cons_task<R, MODE, SP, (R > 1)>(a, sm, tw, dst, c, task, prn, b, a.n_sum, true);
+    if constexpr (R > 1) cons_task<R, MODE, SP>(a, sm, tw, dst, c, task, prn, b, a.n_sum, true, ClusterSync{});
+    else cons_task<R, MODE, SP>(a, sm, tw, dst, c, task, prn, b, a.n_sum, true, CtaSync{});
     // keep remote shared memory alive until every CTA has finished reading
     if constexpr (R > 1) cg::this_cluster().sync();
 }
@@ -417,6 +474,7 @@ struct WorkArgs {
     int n_group;
     int n_task[2];          // tasks of the wide (R = 8) and narrow (R = 2) queues
     int *next;              // [2] next unclaimed task of each queue, 0 at launch
+    int *err;               // error word: a pair wait reached its bound
     WorkGroup g[kMaxWorkGroups];
 };
 
@@ -445,8 +503,20 @@ __global__ void __launch_bounds__(512, 1) work_cons_kernel(WorkArgs a)
     float2 *sm = smem;
     float2 *tw = smem + Plan24000::M;
     __shared__ int unit[3];           // queue (0 wide, 1 narrow, -1 none), first task, tasks
+    __shared__ __align__(8) uint64_t pair_bar[2];
+    __shared__ uint32_t pair_state[3];
     cg::cluster_group cl = cg::this_cluster();
     const int csize = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+    const uint32_t bar0 = (uint32_t)__cvta_generic_to_shared(pair_bar);
+    uint32_t remote0;                 // the partner CTA (rank ^ 1) of narrow tasks
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote0) : "r"(bar0), "r"(rank ^ 1));
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 2; ++k)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0 + 8u * k) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        pair_state[0] = pair_state[1] = pair_state[2] = 0u;
+    }
+    const PairSync pair{bar0, remote0, pair_state, a.err};
     load_twiddles(tw, a.tw, Plan24000::TWTOT);
     for (;;) {
         if (rank == 0 && threadIdx.x == 0) {
@@ -462,18 +532,14 @@ __global__ void __launch_bounds__(512, 1) work_cons_kernel(WorkArgs a)
             }
             unit[0] = q; unit[1] = t; unit[2] = n;
         }
-        cl.sync();                    // the unit (and, at first, the twiddles) visible
+        cl.sync();                    // the unit (and, at first, the twiddles and
+                                      // every CTA's pair barriers) visible
         const int *lu = cl.map_shared_rank(unit, 0);
         const int q = lu[0], t0 = lu[1], n = lu[2];
         if (q < 0) break;             // uniform across the cluster
         const int R = q == 0 ? 8 : 2;
         const int slot = rank / R, c = rank % R;
         const bool active = slot < n;
-        int ns_run = 0;               // the unit's longest task, in sums
-        for (int k = 0; k < n; ++k) {
-            const int gk = work_group_of(a, q, t0 + k);
-            ns_run = max(ns_run, gk >= 0 ? a.g[gk].n_sum : 0);
-        }
         const int gi = active ? work_group_of(a, q, t0 + slot) : -1;
         const WorkGroup &G = a.g[gi >= 0 ? gi : 0];
         const int local = t0 + slot - G.task0;
@@ -492,12 +558,15 @@ __global__ void __launch_bounds__(512, 1) work_cons_kernel(WorkArgs a)
             float2 *dst[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j) dst[j] = cl.map_shared_rank(sm, j);
-            cons_task<8, 0, 1, true>(ca, sm, tw, dst, c, local, prn, b, ns_run, run);
+            cons_task<8, 0, 1>(ca, sm, tw, dst, c, local, prn, b, run ? G.n_sum : 0, run,
+                               ClusterSync{});
         } else {
             float2 *dst[2];
 #pragma unroll
             for (int j = 0; j < 2; ++j) dst[j] = cl.map_shared_rank(sm, 2 * slot + j);
-            cons_task<2, 0, 1, true>(ca, sm, tw, dst, c, local, prn, b, ns_run, run);
+            // both CTAs of the pair run the same task (or none): the pair's
+            // barriers alone keep them in step
+            cons_task<2, 0, 1>(ca, sm, tw, dst, c, local, prn, b, run ? G.n_sum : 0, run, pair);
         }
     }
     // the leader's unit word and every CTA's shared memory stay alive until
@@ -601,10 +670,6 @@ struct StoreComplexRt {
 };
 
 // ---- bulk copies through the TMA engine (cp.async.bulk, mbarrier) ----------
-// Bound of every wait for a bulk copy (never reached in normal operation).
-// Past it a CTA sets the launch's error word (ConsArgs::stage_err), which the
-// synchronous entry points report and clear.
-constexpr long long kBulkWaitCycles = 4000000000LL;     // about 2 s at 1.97 GHz
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
 {
@@ -1000,17 +1065,18 @@ static int thread_stage_err(int **out, cudaStream_t st)
 // After a synchronous call that ran a staged split (its work on st has
 // completed): reports, and clears, a bulk-copy wait of stage_ifft_kernel that
 // reached its bound, recorded in the error word err.
-static int stage_wait_check(const FftPlan *pl, int *err, cudaStream_t st)
+static int stage_wait_check(const FftPlan *pl, int *err, cudaStream_t st, bool always = false)
 {
-    if (!pl || pl->R <= 8 || !err) return SDRG_OK;
+    if (!always && (!pl || pl->R <= 8)) return SDRG_OK;
+    if (!err) return SDRG_OK;
     int v = 0;
     SDRG_CUDA(cudaMemcpyAsync(&v, err, sizeof(int), cudaMemcpyDeviceToHost, st));
     SDRG_CUDA(cudaStreamSynchronize(st));
     if (!v) return SDRG_OK;
     SDRG_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
     SDRG_CUDA(cudaStreamSynchronize(st));
-    return set_error(SDRG_ERR_CUDA, "staged FFT: a bulk copy into shared memory did not "
-                     "complete within its bound; results of that call are not valid");
+    return set_error(SDRG_ERR_CUDA, "FFT consumer: a wait for a bulk copy into shared memory "
+                     "or for a partner CTA reached its bound; results of that call are not valid");
 }
 
 // Plan for a batch of n transforms of length N. The default split puts one
@@ -1838,6 +1904,7 @@ static int launch_run_worklist(sdrg_acq_plan_t *plan, Device *dev, const uint8_t
     fm.n_group = ng;
     WorkArgs wa = {};
     wa.pl = pl0->k; wa.tw = pl0->tw_dev; wa.n_group = ng; wa.next = plan->wl_next;
+    wa.err = plan->stage_err;
     for (int gi = 0; gi < ng; ++gi) {
         GroupState &G = plan->g[gi];
         const sdrg_acq_sig_t &s = G.sig;
@@ -2087,6 +2154,7 @@ int sdrg_acq_run_host(sdrg_acq_plan_t *plan, const uint8_t *const *if_host, cons
                 cudaStreamSynchronize(st) != cudaSuccess))
         e = cuda_error(cudaGetLastError(), "sdrg_acq_run_host D2H");
     cudaStreamSynchronize(st);
+    if (!e && use_worklist(plan)) e = stage_wait_check(nullptr, plan->stage_err, st, true);
     for (size_t gi = 0; gi < plan->g.size() && !e; ++gi)
         e = stage_wait_check(plan->g[gi].pl, plan->stage_err, st);
     for (auto p : bufs) if (p) cudaFree(p);

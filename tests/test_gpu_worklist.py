@@ -1,8 +1,10 @@
 """The work-list consumer (sdrg_acq_set_worklist): every group's (PRN,
 Doppler bin) tasks consumed by one persistent launch against the per-group
-launches on concurrent streams - the same grids and results, bit for bit,
-including narrow units that straddle two groups and groups of different sum
-counts; CUDA-graph replay of the work list; plans it cannot take."""
+launches on concurrent streams - the same arithmetic in another kernel, so
+grids equal within FP32 rounding (1e-5 per cell of max(|P|, mean P)) and the
+same peaks - including narrow units that straddle two groups and groups of
+different sum counts; CUDA-graph replay of the work list, bit for bit against
+its own stream launch; plans it cannot take."""
 import numpy as np
 import pytest
 
@@ -33,9 +35,13 @@ def test_worklist_equals_per_group_launches():
         r1 = plan.run_host(wl.bufs, wl.ix)
         g1 = _grids(plan, wl)
         for a, b in zip(g0, g1):
-            assert np.array_equal(a, b)
-        assert np.array_equal(r0, r1)
-        # a second run over the same buffers (queue heads re-armed)
+            floor = float(a.mean(dtype=np.float64))
+            err = np.abs(a.astype(np.float64) - b) / np.maximum(np.abs(a), floor)
+            assert err.max() <= 1e-5, float(err.max())
+        assert np.array_equal(r0["bin"], r1["bin"]) and np.array_equal(r0["offset"], r1["offset"])
+        assert np.abs(r0["cn0"] - r1["cn0"]).max() < 1e-3
+        # a second run over the same buffers (queue heads re-armed): the same
+        # kernels on the same data, bit for bit
         r2 = plan.run_host(wl.bufs, wl.ix)
         assert np.array_equal(r1, r2)
     finally:
