@@ -86,8 +86,9 @@ def parse():
                     help="weak: one IF block per rank; strong: PRNs dealt over ranks")
     ap.add_argument("--t-sum", type=float, default=20e-3,
                     help="non-coherent time per group (s)")
-    ap.add_argument("--worklist", type=int, choices=(-1, 0, 1), default=-1,
-                    help="consumer launches: 1 one work-list launch, 0 per group, -1 automatic")
+    ap.add_argument("--worklist", type=int, choices=(-1, 0, 1), default=0,
+                    help="consumer launches: 0 per group (default), 1 one work-list launch, "
+                         "-1 the work list where the plan allows it")
     return ap.parse_args()
 
 
@@ -517,7 +518,7 @@ def acq_measure(args, name: str, steps: int, warmup: int, dist, rank: int, world
 
     # the other consumer launch mode on the same plan and buffers, for comparison
     alt = None
-    if plan.set_worklist(0 if worklist else -1) != worklist:
+    if plan.set_worklist(0 if worklist else -1) != worklist:   # the other mode, if any
         for _ in range(2):
             step()
         torch.cuda.synchronize()

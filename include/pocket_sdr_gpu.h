@@ -318,9 +318,10 @@ int sdrg_acq_graph_captures(const sdrg_acq_plan_t *plan);
  * where they fit, of 2 elsewhere; tasks claimed dynamically, the 8-way
  * splits first), after one forward-transform launch for all groups, all on
  * the caller's stream; needs every group on the 24 000-point sub-transform
- * with split 2 or 8 (48 000 / 192 000 points), else SDRG_ERR_ARG. mode 0:
- * each group's forward / consumer / peak launches on concurrent internal
- * streams. mode -1 (default): the work list where the plan allows it. The
+ * with split 2 or 8 (48 000 / 192 000 points), else SDRG_ERR_ARG. mode 0
+ * (default, the faster on the multi-GNSS benchmark): each group's forward /
+ * consumer / peak launches on concurrent internal streams. mode -1: the work
+ * list where the plan allows it, else per-group launches. The
  * arithmetic is the same either way (grids agree within FP32 rounding, the
  * kernels being compiled apart; same peaks). Returns 1 when runs use the work
  * list, 0 when not, or a negative status. A captured graph is re-captured

@@ -97,10 +97,11 @@ class AcqPlan:
         if st:
             check("sdrg_acq_run_graph" if graph else "sdrg_acq_run")
 
-    def set_worklist(self, mode: int = -1) -> bool:
+    def set_worklist(self, mode: int = 1) -> bool:
         """Consumer issue mode (sdrg_acq_set_worklist): 1 the single
-        persistent work-list launch, 0 per-group launches on concurrent
-        streams, -1 automatic. Returns whether runs use the work list."""
+        persistent work-list launch, 0 (the plan's default) per-group launches
+        on concurrent streams, -1 the work list where the plan allows it.
+        Returns whether runs use the work list."""
         r = lib.sdrg_acq_set_worklist(self.handle, int(mode))
         if r < 0:
             check("sdrg_acq_set_worklist")

@@ -31,13 +31,19 @@ struct TapArgs {
     int2 jk[SDR_MAX_CORR];
 };
 
-// One block per (tap, half), blockDim.x = 256: the half-dot products of the
-// tap (c12[2 tap + h]); the last block to finish then applies the polarity
-// test and the scaling for every tap (corr[n], C[2]) and re-arms the ticket.
+// Samples of one half-dot product summed by one block (256 threads x 4).
+constexpr int kCorrChunk = 1024;
+
+// Grid (tap, half, chunk), blockDim.x = 256: block (tap, h, ch) sums the
+// sign products of samples [ch kCorrChunk, (ch + 1) kCorrChunk) of the 16-
+// aligned part of the tap's half-dot into acc[2 tap + h] (int32 atomics: the
+// integer sum is exact whatever the order). The last block to finish (ticket)
+// adds each half's float tail in the reference's order, scales, applies the
+// polarity test and writes corr[n], C[2]; it leaves acc and the ticket at 0.
 template <int CPX>
 __global__ void __launch_bounds__(256) corr_std_kernel(
     const char2 *__restrict__ IQ, const char2 *__restrict__ code, int N, TapArgs ta, float cs,
-    float2 *c12, unsigned *ticket, float2 *corr, float2 *C)
+    int2 *acc, unsigned *ticket, float2 *corr, float2 *C)
 {
     const int tap = blockIdx.x, h = blockIdx.y;
     const int j = ta.jk[tap].x, k = ta.jk[tap].y;
@@ -45,66 +51,85 @@ __global__ void __launch_bounds__(256) corr_std_kernel(
     const char2 *x = IQ + (h == 0 ? 0 : j);
     const char2 *y = code + (size_t)k * N + (h == 0 ? N - j : 0);
     const int main_len = (len / 16) * 16;
+    const int c0 = blockIdx.z * kCorrChunk;
     int sr = 0, si = 0;
-    for (int i = threadIdx.x; i < main_len; i += blockDim.x) {
-        const char2 a = x[i], c = y[i];
-        if (CPX) {
-            sr += sgn_mul8(a.x, c.x) + sgn_mul8(a.y, c.y);
-            si += sgn_mul8(a.y, c.x) + sgn_mul8(a.x, neg8(c.y));
-        } else {
-            sr += sgn_mul8(a.x, c.x);
-            si += sgn_mul8(a.y, c.y);
-        }
-    }
+    if (c0 < main_len) {
+        const int c1 = min(main_len, c0 + kCorrChunk);
+        char2 a[4], c[4];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        sr += __shfl_xor_sync(0xffffffffu, sr, o);
-        si += __shfl_xor_sync(0xffffffffu, si, o);
-    }
-    __shared__ int red[2][8];
-    __shared__ bool last;
-    const int w = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0) { red[0][w] = sr; red[1][w] = si; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int tr = 0, ti = 0;
-        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) { tr += red[0][i]; ti += red[1][i]; }
-        float fr = (float)tr, fi = (float)ti;
-        // the tail in float, one product at a time, in the reference's order
-        for (int i = main_len; i < len; ++i) {
-            const char2 a = x[i], c = y[i];
+        for (int u = 0; u < 4; ++u) {
+            const int i = c0 + threadIdx.x + u * 256;
+            a[u] = i < c1 ? x[i] : make_char2(0, 0);
+            c[u] = i < c1 ? y[i] : make_char2(0, 0);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
             if (CPX) {
-                fr = __fadd_rn(fr, (float)(a.x * c.x + a.y * c.y));
-                fi = __fadd_rn(fi, (float)(a.y * c.x - a.x * c.y));
+                sr += sgn_mul8(a[u].x, c[u].x) + sgn_mul8(a[u].y, c[u].y);
+                si += sgn_mul8(a[u].y, c[u].x) + sgn_mul8(a[u].x, neg8(c[u].y));
             } else {
-                fr = __fadd_rn(fr, (float)(a.x * c.x));
-                fi = __fadd_rn(fi, (float)(a.y * c.y));
+                sr += sgn_mul8(a[u].x, c[u].x);
+                si += sgn_mul8(a[u].y, c[u].y);
             }
         }
-        c12[2 * tap + h] = make_float2(__fmul_rn(fr, cs), __fmul_rn(fi, cs));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            sr += __shfl_xor_sync(0xffffffffu, sr, o);
+            si += __shfl_xor_sync(0xffffffffu, si, o);
+        }
+        if ((threadIdx.x & 31) == 0 && (sr || si)) {
+            atomicAdd(&acc[2 * tap + h].x, sr);
+            atomicAdd(&acc[2 * tap + h].y, si);
+        }
+    }
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
         __threadfence();
-        last = atomicAdd(ticket, 1u) == gridDim.x * gridDim.y - 1;
+        last = atomicAdd(ticket, 1u) == gridDim.x * gridDim.y * gridDim.z - 1;
     }
     __syncthreads();
     if (!last) return;
-    // every block's c12 is visible (each fenced its store before its ticket)
     __threadfence();
-    __shared__ float sign;
+    // every half: its integer sum, then its tail in float one product at a
+    // time in the reference's order, scaled
+    __shared__ float2 c12[2 * SDR_MAX_CORR];
     const int n = ta.n;
+    for (int q = threadIdx.x; q < 2 * n; q += blockDim.x) {
+        const int tq = q >> 1, hq = q & 1;
+        const int jq = ta.jk[tq].x, kq = ta.jk[tq].y;
+        const int lq = hq == 0 ? jq : N - jq;
+        const char2 *xq = IQ + (hq == 0 ? 0 : jq);
+        const char2 *yq = code + (size_t)kq * N + (hq == 0 ? N - jq : 0);
+        float fr = (float)atomicExch(&acc[q].x, 0), fi = (float)atomicExch(&acc[q].y, 0);
+        for (int i = (lq / 16) * 16; i < lq; ++i) {
+            const char2 av = xq[i], cv = yq[i];
+            if (CPX) {
+                fr = __fadd_rn(fr, (float)(av.x * cv.x + av.y * cv.y));
+                fi = __fadd_rn(fi, (float)(av.y * cv.x - av.x * cv.y));
+            } else {
+                fr = __fadd_rn(fr, (float)(av.x * cv.x));
+                fi = __fadd_rn(fi, (float)(av.y * cv.y));
+            }
+        }
+        c12[q] = make_float2(__fmul_rn(fr, cs), __fmul_rn(fi, cs));
+    }
+    __syncthreads();
+    __shared__ float sign;
     if (threadIdx.x == 0) {
         float dot = 0.0f;
         for (int i = 0; i < 3 && i < n; ++i) {
-            const float2 a = __ldcg(c12 + 2 * i), b = __ldcg(c12 + 2 * i + 1);
+            const float2 a = c12[2 * i], b = c12[2 * i + 1];
             dot = __fadd_rn(dot, __fmaf_rn(a.x, b.x, __fmul_rn(a.y, b.y)));
         }
         sign = dot < 0.0f ? -1.0f : 1.0f;
-        if (n > 0) { C[0] = __ldcg(c12); C[1] = __ldcg(c12 + 1); }
+        if (n > 0) { C[0] = c12[0]; C[1] = c12[1]; }
         *ticket = 0u;
     }
     __syncthreads();
     const float fN = (float)N;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const float2 a = __ldcg(c12 + 2 * i), b = __ldcg(c12 + 2 * i + 1);
+        const float2 a = c12[2 * i], b = c12[2 * i + 1];
         corr[i] = make_float2(__fdiv_rn(__fadd_rn(a.x, __fmul_rn(sign, b.x)), fN),
                               __fdiv_rn(__fadd_rn(a.y, __fmul_rn(sign, b.y)), fN));
     }
@@ -135,20 +160,20 @@ static bool tap_params(int N, double coff, const double *pos, int n, int nbank, 
     return true;
 }
 
-// The thread's device scratch of the synchronous correlators: c12 partials
-// (2 SDR_MAX_CORR), outputs (SDR_MAX_CORR + 2) and the finishing ticket
-// (zeroed once; the finishing block leaves it 0).
-static int corr_scratch(float2 **c12, float2 **out, unsigned **ticket, cudaStream_t st)
+// The thread's device scratch of the synchronous correlators: integer
+// partial sums (2 SDR_MAX_CORR int2), outputs (SDR_MAX_CORR + 2) and the
+// finishing ticket, zeroed once (the finishing block leaves them 0).
+static int corr_scratch(int2 **acc, float2 **out, unsigned **ticket, cudaStream_t st)
 {
     ThreadCtx &c = tctx();
-    const size_t bytes = sizeof(float2) * (3 * SDR_MAX_CORR + 2) + 16;
+    const size_t bytes = sizeof(int2) * 2 * SDR_MAX_CORR + sizeof(float2) * (SDR_MAX_CORR + 2) + 16;
     const bool fresh = c.corr_dev.size < bytes;
     int e;
     if ((e = c.corr_dev.reserve(bytes))) return e;
-    *c12 = (float2 *)c.corr_dev.ptr;
-    *out = *c12 + 2 * SDR_MAX_CORR;
+    *acc = (int2 *)c.corr_dev.ptr;
+    *out = (float2 *)(*acc + 2 * SDR_MAX_CORR);
     *ticket = (unsigned *)(*out + SDR_MAX_CORR + 2);
-    if (fresh) SDRG_CUDA(cudaMemsetAsync(*ticket, 0, sizeof(unsigned), st));
+    if (fresh) SDRG_CUDA(cudaMemsetAsync(c.corr_dev.ptr, 0, bytes, st));
     return SDRG_OK;
 }
 
@@ -158,14 +183,16 @@ static int corr_std_run(const char2 *IQ_dev, const char2 *code_dev, int N, const
                         int cpx, float2 *out_h, sdr_cpx_t *corr, sdr_cpx_t *C, cudaStream_t st)
 {
     const int n = ta.n;
-    float2 *c12, *out_d;
+    int2 *acc;
+    float2 *out_d;
     unsigned *ticket;
     int e;
-    if ((e = corr_scratch(&c12, &out_d, &ticket, st))) return e;
-    if (cpx) corr_std_kernel<1><<<dim3(n, 2), 256, 0, st>>>(IQ_dev, code_dev, N, ta, kCScale, c12,
-                                                           ticket, out_d, out_d + n);
-    else     corr_std_kernel<0><<<dim3(n, 2), 256, 0, st>>>(IQ_dev, code_dev, N, ta, kCScale, c12,
-                                                           ticket, out_d, out_d + n);
+    if ((e = corr_scratch(&acc, &out_d, &ticket, st))) return e;
+    const dim3 grid((unsigned)n, 2, (unsigned)((N + kCorrChunk - 1) / kCorrChunk));
+    if (cpx) corr_std_kernel<1><<<grid, 256, 0, st>>>(IQ_dev, code_dev, N, ta, kCScale, acc,
+                                                     ticket, out_d, out_d + n);
+    else     corr_std_kernel<0><<<grid, 256, 0, st>>>(IQ_dev, code_dev, N, ta, kCScale, acc,
+                                                     ticket, out_d, out_d + n);
     SDRG_CUDA(cudaGetLastError());
     SDRG_CUDA(cudaMemcpyAsync(out_h, out_d, sizeof(float2) * (n + 2), cudaMemcpyDeviceToHost, st));
     SDRG_CUDA(cudaStreamSynchronize(st));

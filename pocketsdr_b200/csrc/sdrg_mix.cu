@@ -30,16 +30,39 @@ __device__ __forceinline__ char2 mix_byte(uint8_t byte, uint32_t phase, const ch
 // n < nsplit ? p0a + n step : p0b + (n - nsplit) step (the restart at the
 // buffer wrap). 16 samples per thread: where its 16 samples lie contiguous and
 // 16-byte aligned in the buffer and the output is 16-byte aligned, one
-// 16-byte load and two 16-byte stores; otherwise sample by sample. HBM bound:
-// 1 byte read and 2 bytes written per sample.
+// 16-byte load, the nibbles of four samples sign-extended at once, each
+// rotation as two dp2a of the sample bytes with the carrier's 16-bit
+// coefficient pairs, and two 16-byte stores; otherwise sample by sample
+// (mix_byte). HBM bound by design: 1 byte read and 2 bytes written per sample.
 constexpr int kMixPer = 16;
+
+// Sign-extended nibbles of four packed samples: the low (I) or high (Q)
+// nibble of each byte of w as a signed byte (a nibble n >= 8 becomes n | 0xF0:
+// the multiply sets the upper four bits of exactly those bytes, no carries).
+__device__ __forceinline__ uint32_t nibbles_i(uint32_t w)
+{
+    const uint32_t lo = w & 0x0F0F0F0Fu;
+    return lo | ((lo & 0x08080808u) * 0x1Eu);
+}
+__device__ __forceinline__ uint32_t nibbles_q(uint32_t w)
+{
+    return nibbles_i(w >> 4);
+}
 
 __global__ void __launch_bounds__(256) mix_kernel(
     const uint8_t *__restrict__ buf, int len, int ix, int N, int nsplit, uint32_t p0a,
     uint32_t p0b, uint32_t step, const char2 *__restrict__ ctab_g, char2 *__restrict__ out)
 {
     __shared__ char2 ctab[256];
-    for (int i = threadIdx.x; i < 256; i += blockDim.x) ctab[i] = ctab_g[i];
+    // the same carrier as 16-bit coefficient pairs for dp2a: I' = (cI, -cQ) . (I, Q),
+    // Q' = (cQ, cI) . (I, Q) - the exact integer products and sums of mix_byte
+    __shared__ uint2 cdp[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+        const char2 c = ctab_g[i];
+        ctab[i] = c;
+        cdp[i] = make_uint2((uint32_t)(uint16_t)(int16_t)c.x | ((uint32_t)(uint16_t)(int16_t)(-c.y) << 16),
+                            (uint32_t)(uint16_t)(int16_t)c.y | ((uint32_t)(uint16_t)(int16_t)c.x << 16));
+    }
     __syncthreads();
     const long long n0l = (long long)kMixPer * (blockIdx.x * (long long)blockDim.x + threadIdx.x);
     if (n0l >= N) return;
@@ -55,13 +78,21 @@ __global__ void __launch_bounds__(256) mix_kernel(
         uint32_t ph = n0 < nsplit ? p0a + step * (uint32_t)n0 : p0b + step * (uint32_t)(n0 - nsplit);
         uint32_t o[8];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const char2 a = mix_byte((uint8_t)(wd[k >> 1] >> (16 * (k & 1))), ph, ctab);
-            ph += step;
-            const char2 b = mix_byte((uint8_t)(wd[k >> 1] >> (16 * (k & 1) + 8)), ph, ctab);
-            ph += step;
-            o[k] = (uint32_t)(uint8_t)a.x | ((uint32_t)(uint8_t)a.y << 8) |
-                   ((uint32_t)(uint8_t)b.x << 16) | ((uint32_t)(uint8_t)b.y << 24);
+        for (int q = 0; q < 4; ++q) {
+            const uint32_t I4 = nibbles_i(wd[q]), Q4 = nibbles_q(wd[q]);
+            uint32_t t[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                // sample k of the word: bytes (I, Q) for dp2a
+                const uint32_t sv = __byte_perm(I4, Q4, (uint32_t)(k | ((4 + k) << 4)));
+                const uint2 cf = cdp[ph >> 24];
+                ph += step;
+                const int ii = __dp2a_lo((int)cf.x, (int)sv, 0);
+                const int qq = __dp2a_lo((int)cf.y, (int)sv, 0);
+                t[k] = __byte_perm((uint32_t)ii, (uint32_t)qq, 0x0040u);   // (I', Q') bytes
+            }
+            o[2 * q] = __byte_perm(t[0], t[1], 0x5410u);
+            o[2 * q + 1] = __byte_perm(t[2], t[3], 0x5410u);
         }
         uint4 *d = (uint4 *)(out + n0);
         d[0] = make_uint4(o[0], o[1], o[2], o[3]);

@@ -1284,7 +1284,8 @@ struct sdrg_acq_plan {
     // work-list consumer (sdrg_acq_set_worklist): eligible when every group
     // is on the 24 000-point compile-time plan with split 2 or 8
     bool wl_ok = false;
-    int wl_mode = -1;           // -1 automatic, 0 per-group launches, 1 work list
+    int wl_mode = 0;            // 0 per-group launches, 1 work list (-1: the work list
+                                // where allowed)
     int *wl_next = nullptr;     // [2] device queue heads
 };
 

@@ -55,7 +55,7 @@ def test_worklist_graph_replay_and_narrow_only_plan():
     wl.groups[0].prns = wl.groups[0].prns[:11]      # 11 x 41 tasks: a partial last unit
     plan = _plan(wl)
     try:
-        assert plan.set_worklist(-1) is True
+        assert plan.set_worklist(1) is True
         ref = plan.run_host(wl.bufs, wl.ix)
         bufs = [torch.from_numpy(b).cuda() for b in wl.bufs]
         res = torch.empty(plan.n_res * acquire.RESULT_DTYPE.itemsize, dtype=torch.uint8,
@@ -73,9 +73,10 @@ def test_worklist_graph_replay_and_narrow_only_plan():
 
 
 def test_worklist_refused_for_staged_splits():
+    from pocketsdr_b200.acquire import AcqPlan
     from pocketsdr_b200._lib import GpuError
     wl = synth.acq_long_48mhz(prn_limit=1, n_sum=1, bins=np.array([0.0], np.float32))
-    plan = _plan(wl)
+    plan = AcqPlan(wl.groups, [synth.long_code_ffts(g) for g in wl.groups])
     try:
         assert plan.set_worklist(-1) is False
         with pytest.raises(GpuError, match="24 000-point"):
