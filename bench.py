@@ -302,10 +302,18 @@ def acq_parity(wl, gpu_res, ref, grids_gpu=None) -> dict:
     r = ref["res"]
     same = (gpu_res["bin"] == r["bin"]) & (gpu_res["offset"] == r["offset"])
     tie = ~same & (np.abs(r["at_gpu"] - r["pmax"]) <= 1e-5 * r["pmax"])
+    # a replica tiled from a shorter periodic code (the 12 MHz L1 C/A search:
+    # 1 ms x 4) makes the grid periodic in the offset: its equal maxima lie
+    # one code period apart, in the same Doppler bin
+    period = np.concatenate([np.full(len(g.prns), g.N // g.tile if g.tile > 1 else 0)
+                             for g in wl.groups])
+    same_mod = tie & (gpu_res["bin"] == r["bin"]) & (period > 0) & \
+        (gpu_res["offset"] % np.maximum(period, 1) == r["offset"] % np.maximum(period, 1))
     d_cn0 = np.abs(gpu_res["cn0"].astype(np.float64) - r["cn0"])
     d_fd = np.abs(gpu_res["fd"] - r["fd"])
     out = {"peaks_match": f"{int(same.sum())}/{len(r)}",
            "peaks_tied": int(tie.sum()),
+           "tied_same_bin_offset_mod_code_period": int(same_mod.sum()),
            "peaks_differ": int((~same & ~tie).sum()),
            "cn0_max_diff_db": float(d_cn0[same | tie].max()) if (same | tie).any() else None,
            "fine_dop_max_diff_hz": float(d_fd[same].max()) if same.any() else None,

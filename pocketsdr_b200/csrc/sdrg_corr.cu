@@ -280,14 +280,16 @@ static void corr_std_host(const sdr_cpx16_t *IQ, const sdr_cpx16_t *code, int N,
         c.dev[0].reserve(iqb + 16) || c.host[2].reserve(sizeof(float2) * (SDR_MAX_CORR + 2)))
         goto fail;
     {
+        // the IQ window goes first, so that its copy overlaps the comparison
+        // of the code banks on the host
         uint8_t *h = (uint8_t *)c.host[0].ptr;
         const char2 *code_d = nullptr;
-        if (bank_on_device(code, N, mask, h + iqb, st, &code_d)) goto fail;
         memcpy(h, IQ, iqb);
         if (cudaMemcpyAsync(c.dev[0].ptr, h, iqb, cudaMemcpyHostToDevice, st) != cudaSuccess) {
             cuda_error(cudaGetLastError(), "corr_std H2D");
             goto fail;
         }
+        if (bank_on_device(code, N, mask, h + iqb, st, &code_d)) goto fail;
         if (corr_std_run((const char2 *)c.dev[0].ptr, code_d, N, ta, cpx, (float2 *)c.host[2].ptr,
                          corr, C, st))
             goto fail;
