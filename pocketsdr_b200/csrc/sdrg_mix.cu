@@ -34,7 +34,11 @@ __device__ __forceinline__ char2 mix_byte(uint8_t byte, uint32_t phase, const ch
 // rotation as two dp2a of the sample bytes with the carrier's 16-bit
 // coefficient pairs, and two 16-byte stores; otherwise sample by sample
 // (mix_byte). HBM bound by design: 1 byte read and 2 bytes written per sample.
-constexpr int kMixPer = 16;
+#ifndef SDRG_MIX_VEC
+#define SDRG_MIX_VEC 1
+#endif
+constexpr int kMixVec = SDRG_MIX_VEC;     // 16-byte loads per thread
+constexpr int kMixPer = 16 * kMixVec;
 
 // Sign-extended nibbles of four packed samples: the low (I) or high (Q)
 // nibble of each byte of w as a signed byte (a nibble n >= 8 becomes n | 0xF0:
@@ -73,30 +77,35 @@ __global__ void __launch_bounds__(256) mix_kernel(
                       (n0 + kMixPer <= nsplit || n0 >= nsplit) &&
                       ((((uintptr_t)(buf + pos0)) | ((uintptr_t)(out + n0))) & 15u) == 0;
     if (fast) {
-        const uint4 w = *(const uint4 *)(buf + pos0);
-        const uint32_t wd[4] = {w.x, w.y, w.z, w.w};
+        uint4 w[kMixVec];
+#pragma unroll
+        for (int v = 0; v < kMixVec; ++v) w[v] = *(const uint4 *)(buf + pos0 + 16 * v);
         uint32_t ph = n0 < nsplit ? p0a + step * (uint32_t)n0 : p0b + step * (uint32_t)(n0 - nsplit);
-        uint32_t o[8];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const uint32_t I4 = nibbles_i(wd[q]), Q4 = nibbles_q(wd[q]);
-            uint32_t t[4];
+        for (int v = 0; v < kMixVec; ++v) {
+            const uint32_t wd[4] = {w[v].x, w[v].y, w[v].z, w[v].w};
+            uint32_t o[8];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                // sample k of the word: bytes (I, Q) for dp2a
-                const uint32_t sv = __byte_perm(I4, Q4, (uint32_t)(k | ((4 + k) << 4)));
-                const uint2 cf = cdp[ph >> 24];
-                ph += step;
-                const int ii = __dp2a_lo((int)cf.x, (int)sv, 0);
-                const int qq = __dp2a_lo((int)cf.y, (int)sv, 0);
-                t[k] = __byte_perm((uint32_t)ii, (uint32_t)qq, 0x0040u);   // (I', Q') bytes
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t I4 = nibbles_i(wd[q]), Q4 = nibbles_q(wd[q]);
+                uint32_t t[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    // sample k of the word: bytes (I, Q) for dp2a
+                    const uint32_t sv = __byte_perm(I4, Q4, (uint32_t)(k | ((4 + k) << 4)));
+                    const uint2 cf = cdp[ph >> 24];
+                    ph += step;
+                    const int ii = __dp2a_lo((int)cf.x, (int)sv, 0);
+                    const int qq = __dp2a_lo((int)cf.y, (int)sv, 0);
+                    t[k] = __byte_perm((uint32_t)ii, (uint32_t)qq, 0x0040u);   // (I', Q') bytes
+                }
+                o[2 * q] = __byte_perm(t[0], t[1], 0x5410u);
+                o[2 * q + 1] = __byte_perm(t[2], t[3], 0x5410u);
             }
-            o[2 * q] = __byte_perm(t[0], t[1], 0x5410u);
-            o[2 * q + 1] = __byte_perm(t[2], t[3], 0x5410u);
+            uint4 *d = (uint4 *)(out + n0 + 16 * v);
+            d[0] = make_uint4(o[0], o[1], o[2], o[3]);
+            d[1] = make_uint4(o[4], o[5], o[6], o[7]);
         }
-        uint4 *d = (uint4 *)(out + n0);
-        d[0] = make_uint4(o[0], o[1], o[2], o[3]);
-        d[1] = make_uint4(o[4], o[5], o[6], o[7]);
     } else {
         for (int n = n0; n < N && n < n0 + kMixPer; ++n) {
             int pos = ix + n;
