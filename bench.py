@@ -684,6 +684,17 @@ def run_ours(args):
         keep = ("value", "unit", "ms_per_step", "grid_ms", "refine_ms", "cost_vs_grid", "e2e",
                 "config", "vs_fp64_oracle", "vs_truth", "clocks", "roofline")
         line["extra"]["refine_12mhz"] = {k: rf[k] for k in keep if k in rf}
+        # the tracking correlator batch (256 channels x 44 taps, 100 ms steps)
+        tr = track_measure(args, 3, 3, cpu_leg)
+        keep = ("value", "unit", "ms_per_step", "steps", "config", "e2e", "gpu_launches",
+                "tap_samples_per_s", "clocks", "cpu_baseline")
+        line["extra"]["track_24mhz"] = {k: tr[k] for k in keep if k in tr}
+        # the weak-signal long coherent search at full size (480 000-point
+        # transforms, 42 PRNs x 401 bins x 20 sums; 1.6 s per step)
+        lg, _ = acq_measure(args, "acq_long_48mhz", 2, 3, dist, rank, world, local, cpu_leg)
+        keep = ("value", "unit", "ms_per_step", "steps", "config", "e2e", "gpu_launches",
+                "roofline", "clocks", "cpu_baseline")
+        line["extra"]["acq_long_48mhz"] = {k: lg[k] for k in keep if k in lg}
     if rank == 0:
         emit(line)
     if dist:
@@ -862,13 +873,14 @@ def cpu_track_rate(wl, specs_list, banks_host, max_jobs=600):
 TRACK_EPOCHS_PER_STEP = 100   # one step = 100 ms of the stream
 
 
-def run_track(args):
+def track_measure(args, steps: int, warmup: int, cpu_leg: bool) -> dict:
     """Tracking-correlator workload: every step is 100 ms of the 24 MHz
     8-antenna stream, 100 consecutive 1 ms epochs; each epoch is one batch
     (sdrg_corr_batch) of a correlator job per channel whose code period
     starts there (L1CA/L5I every ms, E1B every 4 ms). Open-loop trajectories,
     so the epochs' jobs are known in advance; still one batch per epoch, as a
-    receiver closing its loops each epoch would run them."""
+    receiver closing its loops each epoch would run them. With cpu_leg, the
+    reference's own mix + corr_std per job on the host's cores beside."""
     import torch
     from pocketsdr_b200 import synth, track
     rank, world, local = dist_info()
@@ -879,7 +891,7 @@ def run_track(args):
     bufs_d = [torch.from_numpy(b).cuda() for b in wl.bufs]
     lens = [len(b) for b in wl.bufs]
     E = TRACK_EPOCHS_PER_STEP
-    n_ep = (args.warmup + args.steps) * E
+    n_ep = (warmup + steps) * E
     specs_list = []
     for e in range(n_ep):
         sp = wl.jobs_at(e * 1e-3, ptrs)
@@ -899,22 +911,22 @@ def run_track(args):
             track.corr_batch(jobs_list[k * E + i], ptr_b, lens, corr.data_ptr() + 4 * i * per_ep,
                              Cb.data_ptr() + 16 * i * max_j, st.cuda_stream)
 
-    for k in range(args.warmup):
+    for k in range(warmup):
         step(k)
     torch.cuda.synchronize()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(args.steps)]
+          for _ in range(steps)]
     clk = ClockSampler(local)
     clk.start()
-    for k in range(args.steps):
+    for k in range(steps):
         flush.fill_(k & 0xFF)
         ev[k][0].record(st)
-        step(args.warmup + k)
+        step(warmup + k)
         ev[k][1].record(st)
     torch.cuda.synchronize()
     clocks = clk.stop()
     ms = sum(a.elapsed_time(b) for a, b in ev)
-    timed = [specs_list[e] for e in range(args.warmup * E, n_ep)]
+    timed = [specs_list[e] for e in range(warmup * E, n_ep)]
     n_jobs = sum(len(sp) for sp in timed)
     value = n_jobs / (ms / 1e3)
     taps = sum(len(s["pos"]) * s["N"] for sp in timed for s in sp)
@@ -935,17 +947,17 @@ def run_track(args):
     e2e_step(0)
     torch.cuda.synchronize()
     e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-              for _ in range(args.steps)]
-    for k in range(args.steps):
+              for _ in range(steps)]
+    for k in range(steps):
         flush.fill_((k + 1) & 0xFF)
         e2e_ev[k][0].record(st)
-        e2e_step(args.warmup + k)
+        e2e_step(warmup + k)
         e2e_ev[k][1].record(st)
     torch.cuda.synchronize()
     e2e_ms = sum(a.elapsed_time(b) for a, b in e2e_ev)
 
     line = {"metric": TRACK_METRIC, "value": value, "unit": "channel-epochs/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "steps": steps, "warmup": warmup, "ms_per_step": ms / steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8",
             "data": "synthetic",
             "config": {"workload": "track_24mhz", "channels": len(wl.channels),
@@ -954,12 +966,19 @@ def run_track(args):
             "e2e": {"value": n_jobs / (e2e_ms / 1e3), "unit": "channel-epochs/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "tap_samples_per_s": taps / (ms / 1e3), "clocks": clocks,
-            "gpu_launches": 3 * E * args.steps}
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            "gpu_launches": 3 * E * steps}
+    if cpu_leg:
         banks_host = synth.track_banks(wl)
         rate, cores, kind, desc = cpu_track_rate(wl, specs_list, banks_host)
         line["cpu_baseline"] = {"value": rate, "unit": "channel-epochs/s", "cores": cores,
                                 "kind": kind, "sample": desc}
+    return line
+
+
+def run_track(args):
+    rank, world, _ = dist_info()
+    line = track_measure(args, args.steps, args.warmup,
+                         rank == 0 and world == 1 and not args.no_cpu_baseline)
     if rank == 0:
         emit(line)
     return 0
