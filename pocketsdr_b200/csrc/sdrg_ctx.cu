@@ -78,6 +78,15 @@ static void build_ctab(int8_t *ctab)
     }
 }
 
+// The upper bound of the SM identifiers (%nsmid; identifiers need not be
+// contiguous), for buffers indexed by the SM a CTA runs on.
+__global__ void nsmid_kernel(int *out)
+{
+    unsigned n;
+    asm volatile("mov.u32 %0, %%nsmid;" : "=r"(n));
+    *out = (int)n;
+}
+
 int ensure_device(Device **out)
 {
     std::lock_guard<std::mutex> lk(g_dev_mtx);
@@ -102,6 +111,16 @@ int ensure_device(Device **out)
         }
         g_dev.sm_count = prop.multiProcessorCount;
         g_dev.smem_optin = prop.sharedMemPerBlockOptin;
+        g_dev.smem_per_sm = prop.sharedMemPerMultiprocessor;
+        {
+            int *d = nullptr, h = 0;
+            SDRG_CUDA(cudaMalloc(&d, sizeof(int)));
+            nsmid_kernel<<<1, 1>>>(d);
+            SDRG_CUDA(cudaGetLastError());
+            SDRG_CUDA(cudaMemcpy(&h, d, sizeof(int), cudaMemcpyDeviceToHost));
+            SDRG_CUDA(cudaFree(d));
+            g_dev.nsmid = h > 0 ? h : prop.multiProcessorCount;
+        }
         build_ctab(g_dev.ctab);
         SDRG_CUDA(cudaMalloc(&g_dev.ctab_dev, 512));
         SDRG_CUDA(cudaMemcpy(g_dev.ctab_dev, g_dev.ctab, 512, cudaMemcpyHostToDevice));

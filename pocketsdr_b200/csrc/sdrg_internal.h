@@ -32,7 +32,9 @@ int cuda_error(cudaError_t e, const char *what);
 struct Device {
     int id = -1;
     int sm_count = 0;
+    int nsmid = 0;              // upper bound of the SM identifiers (%nsmid)
     size_t smem_optin = 0;      // max dynamic shared memory per block
+    size_t smem_per_sm = 0;     // shared memory of one SM
     int8_t ctab[512];           // quantised carrier (I,Q) for 256 phases
     char2 *ctab_dev = nullptr;  // same table on the device
     cudaMemPool_t pool = nullptr;   // the library's stream-ordered scratch pool

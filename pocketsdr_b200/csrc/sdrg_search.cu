@@ -195,6 +195,9 @@ struct ConsArgs {
     // where each CTA's accesses are consecutive; the last sum writes P
     float *Q;               // or null: every sum reads and writes P
     int Mq;
+    int q_by_sm;            // 1: Q row of the SM the CTA runs on (one consumer CTA
+                            // per SM; the row is the CTA's alone for the task's
+                            // sums), 0: Q row of the task and CTA
     int *stage_err;         // staged splits: error word (a bulk-copy wait ran out)
 };
 
@@ -397,7 +400,12 @@ __device__ __forceinline__ void cons_task(const ConsArgs &a, float2 *sm, const f
             const bool useq = R > 1 && a.Q && a.n_sum > 1;
             const int mode = !useq ? kDirect
                 : (s == 0 ? kQFirst : (s == a.n_sum - 1 ? kQLast : kQMid));
-            float *qrow = useq ? a.Q + ((size_t)task * R + c) * a.Mq : nullptr;
+            float *qrow = nullptr;
+            if (useq) {
+                uint32_t sm = 0;
+                if (a.q_by_sm) asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
+                qrow = a.Q + (a.q_by_sm ? (size_t)sm : (size_t)task * R + c) * a.Mq;
+            }
             StorePower<R> st{row, qrow, c, a.Nmax, mode == kDirect ? (a.accumulate || s > 0)
                                                                   : (a.accumulate != 0), mode};
             if constexpr (SP == 1) fft_inverse_static<Plan24000>(sm, tw, st);
@@ -466,7 +474,7 @@ __global__ void __launch_bounds__(512, 1) cons_kernel(ConsArgs a)
 struct WorkGroup {
     const float2 *split, *X, *code;
     float *P, *Q;
-    int R, n_prn, n_bin, n_sum, Nmax, Mq;
+    int R, n_prn, n_bin, n_sum, Nmax, Mq, q_by_sm;
     size_t prn_stride, bin_stride;
     float scale;
     int task0;              // first task of the group in its queue
@@ -498,6 +506,7 @@ __device__ __forceinline__ ConsArgs work_cons_args(const WorkArgs &a, const Work
     ca.n_prn = G.n_prn; ca.n_bin = G.n_bin; ca.n_sum = G.n_sum; ca.prn0 = 0;
     ca.scale = G.scale; ca.Nmax = G.Nmax; ca.prn_stride = G.prn_stride;
     ca.bin_stride = G.bin_stride; ca.accumulate = 0; ca.P = G.P; ca.Q = G.Q; ca.Mq = G.Mq;
+    ca.q_by_sm = G.q_by_sm;
     return ca;
 }
 
@@ -1249,6 +1258,7 @@ struct GroupState {
     float2 *W = nullptr;                // staged splits: [w_tasks][R][M] sub-spectra
     float *Q = nullptr;                 // cluster splits, several sums: power accumulator
     int Mq = 0;                         // its row length, ceil(Nmax / R)
+    int q_by_sm = 0;                    // Q holds one row per SM (see ConsArgs)
     void *peak_parts = nullptr;         // partial peak reductions
     int w_tasks = 0;
     uint32_t *tab_dev = nullptr;        // phstep | ph0a | ph0b | (int) ix | nsplit
@@ -1606,8 +1616,15 @@ sdrg_acq_plan_t *sdrg_acq_plan_new(const sdrg_acq_sig_t *sigs, int n_sig)
                     cudaMalloc(&G.W, staged_bytes(G.pl, G.w_tasks, 0)) == cudaSuccess);
         if (G.pl->R > 1 && G.pl->R <= 8 && s.n_sum > 1) {
             G.Mq = (s.Nmax + G.pl->R - 1) / G.pl->R;
-            ok = ok && cudaMalloc(&G.Q, (size_t)s.n_prn * s.len_fds * G.pl->R * G.Mq *
-                                            sizeof(float)) == cudaSuccess;
+            // a consumer CTA needs more than half of an SM's shared memory, so
+            // at most one runs on an SM at a time: the power accumulator can
+            // be one row per SM (a few MB that stay in L2) instead of one per
+            // task and CTA (1.1 GB for the E1-B group, whose dirty lines were
+            // written back to HBM after every run)
+            G.q_by_sm = 2 * G.pl->smem > dev->smem_per_sm;
+            const size_t rows = G.q_by_sm ? (size_t)dev->nsmid
+                                          : (size_t)s.n_prn * s.len_fds * G.pl->R;
+            ok = ok && cudaMalloc(&G.Q, rows * G.Mq * sizeof(float)) == cudaSuccess;
         }
         ok = ok && cudaMalloc(&G.peak_parts, peak_scratch_bytes(s.n_prn)) == cudaSuccess;
         G.tab_words = 2 * (size_t)s.len_fds + (size_t)s.len_fds * s.n_sum + 2 * (size_t)s.n_sum + s.len_fds;
@@ -1919,7 +1936,8 @@ static int launch_run_worklist(sdrg_acq_plan_t *plan, Device *dev, const uint8_t
         WorkGroup &W = wa.g[gi];
         W.split = G.pl->split_dev; W.X = G.X; W.code = G.code; W.P = G.P; W.Q = G.Q;
         W.R = G.pl->R; W.n_prn = s.n_prn; W.n_bin = s.len_fds; W.n_sum = s.n_sum;
-        W.Nmax = s.Nmax; W.Mq = G.Mq; W.prn_stride = (size_t)s.len_fds * s.Nmax;
+        W.Nmax = s.Nmax; W.Mq = G.Mq; W.q_by_sm = G.q_by_sm;
+        W.prn_stride = (size_t)s.len_fds * s.Nmax;
         W.bin_stride = s.Nmax; W.scale = 1.0f / s.L / s.L;
         const int q = W.R == 8 ? 0 : 1;
         W.task0 = wa.n_task[q];
@@ -2011,7 +2029,8 @@ static int launch_run(sdrg_acq_plan_t *plan, Device *dev, const uint8_t *const *
         ca.code = G.code; ca.n_prn = s.n_prn; ca.n_bin = nb; ca.n_sum = ns; ca.prn0 = 0;
         ca.scale = 1.0f / s.L / s.L; ca.Nmax = s.Nmax;
         ca.prn_stride = (size_t)nb * s.Nmax; ca.bin_stride = s.Nmax;
-        ca.accumulate = 0; ca.P = G.P; ca.Q = G.Q; ca.Mq = G.Mq; ca.stage_err = plan->stage_err;
+        ca.accumulate = 0; ca.P = G.P; ca.Q = G.Q; ca.Mq = G.Mq; ca.q_by_sm = G.q_by_sm;
+        ca.stage_err = plan->stage_err;
         if ((e = prof_begin(plan, st, ev))) return e;
         if ((e = launch_consumer<0>(G.pl, ca, s.n_prn * nb, st, G.W, G.w_tasks))) return e;
         // a staged split launches a combine and an inverse pass per chunk and sum
