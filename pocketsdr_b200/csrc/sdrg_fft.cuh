@@ -476,18 +476,15 @@ __device__ __forceinline__ void s_inner(float2 *sm, const float2 *twp)
 }
 
 // last inverse pass (radix R, stride S = M / R) handing outputs to store()
-#ifndef SDRG_P0_UNROLL
-#define SDRG_P0_UNROLL 1
-#endif
-#ifndef SDRG_PAIR_MAX
-#define SDRG_PAIR_MAX 10
-#endif
-constexpr int kP0Unroll = SDRG_P0_UNROLL;
+// Largest radix whose warp-private passes take butterflies in pairs (radix
+// 15 in pairs and an unrolled last pass measured slower: 9.64 and 9.73 against
+// 9.84 G cells/s on the multi-GNSS search).
+constexpr int kPairMax = 10;
 template <int R, int S, int NT, class Store>
 __device__ __forceinline__ void s_pass0_store(const float2 *sm, const float2 *twp, Store &store)
 {
     constexpr int IT = (S + NT - 1) / NT;
-#pragma unroll kP0Unroll
+#pragma unroll 1
     for (int it = 0; it < IT; ++it) {
         const int i = threadIdx.x + it * NT;
         if (i < S) {
@@ -585,7 +582,7 @@ __device__ __forceinline__ void s_inner_warp(float2 *sm, const float2 *twp)
         // to 16 keep at least half of the lanes busy.
         constexpr int NBLK = REG / LS, IH = (NBLK + 1) / 2;
         const int i = lane & 15;
-        if constexpr (R <= SDRG_PAIR_MAX) {
+        if constexpr (R <= kPairMax) {
 #pragma unroll
             for (int it = 0; it < IH; it += 2) {
                 const int b0 = 2 * it + (lane >> 4), b1 = b0 + 2;
@@ -601,7 +598,7 @@ __device__ __forceinline__ void s_inner_warp(float2 *sm, const float2 *twp)
             }
         }
     } else {
-        if constexpr (R <= SDRG_PAIR_MAX) {
+        if constexpr (R <= kPairMax) {
 #pragma unroll
             for (int it = 0; it < IT; it += 2) {
                 const int b0 = lane + it * 32, b1 = b0 + 32;

@@ -34,10 +34,9 @@ __device__ __forceinline__ char2 mix_byte(uint8_t byte, uint32_t phase, const ch
 // rotation as two dp2a of the sample bytes with the carrier's 16-bit
 // coefficient pairs, and two 16-byte stores; otherwise sample by sample
 // (mix_byte). HBM bound by design: 1 byte read and 2 bytes written per sample.
-#ifndef SDRG_MIX_VEC
-#define SDRG_MIX_VEC 1
-#endif
-constexpr int kMixVec = SDRG_MIX_VEC;     // 16-byte loads per thread
+// 16-byte loads per thread (two measured slower: 1.09 against 1.45 T
+// samples/s)
+constexpr int kMixVec = 1;
 constexpr int kMixPer = 16 * kMixVec;
 
 // Sign-extended nibbles of four packed samples: the low (I) or high (Q)

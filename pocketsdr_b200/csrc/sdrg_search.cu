@@ -28,10 +28,6 @@
 
 namespace cg = cooperative_groups;
 
-#ifndef SDRG_CONS_U2
-#define SDRG_CONS_U2 4
-#endif
-
 namespace sdrg {
 
 // ---------------------------------------------------------------------------
@@ -337,7 +333,7 @@ __device__ __forceinline__ void cons_task(const ConsArgs &a, float2 *sm, const f
         // in flight per thread: 1 CTA of 16 warps per SM). At R = 8 one
         // position already issues 17 loads, which the L2 prefetch serves:
         // a second one only fills the load queue (measured 2 % slower).
-        constexpr int U = R <= 2 ? SDRG_CONS_U2 : (R <= 6 ? 2 : 1);
+        constexpr int U = R <= 2 ? 4 : (R <= 6 ? 2 : 1);
         const int qstep = U * blockDim.x;
         for (int q = q0 + threadIdx.x; run && q < q1; q += qstep) {
             float2 xs[U][R], cs[U][R], ts[U];
