@@ -638,6 +638,56 @@ class Channel:
         return int(sym[0]), Cc
 
 
+TRACK_SO = os.path.join(HERE, "_ref", "libtrack_ref.so")
+
+
+class _TrackJob(C.Structure):
+    # orc_track_job_t in track_bench.c
+    _fields_ = [("buf", _i), ("ix", _i), ("N", _i), ("npos", _i),
+                ("fs", _d), ("fc", _d), ("phi", _d), ("coff", _d),
+                ("pos", _p), ("code", _p), ("corr", _p)]
+
+
+class TrackRun:
+    """The tracking benchmark's CPU baseline: the reference's own sdr_mix_carr
+    + sdr_corr_std for every job of a list, run from C over a pthread pool
+    (track_bench.c over _ref/libsdr_ref.so), so that no Python runs between
+    the calls. ``jobs``: dicts with buf, ix, N, fs, fc, phi, coff, pos, ch;
+    ``banks``: per channel int8 [10 N, 2] code banks."""
+    kind = "reference"
+
+    def __init__(self, bufs, jobs, banks):
+        self.lib = C.CDLL(TRACK_SO)
+        self.lib.orc_track_run.argtypes = [_p, _p, _i, _i]
+        self.lib.orc_track_run.restype = _i
+        self._keep = [np.ascontiguousarray(b, np.uint8) for b in bufs]
+        self.bufs = (_SdrBuff * len(bufs))(
+            *[_SdrBuff(b.ctypes.data_as(C.POINTER(C.c_uint8)), 2, len(b)) for b in self._keep])
+        self._banks = [np.ascontiguousarray(b, np.int8) for b in banks]
+        self.pos = [np.ascontiguousarray(j["pos"], np.float64) for j in jobs]
+        self.corr = np.zeros((len(jobs), max((len(p) for p in self.pos), default=1)), np.complex64)
+        self.jobs = (_TrackJob * max(len(jobs), 1))()
+        for k, j in enumerate(jobs):
+            t = self.jobs[k]
+            t.buf, t.ix, t.N, t.npos = j["buf"], j["ix"], j["N"], len(self.pos[k])
+            t.fs, t.fc, t.phi, t.coff = j["fs"], j["fc"], j["phi"], j["coff"]
+            t.pos = self.pos[k].ctypes.data
+            t.code = self._banks[j["ch"]].ctypes.data
+            t.corr = self.corr[k].ctypes.data
+        self.n = len(jobs)
+
+    def run(self, threads: int) -> np.ndarray:
+        """Runs every job once; returns the correlations [n_jobs, n_pos]."""
+        if self.lib.orc_track_run(C.cast(self.bufs, _p), C.cast(self.jobs, _p), self.n,
+                                  threads) != 0:
+            raise RuntimeError("track_bench: a thread could not start")
+        return self.corr
+
+
+def track_run_available() -> bool:
+    return os.path.exists(TRACK_SO)
+
+
 def best():
     """The reference build when present, else the restatement."""
     return Reference() if reference_available() else Restatement()

@@ -297,3 +297,22 @@ def test_fine_dop_closed_form_matches_reference_lsq():
         got = _lib.lib.sdr_fine_dop(C.c_void_p(P.ctypes.data), N, C.c_void_p(fds.ctypes.data), M,
                                     C.c_void_p(ix.ctypes.data))
         assert abs(got - want) <= 1e-9 * max(abs(want), 1.0), (b, o, got, want)
+
+
+@pytest.mark.skipif(not oracle.track_run_available(), reason="tracking driver (oracle/_ref) absent")
+def test_track_driver_matches_reference_calls():
+    """The tracking baseline's C driver runs the same reference calls as the
+    Python-level Reference.mix_carr + corr_std, result for result."""
+    from pocketsdr_b200 import synth
+    wl = synth.track_24mhz(seed=5)
+    jobs = wl.jobs_at(0.0, [0] * len(wl.channels))[:24]
+    chans = [c for c in wl.channels if abs(round(0.0 / c.T) * c.T) < 1e-9]
+    for s, c in zip(jobs, chans):
+        s["ch"] = wl.channels.index(c)
+    banks = synth.track_banks(wl)
+    corr = oracle.TrackRun(wl.bufs, jobs, banks).run(4)
+    R = oracle.Reference()
+    for k, s in enumerate(jobs):
+        IQ = R.mix_carr(wl.bufs[s["buf"]], s["ix"], s["N"], s["fs"], s["fc"], s["phi"])
+        c, _ = R.corr_std(IQ, banks[s["ch"]], s["coff"], s["pos"], False)
+        assert np.array_equal(c, corr[k, :len(c)])
