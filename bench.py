@@ -381,8 +381,7 @@ def _reference_other(args):
         elif w == "mix_24mhz":
             buf = np.random.default_rng(8).integers(0, 256, MIX_N, dtype=np.uint8)
             rate, cores, kind, desc = cpu_mix_rate(buf, 24e6, 2.0e6 + 1234.5, 0.3, 64_000_000)
-            metric, unit, cfg = MIX_METRIC, "samples/s", {"workload": w,
-                                                          "samples_per_step": MIX_N}
+            metric, unit, cfg = MIX_METRIC, "samples/s", dict(MIX_CFG)
             per_step = MIX_N
         elif w == "search_batch_24mhz":
             wl = make_workload("acq_multi_24mhz", 2)
@@ -1201,6 +1200,11 @@ def run_refine(args):
 MIX_METRIC = ("carrier wipe-off samples/s (sdr_mix_carr on a device-resident 24 MHz complex "
               "IF buffer: 4 s = 96 M packed samples per step)")
 MIX_N = 96_000_000
+MIX_IX = 12345          # window start: not 16-byte aligned, and the window wraps the buffer end
+MIX_CFG = {"workload": "mix_24mhz", "samples_per_step": MIX_N, "ix": MIX_IX,
+           "window": "starts at an unaligned offset and wraps the circular buffer's end",
+           "l2": "flushed between timed steps (512 MB write outside the events); the 288 MB of "
+                 "traffic per step exceeds L2 anyway"}
 
 
 def cpu_mix_rate(buf, fs, fc, phi, n_samples):
@@ -1245,7 +1249,7 @@ def run_mix(args):
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
 
     def step():
-        if lib.sdrg_mix_carr(C.c_void_p(d_buf.data_ptr()), MIX_N, 0, MIX_N, fs, fc, phi,
+        if lib.sdrg_mix_carr(C.c_void_p(d_buf.data_ptr()), MIX_N, MIX_IX, MIX_N, fs, fc, phi,
                              C.c_void_p(d_out.data_ptr()), C.c_void_p(st.cuda_stream)):
             raise RuntimeError("sdrg_mix_carr failed")
 
@@ -1285,14 +1289,11 @@ def run_mix(args):
     line = {"metric": MIX_METRIC, "value": value, "unit": "samples/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/i8",
-            "data": "synthetic", "config": {"workload": "mix_24mhz", "samples_per_step": MIX_N,
-                                            "l2": "flushed between timed steps (512 MB write "
-                                                  "outside the events); the 288 MB of traffic "
-                                                  "per step exceeds L2 anyway"},
+            "data": "synthetic", "config": dict(MIX_CFG),
             "e2e": {"value": MIX_N / (e2e_ms / 1e3) * world, "unit": "samples/s",
                     "h2d_bytes_per_step": MIX_N, "d2h_bytes_per_step": 2 * MIX_N},
             "gpu_launches": args.steps,
-            "roofline": {"kernel": "mix_kernel (carrier wipe-off, 16 samples per thread)",
+            "roofline": {"kernel": "mix_kernel (carrier wipe-off, one dp2a per sample)",
                          "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
                          "peak_source": ("MEASURED_PEAKS.json" if os.path.exists(

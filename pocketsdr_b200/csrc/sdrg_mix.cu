@@ -28,12 +28,14 @@ __device__ __forceinline__ char2 mix_byte(uint8_t byte, uint32_t phase, const ch
 
 // Window sample n is buf[(ix + n) mod len], its carrier phase
 // n < nsplit ? p0a + n step : p0b + (n - nsplit) step (the restart at the
-// buffer wrap). 16 samples per thread: where its 16 samples lie contiguous and
-// 16-byte aligned in the buffer and the output is 16-byte aligned, one
-// 16-byte load, the nibbles of four samples sign-extended at once, each
-// rotation as two dp2a of the sample bytes with the carrier's 16-bit
-// coefficient pairs, and two 16-byte stores; otherwise sample by sample
-// (mix_byte). HBM bound by design: 1 byte read and 2 bytes written per sample.
+// buffer wrap). 16 samples per thread: where its 16 samples lie contiguous in
+// the buffer (inside one segment of the window) and the output is 16-byte
+// aligned, the one or two aligned 16-byte blocks that hold them, realigned
+// with funnel shifts (any window start), the nibbles of four samples
+// sign-extended at once, each rotation as two dp2a of the sample bytes with
+// the carrier's 16-bit coefficient pairs, and two 16-byte stores; otherwise
+// sample by sample (mix_byte). HBM bound by design: 1 byte read and 2 bytes
+// written per sample.
 // 16-byte loads per thread (two measured slower: 1.09 against 1.45 T
 // samples/s)
 constexpr int kMixVec = 1;
@@ -50,6 +52,33 @@ __device__ __forceinline__ uint32_t nibbles_i(uint32_t w)
 __device__ __forceinline__ uint32_t nibbles_q(uint32_t w)
 {
     return nibbles_i(w >> 4);
+}
+
+// bytes s .. s + 15 of the 32 bytes lo:hi (s in 0..15)
+__device__ __forceinline__ uint4 realign16(uint4 lo, uint4 hi, int s)
+{
+    const uint32_t sh = 8u * (uint32_t)(s & 3);
+    const uint32_t w[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+    uint4 r;
+    switch (s >> 2) {
+    case 0:
+        r = make_uint4(__funnelshift_r(w[0], w[1], sh), __funnelshift_r(w[1], w[2], sh),
+                       __funnelshift_r(w[2], w[3], sh), __funnelshift_r(w[3], w[4], sh));
+        break;
+    case 1:
+        r = make_uint4(__funnelshift_r(w[1], w[2], sh), __funnelshift_r(w[2], w[3], sh),
+                       __funnelshift_r(w[3], w[4], sh), __funnelshift_r(w[4], w[5], sh));
+        break;
+    case 2:
+        r = make_uint4(__funnelshift_r(w[2], w[3], sh), __funnelshift_r(w[3], w[4], sh),
+                       __funnelshift_r(w[4], w[5], sh), __funnelshift_r(w[5], w[6], sh));
+        break;
+    default:
+        r = make_uint4(__funnelshift_r(w[3], w[4], sh), __funnelshift_r(w[4], w[5], sh),
+                       __funnelshift_r(w[5], w[6], sh), __funnelshift_r(w[6], w[7], sh));
+        break;
+    }
+    return r;
 }
 
 __global__ void __launch_bounds__(256) mix_kernel(
@@ -72,13 +101,25 @@ __global__ void __launch_bounds__(256) mix_kernel(
     const int n0 = (int)n0l;
     int pos0 = ix + n0;
     if (pos0 >= len) pos0 -= len;
-    const bool fast = n0 + kMixPer <= N && pos0 + kMixPer <= len &&
+    // the aligned block holding the first sample's byte starts s bytes before
+    // it; the second block is needed when s > 0
+    const int s = (int)(((uintptr_t)buf + (uintptr_t)pos0) & 15u), a0 = pos0 - s;
+    const bool fast = n0 + kMixPer <= N && pos0 + kMixPer <= len && a0 >= 0 &&
+                      (s == 0 || a0 + 16 * kMixVec + 16 <= len) &&
                       (n0 + kMixPer <= nsplit || n0 >= nsplit) &&
-                      ((((uintptr_t)(buf + pos0)) | ((uintptr_t)(out + n0))) & 15u) == 0;
+                      (((uintptr_t)(out + n0)) & 15u) == 0;
     if (fast) {
         uint4 w[kMixVec];
+        if (s == 0) {
 #pragma unroll
-        for (int v = 0; v < kMixVec; ++v) w[v] = *(const uint4 *)(buf + pos0 + 16 * v);
+            for (int v = 0; v < kMixVec; ++v) w[v] = *(const uint4 *)(buf + a0 + 16 * v);
+        } else {
+            uint4 b[kMixVec + 1];
+#pragma unroll
+            for (int v = 0; v <= kMixVec; ++v) b[v] = *(const uint4 *)(buf + a0 + 16 * v);
+#pragma unroll
+            for (int v = 0; v < kMixVec; ++v) w[v] = realign16(b[v], b[v + 1], s);
+        }
         uint32_t ph = n0 < nsplit ? p0a + step * (uint32_t)n0 : p0b + step * (uint32_t)(n0 - nsplit);
 #pragma unroll
         for (int v = 0; v < kMixVec; ++v) {

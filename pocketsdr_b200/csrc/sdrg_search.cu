@@ -167,6 +167,26 @@ __global__ void __launch_bounds__(512, 1) fwd_multi_kernel(FwdMulti m)
     fwd_block<0, 1>(a, (int)blockIdx.x - m.blk0[g], smem, tw, (char2 *)(tw + Plan24000::TWTOT));
 }
 
+// In-place split combine of a group's forward sub-spectra: for every (bin,
+// sum) bs and position q, X[bs][r][q] = F_r[q] (r < R) becomes
+// X[bs][j][q] = X(k(q) + j M) (j < R), the spectrum the consumers multiply by
+// each PRN's code. The same arithmetic as the consumer's own combine
+// (split_combine_fwd), done once per bin and sum instead of once per PRN.
+template <int R>
+__global__ void __launch_bounds__(256) xcomb_kernel(float2 *X, const float2 *__restrict__ split,
+                                                    int M)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= M) return;
+    float2 *x = X + (size_t)blockIdx.y * R * M + q;
+    float2 g[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) g[r] = x[(size_t)r * M];
+    split_combine_fwd<R>(g, __ldg(split + q));
+#pragma unroll
+    for (int j = 0; j < R; ++j) x[(size_t)j * M] = g[j];
+}
+
 // ---------------------------------------------------------------------------
 // consumer kernel
 // ---------------------------------------------------------------------------
@@ -195,6 +215,8 @@ struct ConsArgs {
                             // per SM; the row is the CTA's alone for the task's
                             // sums), 0: Q row of the task and CTA
     int *stage_err;         // staged splits: error word (a bulk-copy wait ran out)
+    int x_comb;             // 1: X holds the combined spectrum, X[bs][j][q] = X(k(q) + j M)
+                            // (xcomb_kernel ran); 0: the sub-spectra F_r
 };
 
 // Power store of one sum. kDirect: P = (add ? P : 0) + |y|^2. With the
@@ -307,6 +329,29 @@ struct PairSync {
     }
 };
 
+// One position of the consumer's combine: g[r] = the sub-spectra F_r(k)
+// (x_comb 0) or the spectrum X(k + r M) (x_comb 1), cs[j] the code at
+// k + j M, t = exp(+2 pi i k / L); leaves g[j] = the input of CTA j's
+// inverse transform at this position.
+template <int R>
+__device__ __forceinline__ void combine_point(float2 *g, const float2 *cs, float2 t, int x_comb,
+                                              float scale)
+{
+    if (!x_comb) split_combine_fwd<R>(g, t);   // X[k + jM]
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+        const float2 z = cmul(g[j], cs[j]);
+        g[j] = make_float2(z.x * scale, z.y * scale);
+    }
+    Dft<R, 1>::run(g);                         // sum_j Z e^{+2 pi i c j/R}
+    float2 w = t;
+#pragma unroll
+    for (int j = 1; j < R; ++j) {
+        g[j] = cmul(g[j], w);
+        if (j + 1 < R) w = cmul(w, t);
+    }
+}
+
 // The sums of one consumer task (PRN prn, bin b; this CTA's share c of its
 // R-way split): per sum, combine + code product into the split's shared
 // memory (dst[j]: CTA j of the task), barrier, inverse transform and power
@@ -359,27 +404,7 @@ __device__ __forceinline__ void cons_task(const ConsArgs &a, float2 *sm, const f
                     const float2 z = cmul(g[0], cs[u][0]);
                     dst[0][qq] = make_float2(z.x * a.scale, z.y * a.scale);
                 } else {
-                    const float2 t = ts[u];
-                    const float2 tc = cconj(t);
-                    float2 w = tc;
-#pragma unroll
-                    for (int r = 1; r < R; ++r) {
-                        g[r] = cmul(g[r], w);
-                        if (r + 1 < R) w = cmul(w, tc);
-                    }
-                    Dft<R, -1>::run(g);                 // X[k + jM]
-#pragma unroll
-                    for (int j = 0; j < R; ++j) {
-                        const float2 z = cmul(g[j], cs[u][j]);
-                        g[j] = make_float2(z.x * a.scale, z.y * a.scale);
-                    }
-                    Dft<R, 1>::run(g);                  // sum_j Z e^{+2 pi i c j/R}
-                    w = t;
-#pragma unroll
-                    for (int j = 1; j < R; ++j) {
-                        g[j] = cmul(g[j], w);
-                        if (j + 1 < R) w = cmul(w, t);
-                    }
+                    combine_point<R>(g, cs[u], ts[u], a.x_comb, a.scale);
 #pragma unroll
                     for (int j = 0; j < R; ++j) dst[j][qq] = g[j];
                 }
@@ -474,6 +499,7 @@ struct WorkGroup {
     size_t prn_stride, bin_stride;
     float scale;
     int task0;              // first task of the group in its queue
+    int x_comb;             // X holds the combined spectrum (ConsArgs::x_comb)
 };
 
 struct WorkArgs {
@@ -502,7 +528,7 @@ __device__ __forceinline__ ConsArgs work_cons_args(const WorkArgs &a, const Work
     ca.n_prn = G.n_prn; ca.n_bin = G.n_bin; ca.n_sum = G.n_sum; ca.prn0 = 0;
     ca.scale = G.scale; ca.Nmax = G.Nmax; ca.prn_stride = G.prn_stride;
     ca.bin_stride = G.bin_stride; ca.accumulate = 0; ca.P = G.P; ca.Q = G.Q; ca.Mq = G.Mq;
-    ca.q_by_sm = G.q_by_sm;
+    ca.q_by_sm = G.q_by_sm; ca.x_comb = G.x_comb;
     return ca;
 }
 
@@ -872,6 +898,27 @@ static int launch_fwd(const FftPlan *pl, const FwdArgs &a, int n_blocks, cudaStr
     if (sp) fwd_kernel<MODE, 1><<<n_blocks, pl->threads, pl->smem, st>>>(a);
     else fwd_kernel<MODE, 0><<<n_blocks, pl->threads, pl->smem, st>>>(a);
     SDRG_CUDA(cudaGetLastError());
+    return SDRG_OK;
+}
+
+// Combines the sub-spectra of n_bs (bin, sum) blocks in place; returns 1 in
+// *done when it ran (splits 2..8), 0 otherwise (no split, or a staged one).
+static int launch_xcomb(const FftPlan *pl, float2 *X, int n_bs, cudaStream_t st, int *done)
+{
+    *done = 0;
+    if (pl->R < 2 || pl->R > 8 || n_bs <= 0) return SDRG_OK;
+    const dim3 g((unsigned)((pl->M + 255) / 256), (unsigned)n_bs);
+    switch (pl->R) {
+    case 2: xcomb_kernel<2><<<g, 256, 0, st>>>(X, pl->split_dev, pl->M); break;
+    case 3: xcomb_kernel<3><<<g, 256, 0, st>>>(X, pl->split_dev, pl->M); break;
+    case 4: xcomb_kernel<4><<<g, 256, 0, st>>>(X, pl->split_dev, pl->M); break;
+    case 5: xcomb_kernel<5><<<g, 256, 0, st>>>(X, pl->split_dev, pl->M); break;
+    case 6: xcomb_kernel<6><<<g, 256, 0, st>>>(X, pl->split_dev, pl->M); break;
+    case 8: xcomb_kernel<8><<<g, 256, 0, st>>>(X, pl->split_dev, pl->M); break;
+    default: return SDRG_OK;
+    }
+    SDRG_CUDA(cudaGetLastError());
+    *done = 1;
     return SDRG_OK;
 }
 
@@ -1943,7 +1990,14 @@ static int launch_run_worklist(sdrg_acq_plan_t *plan, Device *dev, const uint8_t
     if ((e = prof_begin(plan, caller, ev))) return e;
     fwd_multi_kernel<<<fm.blk0[ng], pl0->threads, pl0->smem, caller>>>(fm);
     SDRG_CUDA(cudaGetLastError());
-    if ((e = prof_end(plan, caller, ev, 0))) return e;
+    int n_fwd = 1;
+    for (int gi = 0; gi < ng; ++gi) {
+        GroupState &G = plan->g[gi];
+        if ((e = launch_xcomb(G.pl, G.X, G.sig.len_fds * G.sig.n_sum, caller, &wa.g[gi].x_comb)))
+            return e;
+        n_fwd += wa.g[gi].x_comb;
+    }
+    if ((e = prof_end(plan, caller, ev, 0, n_fwd))) return e;
 
     if ((e = prof_begin(plan, caller, ev))) return e;
     SDRG_CUDA(cudaMemsetAsync(plan->wl_next, 0, 2 * sizeof(int), caller));
@@ -2019,8 +2073,11 @@ static int launch_run(sdrg_acq_plan_t *plan, Device *dev, const uint8_t *const *
         cudaEvent_t ev[2];
         if ((e = prof_begin(plan, st, ev))) return e;
         if ((e = launch_fwd<0>(G.pl, fa, nb * ns * G.pl->R, st))) return e;
-        if ((e = prof_end(plan, st, ev, 3 * (int)gi + 0))) return e;
+        int xc = 0;
+        if ((e = launch_xcomb(G.pl, G.X, nb * ns, st, &xc))) return e;
+        if ((e = prof_end(plan, st, ev, 3 * (int)gi + 0, 1 + xc))) return e;
         ConsArgs ca = {};
+        ca.x_comb = xc;
         ca.pl = G.pl->k; ca.tw = G.pl->tw_dev; ca.split = G.pl->split_dev; ca.X = G.X;
         ca.code = G.code; ca.n_prn = s.n_prn; ca.n_bin = nb; ca.n_sum = ns; ca.prn0 = 0;
         ca.scale = 1.0f / s.L / s.L; ca.Nmax = s.Nmax;

@@ -29,6 +29,28 @@ def test_mix_carr_device_matches_reference(ref, gpu, len_buf, ix, N):
     assert np.array_equal(got, want)
 
 
+def test_mix_carr_device_every_alignment(ref, gpu):
+    """Every offset of the window start within a 16-byte block, with the
+    buffer itself starting at each of 4 byte offsets from an aligned address
+    (the kernel realigns 16-byte blocks), windows wrapping the buffer end."""
+    import torch
+    from pocketsdr_b200._lib import lib, torch_stream
+    rng = np.random.default_rng(77)
+    len_buf, N = 4099, 4000
+    for off in range(4):
+        buf = rng.integers(0, 256, len_buf, dtype=np.uint8)
+        d_all = torch.from_numpy(np.concatenate([np.zeros(off, np.uint8), buf])).cuda()
+        for ix in list(range(0, 33)) + [len_buf - 40, len_buf - 1]:
+            fs, fc, phi = 24e6, float(rng.uniform(-6e6, 6e6)), float(rng.uniform(-1.0, 1.0))
+            want = ref.mix_carr(buf, ix, N, fs, fc, phi)
+            d_out = torch.zeros(2 * N, dtype=torch.int8, device="cuda")
+            st = lib.sdrg_mix_carr(C.c_void_p(d_all.data_ptr() + off), len_buf, ix, N, fs, fc,
+                                   phi, C.c_void_p(d_out.data_ptr()), C.c_void_p(torch_stream()))
+            assert st == 0
+            got = d_out.cpu().numpy().reshape(N, 2)
+            assert np.array_equal(got, want), (off, ix)
+
+
 def test_mix_carr_device_rejects_bad_window(gpu):
     from pocketsdr_b200._lib import lib, last_error
     p = C.c_void_p(1)

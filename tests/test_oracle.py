@@ -316,3 +316,4 @@ def test_track_driver_matches_reference_calls():
         IQ = R.mix_carr(wl.bufs[s["buf"]], s["ix"], s["N"], s["fs"], s["fc"], s["phi"])
         c, _ = R.corr_std(IQ, banks[s["ch"]], s["coff"], s["pos"], False)
         assert np.array_equal(c, corr[k, :len(c)])
+
