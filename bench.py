@@ -586,9 +586,9 @@ def acq_measure(args, name: str, steps: int, warmup: int, dist, rank: int, world
         **_fp32_roofline(achieved),
         "flops_per_step": flops_step,
         "traffic": traffic,
-        "traffic_source": ("ncu dram bytes read + written per consumer launch, from a capture of "
-                           "a smaller case scaled to a full launch (profiles/cons_kernel_traffic.txt)"
-                           if traffic else None),
+        "traffic_source": ("ncu dram bytes read + written per consumer launch, measured on the "
+                           "full workload and averaged over the consumer launches of one step "
+                           "(profiles/cons_kernel_traffic.txt)" if traffic else None),
         "time_basis": "span of the concurrent consumer launches per step (CUDA events)",
         "span_ms_per_step": cons_ms / steps,
         "launches": cons_n,
