@@ -279,6 +279,14 @@ static bool shape_for_R(int L, int R, int *Mout, FftPlanK *kout)
             best.r[j] = best.r[j - 1];
             best.r[j - 1] = t;
         }
+    if (M == Plan12000::M) {
+        // the compile-time 12 000-point plan's passes (first radix = its 8
+        // warps, then the 1500-point warp blocks of 10 x 10 x 15), so that
+        // its tables serve that plan
+        best.n = 4;
+        best.r[0] = Plan12000::R0; best.r[1] = Plan12000::R1;
+        best.r[2] = Plan12000::R2; best.r[3] = Plan12000::R3;
+    }
     FftPlanK k{};
     k.M = M;
     k.npass = best.n;

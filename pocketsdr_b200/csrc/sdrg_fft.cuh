@@ -420,16 +420,24 @@ __device__ void fft_inverse(float2 *sm, const float2 *tw, const FftPlanK &pl,
 // ---- compile-time plans -------------------------------------------------------
 // A 4-pass plan fixed at compile time: every stride, table offset, loop trip
 // count and divisor is a constant, so shared-memory addresses take immediate
-// offsets and the butterfly loops unroll. The table layout is the runtime
-// plan's (pass 0: S0 entries; pass p >= 1: S_p * (r_p - 1) entries), so a
-// matching runtime plan's tables serve it unchanged.
-template <int M_, int NT_, int R0_, int R1_, int R2_, int R3_>
+// offsets and the butterfly loops unroll. The global table layout is the
+// runtime plan's (pass 0: S0 entries; pass p >= 1: S_p * (r_p - 1) entries),
+// so a matching runtime plan's tables serve it unchanged. Its passes read one
+// twiddle per butterfly (the first S_p entries of each pass's table) and form
+// the powers in registers, so with COMPACT the shared-memory copy holds only
+// those (T_p: offsets in shared memory, TWS entries; load_twiddles_static):
+// S0 + S1 + S2 entries instead of TWTOT, which lets two 12 000-point CTAs
+// share an SM.
+template <int M_, int NT_, int R0_, int R1_, int R2_, int R3_, bool COMPACT = false>
 struct StaticPlan4 {
     static constexpr int M = M_, NT = NT_;
     static constexpr int R0 = R0_, R1 = R1_, R2 = R2_, R3 = R3_;
     static constexpr int S0 = M / R0, S1 = S0 / R1, S2 = S1 / R2, S3 = S2 / R3;
     static constexpr int O0 = 0, O1 = S0, O2 = O1 + S1 * (R1 - 1), O3 = O2 + S2 * (R2 - 1);
     static constexpr int TWTOT = O3 + S3 * (R3 - 1);
+    static constexpr int T0 = 0, T1 = COMPACT ? S0 : O1, T2 = COMPACT ? S0 + S1 : O2,
+                         T3 = COMPACT ? S0 + S1 + S2 : O3;
+    static constexpr int TWS = COMPACT ? S0 + S1 + S2 : TWTOT;
     static_assert(S3 == 1 && R0 * R1 * R2 * R3 == M, "plan must cover M");
     static bool matches(const FftPlanK &k, int threads)
     {
@@ -441,6 +449,10 @@ struct StaticPlan4 {
 // The plan of every 24 000-point sub-transform (L = 24 000 x {1, 2, 8}: the
 // 12 and 24 MHz searches of 1 ms and 4 ms codes).
 using Plan24000 = StaticPlan4<24000, 512, 16, 10, 10, 15>;
+// 12 000-point sub-transforms of a 4-way split (L = 48 000), two CTAs of 8
+// warps per SM: the same 1500-point warp blocks (10 x 10 x 15) after a first
+// radix of 8, compact twiddles.
+using Plan12000 = StaticPlan4<12000, 256, 8, 10, 10, 15, true>;
 
 // inner pass with compile-time radix R, stride S (sub-length R*S)
 template <int R, int S, int M, int NT, bool FWD>
@@ -630,13 +642,13 @@ __device__ __forceinline__ void fft_forward_static(float2 *sm, const float2 *tw,
 {
     static_assert(P::R0 * 32 == P::NT, "one warp per block after the first pass");
     constexpr int REG = P::M / P::R0;
-    dif_pass0_load<P::R0>(sm, P::M, tw + P::O0, load, threadIdx.x, P::NT);
+    dif_pass0_load<P::R0>(sm, P::M, tw + P::T0, load, threadIdx.x, P::NT);
     __syncthreads();
-    s_inner_warp<P::R1, P::S1, REG, true>(sm, tw + P::O1);
+    s_inner_warp<P::R1, P::S1, REG, true>(sm, tw + P::T1);
     __syncwarp();
-    s_inner_warp<P::R2, P::S2, REG, true>(sm, tw + P::O2);
+    s_inner_warp<P::R2, P::S2, REG, true>(sm, tw + P::T2);
     __syncwarp();
-    s_inner_warp<P::R3, P::S3, REG, true>(sm, tw + P::O3);
+    s_inner_warp<P::R3, P::S3, REG, true>(sm, tw + P::T3);
     __syncthreads();
 }
 
@@ -648,13 +660,14 @@ __device__ __forceinline__ void fft_inverse_static(float2 *sm, const float2 *tw,
 {
     if constexpr (P::R0 * 32 == P::NT) {
         constexpr int REG = P::M / P::R0;
-        s_inner_warp<P::R3, P::S3, REG>(sm, tw + P::O3);
+        s_inner_warp<P::R3, P::S3, REG>(sm, tw + P::T3);
         __syncwarp();
-        s_inner_warp<P::R2, P::S2, REG>(sm, tw + P::O2);
+        s_inner_warp<P::R2, P::S2, REG>(sm, tw + P::T2);
         __syncwarp();
-        s_inner_warp<P::R1, P::S1, REG>(sm, tw + P::O1);
+        s_inner_warp<P::R1, P::S1, REG>(sm, tw + P::T1);
         __syncthreads();
     } else {
+        static_assert(P::TWS == P::TWTOT, "CTA-wide passes read the full tables");
         s_inner<P::R3, P::S3, P::M, P::NT, false>(sm, tw + P::O3);
         __syncthreads();
         s_inner<P::R2, P::S2, P::M, P::NT, false>(sm, tw + P::O2);
@@ -662,7 +675,7 @@ __device__ __forceinline__ void fft_inverse_static(float2 *sm, const float2 *tw,
         s_inner<P::R1, P::S1, P::M, P::NT, false>(sm, tw + P::O1);
         __syncthreads();
     }
-    s_pass0_store<P::R0, P::S0, P::NT>(sm, tw + P::O0, store);
+    s_pass0_store<P::R0, P::S0, P::NT>(sm, tw + P::T0, store);
 }
 
 // Split combine of a length-L = R*M forward transform computed as R
@@ -702,6 +715,23 @@ __device__ __forceinline__ void load_twiddles(float2 *tw_sm, const float2 *tw_g,
         for (int u = 0; u < UL; ++u) {
             const int i = i0 + u * blockDim.x;
             if (i < n) tw_sm[i] = v[u];
+        }
+    }
+}
+
+// The shared-memory twiddles of a compile-time plan: the whole table, or
+// with P's COMPACT layout the first S_p entries of passes 0..2 (pass 3 has
+// stride 1 and no twiddles).
+template <class P>
+__device__ __forceinline__ void load_twiddles_static(float2 *tw_sm, const float2 *tw_g)
+{
+    if constexpr (P::TWS == P::TWTOT) {
+        load_twiddles(tw_sm, tw_g, P::TWTOT);
+    } else {
+        for (int i = threadIdx.x; i < P::TWS; i += blockDim.x) {
+            const int g = i < P::T1 ? P::O0 + i : (i < P::T2 ? P::O1 + (i - P::T1)
+                                                             : P::O2 + (i - P::T2));
+            tw_sm[i] = __ldg(tw_g + g);
         }
     }
 }

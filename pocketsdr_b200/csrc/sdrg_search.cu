@@ -280,6 +280,11 @@ __device__ __forceinline__ void prefetch_l2(const float2 *p, int n)
 // clear, and goes on.
 constexpr long long kBulkWaitCycles = 4000000000LL;     // about 2 s at 1.97 GHz
 
+// The compile-time plan of a consumer instantiation: SP 1 the 24 000-point
+// plan, SP 2 the 12 000-point one (two CTAs per SM), SP 0 none (runtime plan).
+template <int SP> struct PlanOf { using P = Plan24000; };
+template <> struct PlanOf<2> { using P = Plan12000; };
+
 // ---- synchronisation of the CTAs that share a task --------------------------
 struct CtaSync {
     __device__ __forceinline__ void operator()() const { __syncthreads(); }
@@ -364,7 +369,7 @@ __device__ __forceinline__ void cons_task(const ConsArgs &a, float2 *sm, const f
                                           float2 *const *dst, int c, int task, int prn, int b,
                                           int ns_run, bool active, const Sync &sync)
 {
-    const int M = SP ? Plan24000::M : a.pl.M;   // SP: compile-time plan
+    const int M = SP ? PlanOf<SP>::P::M : a.pl.M;   // SP: compile-time plan
     const int Mc = (M + R - 1) / R;
     const int q0 = c * Mc, q1 = min(M, q0 + Mc);
     const float2 *code = a.code + (size_t)(a.code_per_bin ? b : prn) * R * M;
@@ -429,12 +434,12 @@ __device__ __forceinline__ void cons_task(const ConsArgs &a, float2 *sm, const f
             }
             StorePower<R> st{row, qrow, c, a.Nmax, mode == kDirect ? (a.accumulate || s > 0)
                                                                   : (a.accumulate != 0), mode};
-            if constexpr (SP == 1) fft_inverse_static<Plan24000>(sm, tw, st);
+            if constexpr (SP != 0) fft_inverse_static<typename PlanOf<SP>::P>(sm, tw, st);
             else fft_inverse(sm, tw, a.pl, st);
         } else {
             float2 *row = a.Y + (size_t)b * (size_t)R * M;
             StoreComplex<R> st{row, c};
-            if constexpr (SP == 1) fft_inverse_static<Plan24000>(sm, tw, st);
+            if constexpr (SP != 0) fft_inverse_static<typename PlanOf<SP>::P>(sm, tw, st);
             else fft_inverse(sm, tw, a.pl, st);
         }
     }
@@ -446,7 +451,7 @@ __global__ void __launch_bounds__(512, 1) cons_kernel(ConsArgs a)
     extern __shared__ float2 smem[];
     float2 *sm = smem;
     float2 *tw = smem + a.pl.M;
-    const int M = SP ? Plan24000::M : a.pl.M;   // SP: compile-time plan
+    const int M = SP ? PlanOf<SP>::P::M : a.pl.M;   // SP: compile-time plan
     const int c = (R > 1) ? (int)(blockIdx.x % R) : 0;
     // bin-major tasks: the PRNs of one Doppler bin run side by side, so the
     // bin's forward spectra are fetched from HBM once and then hit in L2
@@ -465,7 +470,8 @@ __global__ void __launch_bounds__(512, 1) cons_kernel(ConsArgs a)
         prefetch_l2(code + (size_t)threadIdx.x * M + q0, q1 - q0);
     }
 
-    load_twiddles(tw, a.tw, a.pl.twtot);
+    if constexpr (SP != 0) load_twiddles_static<typename PlanOf<SP>::P>(tw, a.tw);
+    else load_twiddles(tw, a.tw, a.pl.twtot);
 
     float2 *dst[R];
     if constexpr (R > 1) {
@@ -901,6 +907,16 @@ static int launch_fwd(const FftPlan *pl, const FwdArgs &a, int n_blocks, cudaStr
     return SDRG_OK;
 }
 
+// Dynamic shared memory of a consumer launch: the transform and its twiddles
+// (the compact twiddles of the 12 000-point compile-time plan, whose CTAs
+// then fit two per SM).
+static size_t cons_smem(const FftPlan *pl)
+{
+    if (pl->R == 4 && Plan12000::matches(pl->k, pl->threads))
+        return (size_t)(Plan12000::M + Plan12000::TWS) * sizeof(float2);
+    return pl->smem;
+}
+
 // Combines the sub-spectra of n_bs (bin, sum) blocks in place; returns 1 in
 // *done when it ran (splits 2..8), 0 otherwise (no split, or a staged one).
 static int launch_xcomb(const FftPlan *pl, float2 *X, int n_bs, cudaStream_t st, int *done)
@@ -939,7 +955,7 @@ static int launch_cons_RS(const FftPlan *pl, const ConsArgs &a, int n_tasks, cud
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(n_tasks * R));
     cfg.blockDim = dim3(pl->threads);
-    cfg.dynamicSmemBytes = pl->smem;
+    cfg.dynamicSmemBytes = cons_smem(pl);
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -953,13 +969,17 @@ static int launch_cons_RS(const FftPlan *pl, const ConsArgs &a, int n_tasks, cud
 }
 
 // the compile-time 24 000-point plan where it applies (R = 1, 2, 8), the
-// runtime plan otherwise
+// 12 000-point one for 4-way splits, the runtime plan otherwise
 template <int R, int MODE>
 static int launch_cons_R(const FftPlan *pl, const ConsArgs &a, int n_tasks, cudaStream_t st)
 {
     if constexpr (R == 1 || R == 2 || R == 8) {
         if (Plan24000::matches(pl->k, pl->threads))
             return launch_cons_RS<R, MODE, 1>(pl, a, n_tasks, st);
+    }
+    if constexpr (R == 4) {
+        if (Plan12000::matches(pl->k, pl->threads))
+            return launch_cons_RS<R, MODE, 2>(pl, a, n_tasks, st);
     }
     return launch_cons_RS<R, MODE, 0>(pl, a, n_tasks, st);
 }
@@ -1664,7 +1684,7 @@ sdrg_acq_plan_t *sdrg_acq_plan_new(const sdrg_acq_sig_t *sigs, int n_sig)
             // be one row per SM (a few MB that stay in L2) instead of one per
             // task and CTA (1.1 GB for the E1-B group, whose dirty lines were
             // written back to HBM after every run)
-            G.q_by_sm = 2 * G.pl->smem > dev->smem_per_sm;
+            G.q_by_sm = 2 * (cons_smem(G.pl) + 1024) > dev->smem_per_sm;
             const size_t rows = G.q_by_sm ? (size_t)dev->nsmid
                                           : (size_t)s.n_prn * s.len_fds * G.pl->R;
             ok = ok && cudaMalloc(&G.Q, rows * G.Mq * sizeof(float)) == cudaSuccess;
