@@ -451,14 +451,14 @@ __device__ __forceinline__ void sgn_dot4(int &s, uint32_t x, uint32_t c)
 {
     const uint32_t u = (c & 0x7f7f7f7fu) + 0x7f7f7f7fu;        // bit 7: c's low 7 bits != 0
     const uint32_t pos = ((u & ~c) & 0x80808080u) >> 7;        // 1 in lanes with c > 0
-    const uint32_t neg = (c & 0x80808080u) >> 7;               // 1 in lanes with c < 0
-    s = __dp4a((int)x, (int)pos, s);
-    s -= __dp4a((int)x, (int)neg, 0);
+    uint32_t negm;                                              // -1 in lanes with c < 0
+    asm("prmt.b32 %0, %1, 0, 0xBA98;" : "=r"(negm) : "r"(c));  // each byte's sign replicated
+    s = __dp4a((int)x, (int)(pos | negm), s);                   // x * sgn(c), four lanes
     if (FIX) {
         const uint32_t t = x ^ 0x80808080u;                    // 0 in lanes with x = -128
         const uint32_t v = (t & 0x7f7f7f7fu) + 0x7f7f7f7fu;
         const uint32_t m = (~(v | t) & 0x80808080u) >> 7;      // 1 in lanes with x = -128
-        s -= 256 * __dp4a((int)m, (int)neg, 0);
+        s += 256 * __dp4a((int)m, (int)negm, 0);               // minus 256 per such lane
     }
 }
 
