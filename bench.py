@@ -351,6 +351,8 @@ def _reference_other(args):
                 "refinement after its grid search (its finest estimate is sdr_fine_dop); "
                 "refine_12mhz's cpu_baseline times the reference grid plus the FP64 oracle"}
     vals, desc, cores, kind, metric, unit, cfg = [], "", 0, "", "", "", {}
+    # the arithmetic type of each workload's GPU arm, named the same here
+    dtype = {"track_24mhz": "int8", "mix_24mhz": "u8/i8"}.get(w, "f32")
     for k in range(args.warmup + args.steps):
         if w == "track_24mhz":
             from pocketsdr_b200 import synth
@@ -398,7 +400,7 @@ def _reference_other(args):
     v = statistics.median(vals)
     return {"metric": metric, "value": v, "unit": unit, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": per_step / v * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic",
             "config": cfg, "impl": "reference",
             "cpu_baseline": {"value": v, "unit": unit, "cores": cores, "kind": kind, "sample": desc},
             "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
