@@ -51,6 +51,25 @@ def test_mix_carr_device_every_alignment(ref, gpu):
             assert np.array_equal(got, want), (off, ix)
 
 
+def test_mix_carr_device_unaligned_output(ref, gpu):
+    """An output array that does not start on a 16-byte boundary takes the
+    sample-by-sample path; the result is the same."""
+    import torch
+    from pocketsdr_b200._lib import lib, torch_stream
+    rng = np.random.default_rng(91)
+    len_buf, ix, N = 50000, 333, 40000
+    buf = rng.integers(0, 256, len_buf, dtype=np.uint8)
+    want = ref.mix_carr(buf, ix, N, 24e6, 3.1e6, 0.7)
+    d_buf = torch.from_numpy(buf).cuda()
+    d_out = torch.zeros(2 * N + 16, dtype=torch.int8, device="cuda")
+    for off in (2, 6):
+        st = lib.sdrg_mix_carr(C.c_void_p(d_buf.data_ptr()), len_buf, ix, N, 24e6, 3.1e6, 0.7,
+                               C.c_void_p(d_out.data_ptr() + off), C.c_void_p(torch_stream()))
+        assert st == 0
+        got = d_out.cpu().numpy()[off:off + 2 * N].reshape(N, 2)
+        assert np.array_equal(got, want), off
+
+
 def test_mix_carr_device_rejects_bad_window(gpu):
     from pocketsdr_b200._lib import lib, last_error
     p = C.c_void_p(1)
