@@ -286,11 +286,26 @@ template <int SP> struct PlanOf { using P = Plan24000; };
 template <> struct PlanOf<2> { using P = Plan12000; };
 
 // ---- synchronisation of the CTAs that share a task --------------------------
+// A Sync type is a barrier over the CTAs of a task, called whole, or split
+// into arrive() (by every thread, at the same point) and wait() (by every
+// thread, anywhere before it touches what the barrier protects).
 struct CtaSync {
     __device__ __forceinline__ void operator()() const { __syncthreads(); }
+    __device__ __forceinline__ void arrive() const { __syncthreads(); }
+    __device__ __forceinline__ void wait() const {}
 };
 struct ClusterSync {
     __device__ __forceinline__ void operator()() const { cg::this_cluster().sync(); }
+    // split cluster barrier; the unaligned forms, since threads reach wait()
+    // at different points of the combine loop
+    __device__ __forceinline__ void arrive() const
+    {
+        asm volatile("barrier.cluster.arrive.release;" ::: "memory");
+    }
+    __device__ __forceinline__ void wait() const
+    {
+        asm volatile("barrier.cluster.wait.acquire;" ::: "memory");
+    }
 };
 
 // The two CTAs of a 2-way task inside a larger cluster (the work list's
@@ -332,6 +347,8 @@ struct PairSync {
         }
         __syncthreads();
     }
+    __device__ __forceinline__ void arrive() const { (*this)(); }
+    __device__ __forceinline__ void wait() const {}
 };
 
 // One position of the consumer's combine: g[r] = the sub-spectra F_r(k)
@@ -374,8 +391,11 @@ __device__ __forceinline__ void cons_task(const ConsArgs &a, float2 *sm, const f
     const int q0 = c * Mc, q1 = min(M, q0 + Mc);
     const float2 *code = a.code + (size_t)(a.code_per_bin ? b : prn) * R * M;
     for (int s = 0; s < ns_run; ++s) {
-        // all CTAs of the cluster are done with their shared memory
-        sync();
+        // all CTAs of the cluster are done with their shared memory: arrive
+        // here, wait after this thread's first global loads of the combine
+        // are in flight (before its first store into shared memory)
+        sync.arrive();
+        bool waited = false;
         const bool run = active && s < a.n_sum;
         const float2 *Xs = a.X + ((size_t)b * a.n_sum + s) * R * M;
         // U positions per iteration: all their global loads are issued
@@ -400,6 +420,10 @@ __device__ __forceinline__ void cons_task(const ConsArgs &a, float2 *sm, const f
                     cs[u][r] = __ldg(code + (size_t)r * M + ql);
                 }
             }
+            if (!waited) {
+                sync.wait();
+                waited = true;
+            }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 if (!ok[u]) continue;
@@ -415,6 +439,7 @@ __device__ __forceinline__ void cons_task(const ConsArgs &a, float2 *sm, const f
                 }
             }
         }
+        if (!waited) sync.wait();
         sync();
         if (!run) continue;
         // the next sum's spectra head for L2 during this sum's transform
